@@ -1,0 +1,350 @@
+"""Benchmark of the B200 rmeshvk tiled training step.
+
+Workload (one "step"): the batched configuration of the reference's benchmark
+set -- a Delaunay mesh of 100,000 points from an 8-component Gaussian mixture
+(~650k tets), 16 cameras on a sphere of radius U[2.5, 4] with resolutions drawn
+from {256^2, 512^2, 800x600, 1024^2}; one step renders all 16 views, computes
+the L2 loss against seeded targets, back-propagates and applies one Adam update
+(forward + backward + Adam).  Synthetic, seeded data; colours are the
+reference's base-colour training path (spherical harmonics are not evaluated by
+the reference's train_step).
+
+Line printed by rank 0 (one JSON object):
+  value          train-steps/s of the batched, graph-captured path, inputs in HBM
+  e2e            same metric through the public API with the targets in pinned
+                 host memory copied every step and the losses read back
+  plain          train-steps/s of the one-view-per-launch path on the same step
+  roofline       dominant kernel (fused forward+loss+adjoint compositing):
+                 algorithmic bytes / measured launch time vs measured HBM peak
+  cpu_baseline   the CPU oracle (C port of the reference kernels) on all host
+                 cores, timed on a sample of the step and scaled to the metric
+
+``--impl reference`` times the CPU port of the reference's kernels instead (the
+reference itself is a wgpu/Vulkan program that cannot run on this machine).
+Multi-GPU (torchrun): every rank trains its own 16 views (weak scaling) and
+the ranks' gradients are summed before Adam.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+RES = ((256, 256), (512, 512), (800, 600), (1024, 1024))
+N_VIEWS = 16
+LR = dict(lr_verts=1e-4, lr_dens=1e-2, lr_grads=1e-3)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def build_workload(points: int, seed: int, rank: int):
+    from rmesh_b200.camera import orbit_cameras
+    from rmesh_b200.scenes import gmm_cloud, make_scene
+
+    rng = np.random.default_rng(seed)
+    scene = make_scene(gmm_cloud(points, rng), rng, sh_degree=0)
+    cams = orbit_cameras(N_VIEWS, seed=seed + 1 + 1000 * rank, radius=(2.5, 4.0), resolutions=RES)
+    trng = np.random.default_rng(seed + 2 + 1000 * rank)
+    gts = [trng.uniform(0, 1, (c.height, c.width, 3)).astype(np.float32) for c in cams]
+    return scene, cams, gts
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, gpu_index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={gpu_index}", f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.f:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.f.name)
+        load = [s for s in sm if s > 0.5 * max(sm)] if sm else []
+        return {"sm_mhz": float(np.median(load)) if load else None,
+                "sm_max_mhz": float(max(smax)) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_bytes(n_pairs: int, n_pix: int, N: int, M: int) -> int:
+    """Unique traffic of the fused forward+loss+adjoint compositing kernel:
+    both passes read each (tile, tet) slot (4 B) and its tet record (64 B) plus
+    colour (16 B); per pixel the 12 B target; gradients 80 B per tet slot."""
+    rec = 4 + 64 + 16
+    return 2 * n_pairs * rec + 12 * n_pix + 80 * M
+
+
+def run_gpu(args):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    from rmesh_b200 import RMeshRenderer
+    from rmesh_b200 import _lib
+
+    scene, cams, gts = build_workload(args.points, args.seed, rank)
+    r = RMeshRenderer(scene["vertices"], scene["indices"], scene["base_colors"], scene["densities"],
+                      scene["color_grads"], scene["circumdata"], cams[0].width, cams[0].height,
+                      tile_size=args.tile_size, device=local)
+    stream = torch.cuda.Stream(device=local)
+    r.set_stream(stream.cuda_stream)
+    n_pix = sum(c.width * c.height for c in cams)
+    gt_host = torch.from_numpy(np.concatenate([g.ravel() for g in gts])).pin_memory()
+    gt_dev = gt_host.to(f"cuda:{local}")
+    torch.cuda.synchronize()
+
+    slots = r.grad_slots() if world > 1 else None
+
+    def step(mode, gt):
+        if dist is None:
+            return r.train_step_views(cams, gt, loss_type=1, mode=mode, **LR)
+        # data parallel: this rank's views -> sum of all ranks' gradients -> Adam
+        losses = r.accumulate_views(cams, gt, loss_type=1, mode=mode)
+        with torch.cuda.stream(stream):
+            dist.all_reduce(slots)
+        r.apply_adam(**LR)
+        return losses
+
+    def timed(mode, gt, steps):
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            step(mode, gt)
+        e1.record(stream)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if dist is not None:
+            t = torch.tensor([ms], device=f"cuda:{local}")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms / steps
+
+    # warm-up (also sizes the pair buffers and captures the graph)
+    for mode in ("graph", "batched", "plain"):
+        for _ in range(max(1, args.warmup)):
+            step(mode, gt_dev)
+    r.stage_times()  # reset counters
+
+    clk = Clocks(local)
+    ms_graph = timed("graph", gt_dev, args.steps)
+    _, launches, total_launches = r.stage_times()
+    ms_e2e = timed("graph", gt_host, args.steps)
+    clocks = clk.stop()
+    ms_plain = timed("plain", gt_dev, max(1, args.steps // 2))
+    r.stage_times()
+
+    # per-stage device times of the batched path (CUDA events on the library stream)
+    r.set_profiling(True)
+    for _ in range(max(1, args.steps // 2)):
+        step("batched", gt_dev)
+    stage_ms, stage_n, _ = r.stage_times()
+    r.set_profiling(False)
+    nsteps_prof = max(1, args.steps // 2)
+    info = r.info()
+    comp_ms = stage_ms["composite"] / max(stage_n["composite"], 1)
+    alg = algorithmic_bytes(int(info.n_pairs_last), n_pix, r.n_vertices, r.n_tets)
+    peak, peak_kind = peaks()
+    achieved = alg / (comp_ms * 1e-3) / 1e9
+
+    steps_per_s = world * 1000.0 / ms_graph
+    out = {
+        "metric": "fwd+bwd train-steps/s (16 mixed-resolution views, batched graph-captured step)",
+        "value": round(steps_per_s, 4),
+        "unit": "train-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_graph, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded GMM Delaunay mesh, seeded targets)",
+        "config": {
+            "workload": f"batched: {args.points}-point 8-component GMM Delaunay mesh ({r.n_tets} tets), "
+                        f"{N_VIEWS} views from {{256^2,512^2,800x600,1024^2}}, L2 loss, Adam",
+            "n_tets": r.n_tets, "n_vertices": r.n_vertices, "views_per_gpu": N_VIEWS,
+            "pixels_per_step_per_gpu": n_pix, "tile_size": args.tile_size, "color_mode": "base_colors",
+            "parallelism": f"dp{world} (views sharded, gradients summed)" if world > 1 else "single GPU",
+            "l2": "inputs larger than L2 (mesh records + pair lists > 126 MB per step)",
+        },
+        "mpix_per_s": round(world * n_pix / (ms_graph * 1e-3) / 1e6, 2),
+        "plain": {"value": round(world * 1000.0 / ms_plain, 4), "unit": "train-steps/s", "ms_per_step": round(ms_plain, 4)},
+        "batched_graph_vs_plain": round(ms_plain / ms_graph, 3),
+        "e2e": {"value": round(world * 1000.0 / ms_e2e, 4), "unit": "train-steps/s",
+                "h2d_bytes_per_step": int(n_pix * 12 + N_VIEWS * 160 + 48),
+                "d2h_bytes_per_step": int(_lib.COUNTERS_BYTES)},
+        "gpu_launches": int(total_launches),
+        "stage_ms_per_step": {k: round(v / nsteps_prof, 4) for k, v in stage_ms.items()},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "kernel": "tile_kernel<12,kModeTrain> (fused forward+loss+adjoint)",
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
+                     "fallback 6.65 TB/s", "launch_ms": round(comp_ms, 4), "algorithmic_bytes": alg,
+                     "n_pairs": int(info.n_pairs_last)},
+        "clocks": clocks,
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(scene, cams, gts, args)
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    r.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def cpu_baseline(scene, cams, gts, args, budget_s=20.0):
+    """The oracle's train step (project, emit, sort, ranges, rasterize, loss,
+    adjoint, Adam) on all host cores for views of the step until ~budget_s,
+    scaled by pixels to a full step."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle
+
+    o = Oracle("f32")
+    threads = o.max_threads
+    # cheapest views first so the sample covers several views within the budget
+    order = sorted(range(len(cams)), key=lambda i: cams[i].width * cams[i].height)
+    t0 = time.perf_counter()
+    px_done, views_done = 0, 0
+    for i in order:
+        cam, gt = cams[i], gts[i]
+        fwd = o.forward_tiled(scene, cam, args.tile_size)
+        _, dl = o.loss(fwd["image"], gt, 1)
+        o.backward(scene, cam, dl, fwd, args.tile_size, threads=threads)
+        px_done += cam.width * cam.height
+        views_done += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    n_pix = sum(c.width * c.height for c in cams)
+    t_step = dt * n_pix / px_done
+    return {"value": round(1.0 / t_step, 6), "unit": "train-steps/s", "cores": threads, "kind": "port",
+            "sample": f"{views_done} of {len(cams)} views ({px_done} px) in {dt:.1f} s, scaled by pixels "
+                      f"to the {n_pix}-px step; C oracle, OpenMP {threads} threads",
+            "mpix_per_s": round(px_done / dt / 1e6, 4)}
+
+
+def run_reference(args):
+    """CPU port of the reference kernels (the reference's wgpu pipeline needs a
+    Vulkan/Metal device, unavailable on this machine)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    scene, cams, gts = build_workload(args.points, args.seed, 0)
+    n_pix = sum(c.width * c.height for c in cams)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from oracle import Oracle
+
+    o = Oracle("f32")
+    threads = o.max_threads
+    cam = min(cams, key=lambda c: c.width * c.height)
+    gt = gts[cams.index(cam)]
+
+    def one():
+        fwd = o.forward_tiled(scene, cam, args.tile_size)
+        _, dl = o.loss(fwd["image"], gt, 1)
+        o.backward(scene, cam, dl, fwd, args.tile_size, threads=threads)
+
+    for _ in range(args.warmup):
+        one()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        one()
+    dt = (time.perf_counter() - t0) / args.steps
+    t_step = dt * n_pix / (cam.width * cam.height)
+    v = round(1.0 / t_step, 6)
+    sample = (f"one {cam.width}x{cam.height} view per step ({cam.width * cam.height} px), scaled by pixels to the "
+              f"{n_pix}-px 16-view step; C port of the reference kernels, OpenMP {threads} threads")
+    print(json.dumps({
+        "impl": "reference", "metric": "fwd+bwd train-steps/s (16 mixed-resolution views, batched graph-captured step)",
+        "value": v, "unit": "train-steps/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(t_step * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded GMM Delaunay mesh, seeded targets)",
+        "config": {"workload": f"batched: {args.points}-point GMM Delaunay mesh, {N_VIEWS} views"},
+        "cpu_baseline": {"value": v, "unit": "train-steps/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": v, "unit": "train-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference's own pipeline is wgpu (Vulkan/Metal) and cannot run here; this is its CPU port",
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--points", type=int, default=100_000)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--tile-size", type=int, default=12)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,188 @@
+/*
+ * rmesh_b200.h -- C ABI of the B200-native rmeshvk tiled volume-rendering path.
+ *
+ * One context owns a tet mesh (fixed topology), its trainable parameters, the
+ * Adam moments and every device buffer of the path.  Each entry point below
+ * replaces one method of the reference's PyO3 class `RMeshRenderer`
+ * (crates/rmesh-python/src/lib.rs); the comment on each names the method and
+ * its lines.  Paths are relative to the reference repository root.
+ *
+ * Conventions
+ *  - Every call returns an int status (RMESH_OK = 0).  rmesh_last_error()
+ *    returns a message for the last failing call on that context.
+ *  - Array pointers may be host memory or CUDA device memory (unified virtual
+ *    addressing decides); device pointers avoid a host round trip.
+ *  - Arrays are flat, C-contiguous, float32 / uint32, with the reference's
+ *    layouts: vertices [3N], indices [4M], base_colors [3M], densities [M],
+ *    color_grads [3M], circumdata [4M] = (cx, cy, cz, r^2), images [H][W][4]
+ *    premultiplied RGBA, ground truth [H][W][3] RGB.
+ *  - Work is ordered on the context's CUDA stream (rmesh_set_stream); calls
+ *    that return host-visible results synchronise that stream.  A context is
+ *    not thread-safe; use one per thread.
+ */
+#ifndef RMESH_B200_H
+#define RMESH_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RMESH_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define RMESH_API __attribute__((visibility("default")))
+#else
+#define RMESH_API
+#endif
+
+/* status codes */
+#define RMESH_OK 0
+#define RMESH_ERR_INVALID_ARG 1  /* bad sizes/pointers (reference: PyValueError) */
+#define RMESH_ERR_CUDA 2         /* CUDA runtime error (reference: PyRuntimeError, lib.rs:306-329) */
+#define RMESH_ERR_OOM 3          /* device allocation failed */
+#define RMESH_ERR_PAIR_OVERFLOW 4 /* pair buffers too small even after growing to the limit */
+#define RMESH_ERR_TIMEOUT 5      /* a bounded device spin gave up (kernel returned an error, no hang) */
+#define RMESH_ERR_STATE 6        /* call order violated (e.g. backward before forward_tiled) */
+#define RMESH_ERR_NO_DEVICE 7    /* no CUDA device / library built for another architecture */
+
+typedef struct RmeshCtx RmeshCtx;
+
+/* Mesh and initial parameters (reference constructor, lib.rs:265-277). */
+typedef struct {
+  int64_t n_vertices;        /* N */
+  int64_t n_tets;            /* M */
+  const float* vertices;     /* [3N] */
+  const uint32_t* indices;   /* [4M] */
+  const float* base_colors;  /* [3M] */
+  const float* densities;    /* [M] */
+  const float* color_grads;  /* [3M] */
+  const float* circumdata;   /* [4M] */
+  int32_t width;             /* default view size */
+  int32_t height;
+  int32_t aux_dim;           /* reference aux_dim (only 0 is supported) */
+  int32_t tile_size;         /* 0 -> 12, the reference's hard-coded value (lib.rs:442) */
+  int32_t device;            /* CUDA device ordinal, -1 = current */
+  int32_t reserved[3];
+} RmeshSceneDesc;
+
+/* One view: the three arrays of the reference camera methods (lib.rs:1040-1048)
+ * plus its image size. */
+typedef struct {
+  float cam_pos[3];
+  float vp[16];              /* view-projection, column-major */
+  float c2w_intrinsics[16];  /* c2w col0 xyz,0, col1 xyz,0, col2 xyz,0, fx,fy,cx,cy */
+  int32_t width;
+  int32_t height;
+} RmeshCamera;
+
+/* Options of the multi-view training step (no reference counterpart; the
+ * learning rates and loss type are those of train_step, lib.rs:2405-2415). */
+typedef struct {
+  float lr_verts;
+  float lr_dens;
+  float lr_grads;
+  float lr_base;      /* 0 keeps base colours fixed, as the reference train_step does */
+  int32_t loss_type;  /* 0 = L1, 1 = L2 */
+  int32_t mode;       /* RMESH_MODE_* */
+  int32_t reserved[2];
+} RmeshTrainOpts;
+
+#define RMESH_MODE_PLAIN 0    /* one launch sequence per view, one tile per CTA */
+#define RMESH_MODE_BATCHED 1  /* all views in one launch sequence, persistent (view,tile) queue */
+#define RMESH_MODE_GRAPH 2    /* BATCHED, captured once as a CUDA graph and replayed */
+
+typedef struct {
+  int64_t n_vertices, n_tets;
+  int32_t width, height, tile_size, n_views_last;
+  uint32_t step;
+  uint32_t last_error_bits;      /* device status bits of the last run */
+  uint64_t n_visible_last;       /* tile-touching (view, tet) pairs of the last run */
+  uint64_t n_pairs_last;         /* (tile, tet) slots of the last run */
+  uint64_t pair_capacity;
+  uint64_t device_bytes;         /* device memory held by the context */
+} RmeshInfo;
+
+/* ---- lifetime ------------------------------------------------------------ */
+/* RMeshRenderer.__new__ (lib.rs:265-870): copies every input to the device. */
+RMESH_API int rmesh_create(const RmeshSceneDesc* desc, RmeshCtx** out);
+RMESH_API int rmesh_destroy(RmeshCtx* ctx);
+RMESH_API const char* rmesh_last_error(const RmeshCtx* ctx);
+RMESH_API int rmesh_abi_version(void);
+
+/* ---- settings ------------------------------------------------------------- */
+RMESH_API int rmesh_set_stream(RmeshCtx* ctx, void* cuda_stream);     /* no reference counterpart */
+RMESH_API int rmesh_set_min_t(RmeshCtx* ctx, float min_t);            /* set_min_t, lib.rs:873-875 */
+RMESH_API int rmesh_set_tile_size(RmeshCtx* ctx, int32_t tile_size);  /* 8, 12 or 16 (reference fixes 12) */
+
+/* ---- parameters ----------------------------------------------------------- */
+/* update_params, lib.rs:2641-2669 (any pointer may be NULL to keep that group) */
+RMESH_API int rmesh_update_params(RmeshCtx* ctx, const float* vertices, const float* base_colors,
+                        const float* densities, const float* color_grads);
+/* get_params, lib.rs:2674-2686 */
+RMESH_API int rmesh_get_params(RmeshCtx* ctx, float* vertices, float* base_colors, float* densities,
+                     float* color_grads);
+/* getters step/width/height, lib.rs:2688-2705 */
+RMESH_API int rmesh_get_info(RmeshCtx* ctx, RmeshInfo* info);
+
+/* ---- the path ------------------------------------------------------------- */
+/* forward_tiled, lib.rs:1041-1204: project -> bin -> sort -> ranges -> composite.
+ * rgba_out [H][W][4]; aux_out [H][W][8] or NULL (render_aux). */
+RMESH_API int rmesh_forward_tiled(RmeshCtx* ctx, const RmeshCamera* cam, float* rgba_out, float* aux_out);
+
+/* backward, lib.rs:1894-2031: must follow rmesh_forward_tiled on the same context;
+ * reuses that call's sorted tile lists and image.  Outputs (any may be NULL):
+ * d_vertices [3N], d_densities [M], d_base_colors [3M], d_color_grads [3M]. */
+RMESH_API int rmesh_backward(RmeshCtx* ctx, const float* dl_d_image, float* d_vertices, float* d_densities,
+                   float* d_base_colors, float* d_color_grads);
+
+/* train_step, lib.rs:2405-2636: forward, loss, adjoint, Adam on vertices,
+ * densities and color_grads; step += 1.  gt_rgb [H][W][3].  *loss_out receives
+ * sum over pixels and RGB of (r-gt)^2 / n_pixels (L2) or |r-gt| / n_pixels (L1);
+ * the reference returns 0.0 here (its loss buffer is never written). */
+RMESH_API int rmesh_train_step(RmeshCtx* ctx, const RmeshCamera* cam, const float* gt_rgb, float lr_verts,
+                     float lr_dens, float lr_grads, int32_t loss_type, float* loss_out);
+
+/* Multi-view training step (no reference counterpart): the gradient of the sum
+ * of the per-view losses over n_views cameras, then ONE Adam update.
+ * gt_rgb holds the views' [H][W][3] images back to back.  loss_out (optional)
+ * receives n_views per-view losses. */
+RMESH_API int rmesh_train_step_views(RmeshCtx* ctx, const RmeshCamera* cams, int32_t n_views, const float* gt_rgb,
+                           const RmeshTrainOpts* opts, float* loss_out);
+
+/* Data-parallel split of rmesh_train_step_views (no reference counterpart):
+ * accumulate the gradient of this rank's views into the context's per-tet
+ * gradient slots (zeroed first, no Adam); expose those slots (device memory,
+ * n_floats = 20 * M) so the caller can sum them across ranks, e.g. with an
+ * NCCL all-reduce; then apply one Adam update from the slots. */
+RMESH_API int rmesh_accumulate_views(RmeshCtx* ctx, const RmeshCamera* cams, int32_t n_views, const float* gt_rgb,
+                                     const RmeshTrainOpts* opts, float* loss_out);
+RMESH_API int rmesh_grad_slots(RmeshCtx* ctx, float** device_ptr, uint64_t* n_floats);
+RMESH_API int rmesh_apply_adam(RmeshCtx* ctx, const RmeshTrainOpts* opts);
+
+/* ---- inspection (parity tests) --------------------------------------------- */
+/* tiles_touched of the last forward, indexed by tet id ([M], single view). */
+RMESH_API int rmesh_debug_tiles_touched(RmeshCtx* ctx, uint32_t* out);
+/* sorted (tile id, tet id) slots of the last forward; *n receives the slot count
+ * (sentinel slots carry tile 0xFFFFFFFF); at most cap entries are written. */
+RMESH_API int rmesh_debug_pairs(RmeshCtx* ctx, uint32_t* tile_ids, uint32_t* tet_ids, uint64_t cap, uint64_t* n);
+/* [start, end) per tile of the last forward ([2 * tiles]). */
+RMESH_API int rmesh_debug_ranges(RmeshCtx* ctx, uint32_t* ranges, uint64_t n_tiles);
+
+/* ---- profiling -------------------------------------------------------------- */
+/* When enabled, CUDA events bracket each stage on the context stream; the
+ * accumulated milliseconds are returned by rmesh_stage_times in the order
+ * records, project, tet_sort, emit, pair_sort, ranges, composite, adam.
+ * ms_out has RMESH_N_STAGES entries; launches_out has RMESH_N_STAGES + 1
+ * (per-stage span counts, then the number of kernels launched).  Both are
+ * reset by the call. */
+#define RMESH_N_STAGES 8
+RMESH_API int rmesh_set_profiling(RmeshCtx* ctx, int32_t on);
+RMESH_API int rmesh_stage_times(RmeshCtx* ctx, float* ms_out, int32_t* launches_out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RMESH_B200_H */

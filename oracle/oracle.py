@@ -1,0 +1,246 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+Loads ``oracle/lib/librmesh_oracle_{f32,f64}.so`` (built by ``oracle/Makefile``)
+and sequences the restated kernels the way the reference binding does:
+
+* ``forward_tiled``  crates/rmesh-python/src/lib.rs:1041-1204
+  project -> emit (sentinel-filled slots) -> stable sort -> tile ranges -> rasterize
+* ``backward``       crates/rmesh-python/src/lib.rs:1894-2031
+* ``train_step``     crates/rmesh-python/src/lib.rs:2405-2636
+  (step += 1; Adam on vertices, densities, color_grads; base colors untouched)
+
+Only the test tree, the smoke check and the benchmark's CPU baseline use it.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIBS = {}
+
+_f32p = ctypes.POINTER(ctypes.c_float)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_u8p = ctypes.POINTER(ctypes.c_uint8)
+_i64p = ctypes.POINTER(ctypes.c_int64)
+
+
+def build() -> None:
+    """Compile the oracle libraries (gcc, no GPU needed)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def _lib(dtype: str):
+    if dtype not in _LIBS:
+        path = os.path.join(_HERE, "lib", f"librmesh_oracle_{dtype}.so")
+        if not os.path.exists(path):
+            build()
+        _LIBS[dtype] = ctypes.CDLL(path)
+    return _LIBS[dtype]
+
+
+def _ptr(a, ctype):
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctype)
+
+
+class Oracle:
+    """CPU restatement of the tiled path in float32 (``dtype='f32'``) or float64."""
+
+    def __init__(self, dtype: str = "f32", threads: int = 0):
+        self.dtype = dtype
+        self.np = np.float32 if dtype == "f32" else np.float64
+        self.rp = _f32p if dtype == "f32" else _f64p
+        self.lib = _lib(dtype)
+        s = "_" + dtype
+        L = self.lib
+        self._project = getattr(L, "orc_project" + s)
+        self._emit = getattr(L, "orc_emit" + s)
+        self._emit.restype = ctypes.c_int64
+        self._sort = getattr(L, "orc_sort_pairs" + s)
+        self._bits = getattr(L, "orc_sorting_bits" + s)
+        self._ranges = getattr(L, "orc_tile_ranges" + s)
+        self._raster = getattr(L, "orc_rasterize" + s)
+        self._loss = getattr(L, "orc_loss" + s)
+        self._loss.restype = ctypes.c_double
+        self._backward = getattr(L, "orc_backward" + s)
+        self._adam = getattr(L, "orc_adam" + s)
+        rt = ctypes.c_float if dtype == "f32" else ctypes.c_double
+        self._rt = rt
+        self._raster.argtypes = [self.rp, _u32p, self.rp, self.rp, self.rp, _u32p, _u32p, self.rp, self.rp,
+                                 self.rp, self.rp, ctypes.c_int, ctypes.c_int, ctypes.c_int, rt,
+                                 self.rp, self.rp, _u32p]
+        self._adam.argtypes = [ctypes.c_int64, self.rp, self.rp, self.rp, self.rp, ctypes.c_uint32, rt, rt, rt, rt]
+        if threads > 0:
+            getattr(L, "orc_set_threads" + s)(int(threads))
+        self.max_threads = getattr(L, "orc_max_threads" + s)()
+
+    # ---- helpers ----------------------------------------------------------
+    def _r(self, a):
+        return np.ascontiguousarray(np.asarray(a, dtype=self.np))
+
+    @staticmethod
+    def _u(a):
+        return np.ascontiguousarray(np.asarray(a, dtype=np.uint32))
+
+    def _cam(self, cam):
+        ci = np.asarray(cam.c2w_intrinsics, dtype=np.float64)
+        c2w = np.concatenate([ci[0:3], ci[4:7], ci[8:11]])
+        return (self._r(cam.vp), self._r(c2w), self._r(ci[12:16]), self._r(cam.cam_pos),
+                int(cam.width), int(cam.height))
+
+    @staticmethod
+    def sorting_bits(num_tiles: int) -> int:
+        tile_bits = 1 if num_tiles <= 1 else int(num_tiles - 1).bit_length()
+        return (32 + tile_bits + 7) & ~7
+
+    # ---- stages -----------------------------------------------------------
+    def project(self, scene, cam, tile_size=12, sh_packed=None, sh_degree=0):
+        v, idx = self._r(scene["vertices"]), self._u(scene["indices"])
+        m = idx.size // 4
+        vp, c2w, intr, cp, W, H = self._cam(cam)
+        visible = np.zeros(m, dtype=np.uint8)
+        tt = np.zeros(m, dtype=np.uint32)
+        colors = np.zeros(3 * m, dtype=self.np)
+        shp = None if sh_packed is None else self._u(sh_packed)
+        self._project(ctypes.c_int64(m), _ptr(v, self.rp), _ptr(idx, _u32p), _ptr(self._r(scene["densities"]), self.rp),
+                      _ptr(self._r(scene["color_grads"]), self.rp), _ptr(self._r(scene["circumdata"]), self.rp),
+                      _ptr(self._r(scene["base_colors"]), self.rp), _ptr(shp, _u32p), ctypes.c_int(sh_degree),
+                      _ptr(vp, self.rp), _ptr(cp, self.rp), ctypes.c_int(W), ctypes.c_int(H), ctypes.c_int(tile_size),
+                      _ptr(visible, _u8p), _ptr(tt, _u32p), _ptr(colors, self.rp))
+        return visible, tt, colors
+
+    def emit(self, scene, cam, visible, tiles_touched, tile_size=12):
+        v, idx = self._r(scene["vertices"]), self._u(scene["indices"])
+        m = idx.size // 4
+        vp, c2w, intr, cp, W, H = self._cam(cam)
+        cap = int(tiles_touched[visible.astype(bool)].astype(np.int64).sum())
+        lo = np.zeros(max(cap, 1), dtype=np.uint32)
+        hi = np.zeros(max(cap, 1), dtype=np.uint32)
+        vals = np.zeros(max(cap, 1), dtype=np.uint32)
+        emitted = ctypes.c_int64(0)
+        P = self._emit(ctypes.c_int64(m), _ptr(v, self.rp), _ptr(idx, _u32p), _ptr(self._r(scene["circumdata"]), self.rp),
+                       _ptr(vp, self.rp), _ptr(cp, self.rp), ctypes.c_int(W), ctypes.c_int(H), ctypes.c_int(tile_size),
+                       _ptr(np.ascontiguousarray(visible), _u8p), _ptr(self._u(tiles_touched), _u32p),
+                       _ptr(lo, _u32p), _ptr(hi, _u32p), _ptr(vals, _u32p), ctypes.c_int64(cap),
+                       ctypes.byref(emitted))
+        assert P == cap
+        return lo[:P], hi[:P], vals[:P], int(emitted.value)
+
+    def sort_pairs(self, lo, hi, vals, num_tiles):
+        lo, hi, vals = lo.copy(), hi.copy(), vals.copy()
+        self._sort(ctypes.c_int64(lo.size), ctypes.c_int(self.sorting_bits(num_tiles)), _ptr(lo, _u32p),
+                   _ptr(hi, _u32p), _ptr(vals, _u32p))
+        return lo, hi, vals
+
+    def tile_ranges(self, hi_sorted, num_tiles):
+        ranges = np.zeros(2 * num_tiles, dtype=np.uint32)
+        self._ranges(ctypes.c_int64(hi_sorted.size), _ptr(self._u(hi_sorted), _u32p), _ptr(ranges, _u32p))
+        return ranges
+
+    def rasterize(self, scene, cam, colors, vals, ranges, tile_size=12, min_t=0.0, aux=False, stats=False):
+        vp, c2w, intr, cp, W, H = self._cam(cam)
+        rgba = np.zeros(H * W * 4, dtype=self.np)
+        auxb = np.zeros(H * W * 8, dtype=self.np) if aux else None
+        st = np.zeros(H * W * 4, dtype=np.uint32) if stats else None
+        self._raster(_ptr(self._r(scene["vertices"]), self.rp), _ptr(self._u(scene["indices"]), _u32p),
+                     _ptr(self._r(colors), self.rp), _ptr(self._r(scene["densities"]), self.rp),
+                     _ptr(self._r(scene["color_grads"]), self.rp), _ptr(self._u(vals), _u32p),
+                     _ptr(self._u(ranges), _u32p), _ptr(vp, self.rp), _ptr(c2w, self.rp), _ptr(intr, self.rp),
+                     _ptr(cp, self.rp), W, H, tile_size, self._rt(min_t), _ptr(rgba, self.rp), _ptr(auxb, self.rp),
+                     _ptr(st, _u32p))
+        out = {"image": rgba.reshape(H, W, 4)}
+        if aux:
+            out["aux"] = auxb.reshape(H, W, 8)
+        if stats:
+            out["stats"] = st.reshape(H, W, 4)
+        return out
+
+    def loss(self, rendered, gt, loss_type=1):
+        rendered = self._r(rendered)
+        H, W = rendered.shape[0], rendered.shape[1]
+        dl = np.zeros(H * W * 4, dtype=self.np)
+        val = self._loss(ctypes.c_int(W), ctypes.c_int(H), ctypes.c_int(loss_type), _ptr(rendered, self.rp),
+                         _ptr(self._r(gt), self.rp), _ptr(dl, self.rp))
+        return float(val), dl.reshape(H, W, 4)
+
+    def backward_raw(self, scene, cam, colors, vals, ranges, dl, rendered, tile_size=12, threads=1):
+        vp, c2w, intr, cp, W, H = self._cam(cam)
+        n = scene["vertices"].size
+        m = scene["indices"].size // 4
+        dv = np.zeros(n, dtype=self.np)
+        dd = np.zeros(m, dtype=self.np)
+        dg = np.zeros(3 * m, dtype=self.np)
+        db = np.zeros(3 * m, dtype=self.np)
+        self._backward(_ptr(self._r(scene["vertices"]), self.rp), _ptr(self._u(scene["indices"]), _u32p),
+                       _ptr(self._r(colors), self.rp), _ptr(self._r(scene["densities"]), self.rp),
+                       _ptr(self._r(scene["color_grads"]), self.rp), _ptr(self._u(vals), _u32p),
+                       _ptr(self._u(ranges), _u32p), _ptr(vp, self.rp), _ptr(c2w, self.rp), _ptr(intr, self.rp),
+                       _ptr(cp, self.rp), ctypes.c_int(W), ctypes.c_int(H), ctypes.c_int(tile_size),
+                       _ptr(self._r(dl), self.rp), _ptr(self._r(rendered), self.rp), _ptr(dv, self.rp),
+                       _ptr(dd, self.rp), _ptr(dg, self.rp), _ptr(db, self.rp), ctypes.c_int(threads))
+        return {"d_vertices": dv, "d_densities": dd, "d_color_grads": dg, "d_base_colors": db}
+
+    def adam(self, params, grads, m, v, step, lr, beta1=0.9, beta2=0.999, eps=1e-8):
+        """In place on float arrays of this oracle's dtype."""
+        self._adam(ctypes.c_int64(params.size), _ptr(params, self.rp), _ptr(self._r(grads), self.rp),
+                   _ptr(m, self.rp), _ptr(v, self.rp), ctypes.c_uint32(step), self._rt(lr), self._rt(beta1),
+                   self._rt(beta2), self._rt(eps))
+
+    # ---- host sequencing --------------------------------------------------
+    def forward_tiled(self, scene, cam, tile_size=12, min_t=0.0, aux=False, stats=False,
+                      sh_packed=None, sh_degree=0):
+        """lib.rs:1041-1204.  Returns the image plus every intermediate buffer."""
+        W, H = int(cam.width), int(cam.height)
+        tiles_x = (W + tile_size - 1) // tile_size
+        tiles_y = (H + tile_size - 1) // tile_size
+        num_tiles = tiles_x * tiles_y
+        visible, tt, colors = self.project(scene, cam, tile_size, sh_packed, sh_degree)
+        lo, hi, vals, emitted = self.emit(scene, cam, visible, tt, tile_size)
+        slo, shi, svals = self.sort_pairs(lo, hi, vals, num_tiles)
+        ranges = self.tile_ranges(shi, num_tiles)
+        out = self.rasterize(scene, cam, colors, svals, ranges, tile_size, min_t, aux, stats)
+        out.update(visible=visible, tiles_touched=tt, colors=colors, key_lo=slo, key_hi=shi, vals=svals,
+                   ranges=ranges, P=int(lo.size), emitted=emitted, num_tiles=num_tiles,
+                   unsorted=(lo, hi, vals))
+        return out
+
+    def backward(self, scene, cam, dl_d_image, fwd, tile_size=12, threads=1):
+        """lib.rs:1894-2031 (the sort it redoes equals the forward's)."""
+        return self.backward_raw(scene, cam, fwd["colors"], fwd["vals"], fwd["ranges"],
+                                 np.asarray(dl_d_image).reshape(-1), fwd["image"].reshape(-1), tile_size, threads)
+
+    def loss_value(self, scene, cam, gt, loss_type=1, tile_size=12):
+        fwd = self.forward_tiled(scene, cam, tile_size)
+        val, _ = self.loss(fwd["image"], gt, loss_type)
+        return val
+
+
+class OracleTrainer:
+    """lib.rs:2405-2636 on the CPU: one view per step, Adam on three groups."""
+
+    def __init__(self, scene, dtype="f32", tile_size=12):
+        self.o = Oracle(dtype)
+        self.scene = {k: (np.array(v, dtype=self.o.np) if k in ("vertices", "densities", "color_grads",
+                                                                "base_colors", "circumdata") else v)
+                      for k, v in scene.items()}
+        self.tile_size = tile_size
+        self.step = 0
+        z = lambda k: np.zeros_like(self.scene[k])
+        self.m = {k: z(k) for k in ("vertices", "densities", "color_grads")}
+        self.v = {k: z(k) for k in ("vertices", "densities", "color_grads")}
+
+    def train_step(self, cam, gt, lr_verts, lr_dens, lr_grads, loss_type=1):
+        fwd = self.o.forward_tiled(self.scene, cam, self.tile_size)
+        loss, dl = self.o.loss(fwd["image"], gt, loss_type)
+        g = self.o.backward(self.scene, cam, dl, fwd, self.tile_size)
+        self.step += 1
+        for key, gk, lr in (("vertices", "d_vertices", lr_verts), ("densities", "d_densities", lr_dens),
+                            ("color_grads", "d_color_grads", lr_grads)):
+            self.o.adam(self.scene[key], g[gk], self.m[key], self.v[key], self.step, lr)
+        return loss, fwd, g

@@ -1,0 +1,1040 @@
+// C-ABI implementation: context, device buffers and stage sequencing.
+//
+// Host sequencing restates crates/rmesh-python/src/lib.rs:
+//   forward_tiled  :1041-1204   backward :1894-2031   train_step :2405-2636
+// with three B200 changes: (1) no host readback between stages -- counts stay
+// on the device and every kernel reads them from there; (2) the adjoint reuses
+// the forward's sorted tile lists instead of re-sorting; (3) train steps run the
+// fused forward+loss+adjoint tile kernel and one multi-group Adam launch.
+//
+// Capacity: pair buffers start from an estimate; a run that overflows raises a
+// device bit, Adam is skipped on the device, and the host grows the buffers to
+// the exact count and repeats the call.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/rmesh_b200.h"
+#include "adam.cuh"
+#include "bin.cuh"
+#include "common.cuh"
+#include "project.cuh"
+#include "sort.cuh"
+#include "tile.cuh"
+
+using namespace rm;
+
+static_assert(sizeof(Counters) == 792, "Counters layout is mirrored by the Python binding");
+
+namespace {
+
+struct DevBuf {
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    bytes = 0;
+  }
+  // grows (never shrinks); returns a cudaError_t; *grew set when reallocated
+  cudaError_t ensure(size_t n, bool* grew = nullptr) {
+    if (n <= bytes && p) return cudaSuccess;
+    release();
+    size_t want = std::max<size_t>(n, 256);
+    cudaError_t e = cudaMalloc(&p, want);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return e;
+    }
+    bytes = want;
+    if (grew) *grew = true;
+    return cudaSuccess;
+  }
+  template <typename T>
+  T* as() const {
+    return reinterpret_cast<T*>(p);
+  }
+};
+
+enum Stage { kStRecords = 0, kStProject, kStTetSort, kStEmit, kStPairSort, kStRanges, kStComposite, kStAdam };
+
+struct EventPair {
+  int stage;
+  cudaEvent_t a, b;
+};
+
+}  // namespace
+
+struct RmeshCtx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int64_t N = 0, M = 0;
+  int width = 0, height = 0, tile_size = 12;
+  float min_t = 0.0f;
+  uint32_t step = 0;
+  std::string err;
+  int num_sms = 148;
+
+  // parameters + optimizer state
+  DevBuf verts, idx, dens, cgrad, base, circ;
+  DevBuf m_verts, v_verts, m_dens, v_dens, m_cgrad, v_cgrad, m_base, v_base;
+  DevBuf rec, color4, grad_slot, csr_off, csr_ref;
+
+  // per-run
+  DevBuf views_d, counters_d, hp_d, sort_state, sort_status, scan_status;
+  DevBuf vis_key, vis_val, vis_tet, vis_cnt, vis_proj, vis_key_alt, vis_val_alt, tiles_touched;
+  DevBuf pair_key, pair_val, pair_key_alt, pair_val_alt, ranges;
+  DevBuf rgba, aux, dl, gt, out_a, out_b, out_c, out_d;
+  uint64_t cap_pairs = 0;
+  uint64_t generation = 0;  // bumped whenever a buffer is reallocated
+
+  // pinned host staging
+  ViewParams* views_h = nullptr;
+  Counters* counters_h = nullptr;
+  AdamParams* hp_h = nullptr;
+
+  // results of the last run
+  uint32_t* sorted_pair_key = nullptr;
+  uint32_t* sorted_pair_val = nullptr;
+  bool have_forward = false;
+  uint32_t last_tiles = 0;
+  int last_views = 0;
+  uint32_t last_err_bits = 0;
+  uint64_t last_n_vis = 0, last_n_pairs = 0;
+  int last_cnt = 1;  // Counters blocks written by the last training run
+
+  // CUDA graph of the batched train step
+  cudaGraphExec_t graph = nullptr;
+  std::vector<int64_t> graph_sig;
+  int graph_kernels = 0;  // kernels per replay (counted at capture)
+
+  // profiling
+  bool profiling = false;
+  std::vector<EventPair> events;
+  std::vector<cudaEvent_t> event_pool;
+  float stage_ms[RMESH_N_STAGES] = {0};
+  int stage_launches[RMESH_N_STAGES] = {0};
+  int kernel_launches = 0;
+};
+
+namespace {
+
+int fail(RmeshCtx* c, int code, const std::string& msg) {
+  if (c) c->err = msg;
+  return code;
+}
+
+#define CK(call)                                                                                  \
+  do {                                                                                            \
+    cudaError_t e__ = (call);                                                                     \
+    if (e__ != cudaSuccess)                                                                       \
+      return fail(c, e__ == cudaErrorMemoryAllocation ? RMESH_ERR_OOM : RMESH_ERR_CUDA,           \
+                  std::string(#call) + ": " + cudaGetErrorString(e__));                           \
+  } while (0)
+
+#define CKL()                                                                                     \
+  do {                                                                                            \
+    cudaError_t e__ = cudaGetLastError();                                                         \
+    if (e__ != cudaSuccess) return fail(c, RMESH_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e__)); \
+    c->kernel_launches++;                                                                         \
+  } while (0)
+
+cudaEvent_t take_event(RmeshCtx* c) {
+  if (!c->event_pool.empty()) {
+    cudaEvent_t e = c->event_pool.back();
+    c->event_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  return e;
+}
+
+struct StageScope {
+  RmeshCtx* c;
+  int stage;
+  cudaEvent_t a = nullptr;
+  StageScope(RmeshCtx* c_, int s, bool capturing) : c(c_), stage(s) {
+    if (c->profiling && !capturing) {
+      a = take_event(c);
+      cudaEventRecord(a, c->stream);
+    }
+  }
+  ~StageScope() {
+    if (a) {
+      cudaEvent_t b = take_event(c);
+      cudaEventRecord(b, c->stream);
+      c->events.push_back({stage, a, b});
+    }
+  }
+};
+
+bool is_device_ptr(const void* p) {
+  if (!p) return false;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+int bitlen(uint64_t x) {  // number of bits to represent x (x >= 1 -> >= 1)
+  int b = 0;
+  while (x) {
+    ++b;
+    x >>= 1;
+  }
+  return b;
+}
+
+int ensure_buf(RmeshCtx* c, DevBuf& b, size_t bytes) {
+  bool grew = false;
+  cudaError_t e = b.ensure(bytes, &grew);
+  if (e != cudaSuccess) return fail(c, RMESH_ERR_OOM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  if (grew) c->generation++;
+  return RMESH_OK;
+}
+
+#define CKR(expr)              \
+  do {                         \
+    int r__ = (expr);          \
+    if (r__ != RMESH_OK) return r__; \
+  } while (0)
+
+// ---------------------------------------------------------------- sorting
+template <typename K>
+int radix_sort(RmeshCtx* c, K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt, const void* n_ptr, int n_is_u64,
+               uint64_t cap, int bits, K** out_keys, uint32_t** out_vals, bool capturing) {
+  const int passes = std::max(1, (bits + 7) / 8);
+  SortState* st = c->sort_state.as<SortState>();
+  Counters* cnt = c->counters_d.as<Counters>();
+  CK(cudaMemsetAsync(st->hist, 0, sizeof(st->hist), c->stream));
+  const int hist_blocks = (int)std::min<uint64_t>((cap + 255) / 256, (uint64_t)c->num_sms * 8);
+  sort_hist_kernel<K><<<std::max(1, hist_blocks), 256, 0, c->stream>>>(keys, n_ptr, n_is_u64, cap, 0, passes, st);
+  CKL();
+  sort_scan_kernel<<<1, 256, 0, c->stream>>>(passes, st);
+  CKL();
+  const size_t smem = sizeof(K) * kSortPart + sizeof(uint32_t) * kSortPart + sizeof(uint32_t) * (kSortWarps * 256 + 512);
+  const unsigned grid = (unsigned)std::max<uint64_t>(1, (cap + kSortPart - 1) / kSortPart);
+  K* kin = keys;
+  uint32_t* vin = vals;
+  K* kout = keys_alt;
+  uint32_t* vout = vals_alt;
+  for (int p = 0; p < passes; ++p) {
+    onesweep_kernel<K><<<grid, kSortThreads, smem, c->stream>>>(kin, vin, kout, vout, n_ptr, n_is_u64, cap, 8 * p, p,
+                                                                st, c->sort_status.as<unsigned long long>(),
+                                                                &cnt->err);
+    CKL();
+    std::swap(kin, kout);
+    std::swap(vin, vout);
+  }
+  (void)capturing;
+  *out_keys = kin;
+  *out_vals = vin;
+  return RMESH_OK;
+}
+
+int setup_sort_attrs() {
+  static bool done = false;
+  if (done) return 0;
+  const int s64 = (int)(sizeof(uint64_t) * kSortPart + sizeof(uint32_t) * kSortPart + sizeof(uint32_t) * (kSortWarps * 256 + 512));
+  const int s32 = (int)(sizeof(uint32_t) * kSortPart + sizeof(uint32_t) * kSortPart + sizeof(uint32_t) * (kSortWarps * 256 + 512));
+  if (cudaFuncSetAttribute(onesweep_kernel<unsigned long long>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64) != cudaSuccess) return 1;
+  if (cudaFuncSetAttribute(onesweep_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32) != cudaSuccess) return 1;
+  done = true;
+  return 0;
+}
+
+// ---------------------------------------------------------------- buffers
+int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t total_tiles) {
+  const uint64_t items = (uint64_t)n_views * (uint64_t)c->M;
+  CKR(ensure_buf(c, c->vis_key, items * 8));
+  CKR(ensure_buf(c, c->vis_key_alt, items * 8));
+  CKR(ensure_buf(c, c->vis_val, items * 4));
+  CKR(ensure_buf(c, c->vis_val_alt, items * 4));
+  CKR(ensure_buf(c, c->vis_tet, items * 4));
+  CKR(ensure_buf(c, c->vis_cnt, items * 4));
+  CKR(ensure_buf(c, c->vis_proj, items * 32));
+  CKR(ensure_buf(c, c->tiles_touched, items * 4));
+  if (c->cap_pairs == 0) c->cap_pairs = std::max<uint64_t>(8 * items, 1u << 16);
+  CKR(ensure_buf(c, c->pair_key, c->cap_pairs * 4));
+  CKR(ensure_buf(c, c->pair_val, c->cap_pairs * 4));
+  CKR(ensure_buf(c, c->pair_key_alt, c->cap_pairs * 4));
+  CKR(ensure_buf(c, c->pair_val_alt, c->cap_pairs * 4));
+  const uint64_t sort_items = std::max<uint64_t>(std::max<uint64_t>(items, c->cap_pairs), 4ull * c->M);
+  CKR(ensure_buf(c, c->sort_status, ((sort_items + kSortPart - 1) / kSortPart + 1) * 256 * 8));
+  CKR(ensure_buf(c, c->scan_status, ((items + 255) / 256 + 2) * 8));
+  CKR(ensure_buf(c, c->ranges, (uint64_t)std::max<uint32_t>(total_tiles, 1) * 8));
+  CKR(ensure_buf(c, c->rgba, std::max<uint64_t>(total_pixels, 1) * 16));
+  return RMESH_OK;
+}
+
+// views_h[0..n) must be filled; uploads them
+int upload_views(RmeshCtx* c, int n) {
+  CK(cudaMemcpyAsync(c->views_d.p, c->views_h, sizeof(ViewParams) * n, cudaMemcpyHostToDevice, c->stream));
+  return RMESH_OK;
+}
+
+int fill_view(RmeshCtx* c, const RmeshCamera& cam, ViewParams& v, uint32_t tile_base, uint32_t pix_base) {
+  if (cam.width <= 0 || cam.height <= 0 || cam.width > 65536 || cam.height > 65536)
+    return fail(c, RMESH_ERR_INVALID_ARG, "camera width/height out of range");
+  memset(&v, 0, sizeof(v));
+  memcpy(v.vp, cam.vp, sizeof(v.vp));
+  const float* ci = cam.c2w_intrinsics;
+  for (int k = 0; k < 3; ++k) {
+    v.c2w[k] = ci[k];
+    v.c2w[3 + k] = ci[4 + k];
+    v.c2w[6 + k] = ci[8 + k];
+  }
+  v.fx = ci[12];
+  v.fy = ci[13];
+  v.cx = ci[14];
+  v.cy = ci[15];
+  v.cam[0] = cam.cam_pos[0];
+  v.cam[1] = cam.cam_pos[1];
+  v.cam[2] = cam.cam_pos[2];
+  v.min_t = c->min_t;
+  v.W = cam.width;
+  v.H = cam.height;
+  v.Wf = (float)cam.width;
+  v.Hf = (float)cam.height;
+  v.n_pixels = (float)((uint32_t)cam.width * (uint32_t)cam.height);
+  v.TS = c->tile_size;
+  v.tiles_x = (cam.width + c->tile_size - 1) / c->tile_size;
+  v.tiles_y = (cam.height + c->tile_size - 1) / c->tile_size;
+  v.tile_base = tile_base;
+  v.pix_base = pix_base;
+  return RMESH_OK;
+}
+
+// ---------------------------------------------------------------- stages
+int run_records(RmeshCtx* c, bool capturing) {
+  StageScope sc(c, kStRecords, capturing);
+  const int M = (int)c->M;
+  build_records_kernel<<<(M + 255) / 256, 256, 0, c->stream>>>(M, c->verts.as<float>(), c->idx.as<uint4>(),
+                                                               c->dens.as<float>(), c->cgrad.as<float>(),
+                                                               c->base.as<float>(), c->rec.as<TetRec>(),
+                                                               c->color4.as<float4>());
+  CKL();
+  return RMESH_OK;
+}
+
+// project -> tet sort -> emit -> pair sort -> ranges for n_views views at views_dev
+int run_bin(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t total_tiles, Counters* cnt,
+            bool capturing) {
+  const uint64_t items = (uint64_t)n_views * (uint64_t)c->M;
+  const unsigned nblk = (unsigned)((items + 255) / 256);
+  unsigned long long* status = c->scan_status.as<unsigned long long>();
+  uint32_t* ticket = reinterpret_cast<uint32_t*>(status + nblk + 1);
+  {
+    StageScope sc(c, kStProject, capturing);
+    CK(cudaMemsetAsync(status, 0, (size_t)(nblk + 2) * 8, c->stream));
+    ProjectArgs pa;
+    pa.M = (int)c->M;
+    pa.n_views = n_views;
+    pa.views = views_dev;
+    pa.rec = c->rec.as<TetRec>();
+    pa.circ = c->circ.as<float4>();
+    pa.vis_key = c->vis_key.as<unsigned long long>();
+    pa.vis_val = c->vis_val.as<uint32_t>();
+    pa.vis_tet = c->vis_tet.as<uint32_t>();
+    pa.vis_cnt = c->vis_cnt.as<uint32_t>();
+    pa.vis_proj = c->vis_proj.as<float4>();
+    pa.tiles_touched = c->tiles_touched.as<uint32_t>();
+    pa.status = status;
+    pa.ticket = ticket;
+    pa.counters = cnt;
+    project_kernel<<<nblk, 256, 0, c->stream>>>(pa);
+    CKL();
+  }
+  unsigned long long* tk = nullptr;
+  uint32_t* tv = nullptr;
+  {
+    StageScope sc(c, kStTetSort, capturing);
+    const int view_bits = n_views <= 1 ? 0 : bitlen((uint64_t)(n_views - 1));
+    CKR(radix_sort<unsigned long long>(c, c->vis_key.as<unsigned long long>(), c->vis_val.as<uint32_t>(),
+                                       c->vis_key_alt.as<unsigned long long>(), c->vis_val_alt.as<uint32_t>(),
+                                       &cnt->n_vis, 0, items, 32 + view_bits, &tk, &tv, capturing));
+  }
+  {
+    StageScope sc(c, kStEmit, capturing);
+    CK(cudaMemsetAsync(status, 0, (size_t)(nblk + 2) * 8, c->stream));
+    EmitArgs ea;
+    ea.views = views_dev;
+    ea.tet_key_sorted = tk;
+    ea.tet_val_sorted = tv;
+    ea.vis_tet = c->vis_tet.as<uint32_t>();
+    ea.vis_cnt = c->vis_cnt.as<uint32_t>();
+    ea.vis_proj = c->vis_proj.as<float4>();
+    ea.n_vis_ptr = &cnt->n_vis;
+    ea.pair_key = c->pair_key.as<uint32_t>();
+    ea.pair_val = c->pair_val.as<uint32_t>();
+    ea.cap = c->cap_pairs;
+    ea.status = status;
+    ea.ticket = ticket;
+    ea.counters = cnt;
+    emit_kernel<<<nblk, 256, 0, c->stream>>>(ea);
+    CKL();
+  }
+  {
+    StageScope sc(c, kStPairSort, capturing);
+    const int bits = std::max(1, bitlen(total_tiles));
+    CKR(radix_sort<uint32_t>(c, c->pair_key.as<uint32_t>(), c->pair_val.as<uint32_t>(), c->pair_key_alt.as<uint32_t>(),
+                             c->pair_val_alt.as<uint32_t>(), &cnt->n_pairs, 1, c->cap_pairs, bits,
+                             &c->sorted_pair_key, &c->sorted_pair_val, capturing));
+  }
+  {
+    StageScope sc(c, kStRanges, capturing);
+    CK(cudaMemsetAsync(c->ranges.p, 0, (size_t)total_tiles * 8, c->stream));
+    const int blocks = (int)std::min<uint64_t>((c->cap_pairs + 255) / 256, (uint64_t)c->num_sms * 16);
+    ranges_kernel<<<std::max(1, blocks), 256, 0, c->stream>>>(c->sorted_pair_key, &cnt->n_pairs, c->cap_pairs,
+                                                               c->ranges.as<uint2>(), views_dev, n_views, cnt);
+    CKL();
+  }
+  return RMESH_OK;
+}
+
+template <int TS, int MODE, bool AUX>
+int launch_tile_t(RmeshCtx* c, TileArgs& ta, uint32_t n_tiles, bool persistent) {
+  constexpr int NT = ((TS * TS + 31) / 32) * 32;
+  unsigned grid = n_tiles;
+  if (persistent) {
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tile_kernel<TS, MODE, AUX>, NT, 0);
+    grid = (unsigned)std::max(1, occ) * (unsigned)c->num_sms;
+    grid = std::min<unsigned>(grid, std::max<uint32_t>(n_tiles, 1));
+  }
+  ta.persistent = persistent ? 1 : 0;
+  if (grid == 0) return RMESH_OK;
+  tile_kernel<TS, MODE, AUX><<<grid, NT, 0, c->stream>>>(ta);
+  CKL();
+  return RMESH_OK;
+}
+
+template <int MODE, bool AUX>
+int launch_tile_m(RmeshCtx* c, TileArgs& ta, uint32_t n_tiles, bool persistent) {
+  switch (c->tile_size) {
+    case 8: return launch_tile_t<8, MODE, AUX>(c, ta, n_tiles, persistent);
+    case 12: return launch_tile_t<12, MODE, AUX>(c, ta, n_tiles, persistent);
+    case 16: return launch_tile_t<16, MODE, AUX>(c, ta, n_tiles, persistent);
+    default: return fail(c, RMESH_ERR_INVALID_ARG, "tile size must be 8, 12 or 16");
+  }
+}
+
+TileArgs base_tile_args(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t n_tiles, Counters* cnt) {
+  TileArgs ta;
+  memset(&ta, 0, sizeof(ta));
+  ta.views = views_dev;
+  ta.n_views = n_views;
+  ta.n_tiles = n_tiles;
+  ta.ranges = c->ranges.as<uint2>();
+  ta.pair_val = c->sorted_pair_val;
+  ta.rec = c->rec.as<TetRec>();
+  ta.color4 = c->color4.as<float4>();
+  ta.color_view_stride = 0;
+  ta.grad_slot = c->grad_slot.as<float>();
+  ta.counters = cnt;
+  ta.hp = c->hp_d.as<AdamParams>();
+  return ta;
+}
+
+int sync_counters(RmeshCtx* c, int n) {
+  CK(cudaMemcpyAsync(c->counters_h, c->counters_d.p, sizeof(Counters) * n, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  uint32_t bits = 0;
+  uint64_t nv = 0, np = 0;
+  for (int i = 0; i < n; ++i) {
+    bits |= c->counters_h[i].err;
+    nv += c->counters_h[i].n_vis;
+    np = std::max<uint64_t>(np, c->counters_h[i].n_pairs);
+  }
+  c->last_err_bits = bits;
+  c->last_n_vis = nv;
+  c->last_n_pairs = np;
+  return RMESH_OK;
+}
+
+// grows pair capacity after an overflow; returns true when a retry makes sense
+bool grow_pairs(RmeshCtx* c) {
+  const uint64_t need = c->last_n_pairs + c->last_n_pairs / 4 + 4096;
+  const uint64_t limit = (1ull << 31) - 1;
+  if (need <= c->cap_pairs || c->cap_pairs >= limit) return false;
+  c->cap_pairs = std::min(need, limit);
+  return true;
+}
+
+int status_from_bits(RmeshCtx* c) {
+  if (c->last_err_bits & kErrSpinTimeout) return fail(c, RMESH_ERR_TIMEOUT, "device spin wait gave up");
+  if (c->last_err_bits & kErrPairOverflow) return fail(c, RMESH_ERR_PAIR_OVERFLOW, "pair buffer overflow");
+  return RMESH_OK;
+}
+
+int copy_in(RmeshCtx* c, DevBuf& dst, const void* src, size_t bytes) {
+  if (!src || !bytes) return RMESH_OK;
+  CK(cudaMemcpyAsync(dst.p, src, bytes, cudaMemcpyDefault, c->stream));
+  return RMESH_OK;
+}
+
+// ---------------------------------------------------------------- train
+int launch_adam(RmeshCtx* c, int n_cnt, bool capturing) {
+  StageScope sc(c, kStAdam, capturing);
+  AdamArgs aa;
+  aa.N = (int)c->N;
+  aa.M = (int)c->M;
+  aa.verts = c->verts.as<float>();
+  aa.dens = c->dens.as<float>();
+  aa.cgrad = c->cgrad.as<float>();
+  aa.base = c->base.as<float>();
+  aa.m_verts = c->m_verts.as<float>();
+  aa.v_verts = c->v_verts.as<float>();
+  aa.m_dens = c->m_dens.as<float>();
+  aa.v_dens = c->v_dens.as<float>();
+  aa.m_cgrad = c->m_cgrad.as<float>();
+  aa.v_cgrad = c->v_cgrad.as<float>();
+  aa.m_base = c->m_base.as<float>();
+  aa.v_base = c->v_base.as<float>();
+  aa.grad_slot = c->grad_slot.as<float>();
+  aa.csr_off = c->csr_off.as<uint32_t>();
+  aa.csr_ref = c->csr_ref.as<uint32_t>();
+  aa.hp = c->hp_d.as<AdamParams>();
+  aa.counters = c->counters_d.as<Counters>();
+  aa.n_counters = n_cnt;
+  const int blocks = (int)std::min<int64_t>((c->N + c->M + 255) / 256, (int64_t)c->num_sms * 16);
+  adam_kernel<<<std::max(1, blocks), 256, 0, c->stream>>>(aa);
+  CKL();
+  return RMESH_OK;
+}
+
+// Forward + loss + adjoint over n_views cameras, gradients summed into the
+// per-tet slots; then (do_adam) one multi-group Adam launch.
+int train_views(RmeshCtx* c, const RmeshCamera* cams, int n_views, const float* gt, const RmeshTrainOpts* o,
+                float* loss_out, bool do_adam = true) {
+  if (n_views <= 0 || n_views > kMaxViews) return fail(c, RMESH_ERR_INVALID_ARG, "n_views out of range");
+  if (!cams || !gt || !o) return fail(c, RMESH_ERR_INVALID_ARG, "null argument");
+  if (o->loss_type != 0 && o->loss_type != 1) return fail(c, RMESH_ERR_INVALID_ARG, "loss_type must be 0 or 1");
+  const int mode = o->mode;
+  const bool plain = mode == RMESH_MODE_PLAIN;
+  // view table: batched numbering (tiles and pixels back to back)
+  uint64_t total_pix = 0;
+  uint32_t total_tiles = 0, max_tiles = 0;
+  std::vector<uint32_t> view_tiles(n_views);
+  for (int v = 0; v < n_views; ++v) {
+    CKR(fill_view(c, cams[v], c->views_h[v], plain ? 0u : total_tiles, (uint32_t)total_pix));
+    view_tiles[v] = (uint32_t)(c->views_h[v].tiles_x * c->views_h[v].tiles_y);
+    total_tiles += view_tiles[v];
+    max_tiles = std::max(max_tiles, view_tiles[v]);
+    total_pix += (uint64_t)cams[v].width * cams[v].height;
+  }
+  const int run_views = plain ? 1 : n_views;
+  const bool direct_gt = is_device_ptr(gt);
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    CKR(ensure_run_buffers(c, run_views, total_pix, plain ? max_tiles : total_tiles));
+    if (!direct_gt) CKR(ensure_buf(c, c->gt, total_pix * 12));
+    AdamParams& hp = *c->hp_h;
+    hp.step = c->step + 1;
+    hp.lr_verts = o->lr_verts;
+    hp.lr_dens = o->lr_dens;
+    hp.lr_grads = o->lr_grads;
+    hp.lr_base = o->lr_base;
+    hp.lr_sh = 0.0f;
+    hp.beta1 = 0.9f;
+    hp.beta2 = 0.999f;
+    hp.eps = 1e-8f;
+    hp.loss_type = o->loss_type;
+    CK(cudaMemcpyAsync(c->hp_d.p, c->hp_h, sizeof(AdamParams), cudaMemcpyHostToDevice, c->stream));
+    CKR(upload_views(c, n_views));
+    const float* gt_dev = direct_gt ? gt : c->gt.as<float>();
+    if (!direct_gt) CK(cudaMemcpyAsync(c->gt.p, gt, total_pix * 12, cudaMemcpyHostToDevice, c->stream));
+
+    const int n_cnt = plain ? n_views : 1;
+    auto enqueue = [&](bool capturing) -> int {
+      Counters* cnt = c->counters_d.as<Counters>();
+      CK(cudaMemsetAsync(cnt, 0, sizeof(Counters) * n_cnt, c->stream));
+      CK(cudaMemsetAsync(c->grad_slot.p, 0, (size_t)c->M * kGradSlot * 4, c->stream));
+      CKR(run_records(c, capturing));
+      ViewParams* vd = c->views_d.as<ViewParams>();
+      if (plain) {
+        for (int v = 0; v < n_views; ++v) {
+          CKR(run_bin(c, vd + v, 1, view_tiles[v], cnt + v, capturing));
+          StageScope sc(c, kStComposite, capturing);
+          TileArgs ta = base_tile_args(c, vd + v, 1, view_tiles[v], cnt + v);
+          ta.gt_rgb = gt_dev;
+          CKR((launch_tile_m<kModeTrain, false>(c, ta, view_tiles[v], false)));
+        }
+      } else {
+        CKR(run_bin(c, vd, n_views, total_tiles, cnt, capturing));
+        StageScope sc(c, kStComposite, capturing);
+        TileArgs ta = base_tile_args(c, vd, n_views, total_tiles, cnt);
+        ta.gt_rgb = gt_dev;
+        CKR((launch_tile_m<kModeTrain, false>(c, ta, total_tiles, true)));
+      }
+      if (do_adam) CKR(launch_adam(c, n_cnt, capturing));
+      return RMESH_OK;
+    };
+
+    if (mode == RMESH_MODE_GRAPH) {
+      std::vector<int64_t> sig = {n_views, c->tile_size, (int64_t)c->cap_pairs, (int64_t)c->generation,
+                                  (int64_t)(uintptr_t)gt_dev, o->loss_type, do_adam ? 1 : 0};
+      for (int v = 0; v < n_views; ++v) {
+        sig.push_back(cams[v].width);
+        sig.push_back(cams[v].height);
+      }
+      if (!c->graph || sig != c->graph_sig) {
+        if (c->graph) {
+          cudaGraphExecDestroy(c->graph);
+          c->graph = nullptr;
+        }
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        const int before = c->kernel_launches;
+        int r = enqueue(true);
+        c->graph_kernels = c->kernel_launches - before;
+        c->kernel_launches = before;
+        cudaError_t e = cudaStreamEndCapture(c->stream, &g);
+        if (r != RMESH_OK) return r;
+        if (e != cudaSuccess) return fail(c, RMESH_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&c->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return fail(c, RMESH_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        c->graph_sig = sig;
+      }
+      {
+        StageScope sc(c, kStComposite, false);  // whole graph accounted as one span
+        CK(cudaGraphLaunch(c->graph, c->stream));
+        c->kernel_launches += c->graph_kernels;
+      }
+    } else {
+      CKR(enqueue(false));
+    }
+    CKR(sync_counters(c, n_cnt));
+    if ((c->last_err_bits & kErrPairOverflow) && grow_pairs(c)) continue;
+    CKR(status_from_bits(c));
+    if (do_adam) c->step += 1;
+    c->have_forward = false;
+    c->last_cnt = n_cnt;
+    if (loss_out) {
+      for (int v = 0; v < n_views; ++v) {
+        const double l = plain ? c->counters_h[v].loss[0] : c->counters_h[0].loss[v];
+        loss_out[v] = (float)(l / (double)((uint64_t)cams[v].width * cams[v].height));
+      }
+    }
+    c->last_views = n_views;
+    return RMESH_OK;
+  }
+  return fail(c, RMESH_ERR_PAIR_OVERFLOW, "pair buffers could not be grown enough");
+}
+
+int build_csr(RmeshCtx* c) {
+  const uint64_t n_refs = 4ull * (uint64_t)c->M;
+  CKR(ensure_buf(c, c->csr_off, (c->N + 1) * 4));
+  CKR(ensure_buf(c, c->csr_ref, n_refs * 4));
+  DevBuf k0, k1, v1, nbuf;
+  CKR(ensure_buf(c, k0, n_refs * 4));
+  CKR(ensure_buf(c, k1, n_refs * 4));
+  CKR(ensure_buf(c, v1, n_refs * 4));
+  CKR(ensure_buf(c, nbuf, 8));
+  const uint32_t n32 = (uint32_t)n_refs;
+  CK(cudaMemcpyAsync(nbuf.p, &n32, 4, cudaMemcpyHostToDevice, c->stream));
+  csr_fill_kernel<<<(unsigned)((n_refs + 255) / 256), 256, 0, c->stream>>>((int)c->M, c->idx.as<uint32_t>(),
+                                                                          k0.as<uint32_t>(), c->csr_ref.as<uint32_t>());
+  CKL();
+  CKR(ensure_buf(c, c->sort_status, ((n_refs + kSortPart - 1) / kSortPart + 1) * 256 * 8));
+  CK(cudaMemsetAsync(c->counters_d.p, 0, sizeof(Counters), c->stream));
+  uint32_t* ok_keys = nullptr;
+  uint32_t* ok_vals = nullptr;
+  CKR(radix_sort<uint32_t>(c, k0.as<uint32_t>(), c->csr_ref.as<uint32_t>(), k1.as<uint32_t>(), v1.as<uint32_t>(),
+                           nbuf.p, 0, n_refs, std::max(1, bitlen((uint64_t)std::max<int64_t>(c->N - 1, 1))), &ok_keys,
+                           &ok_vals, false));
+  if (ok_vals != c->csr_ref.as<uint32_t>())
+    CK(cudaMemcpyAsync(c->csr_ref.p, ok_vals, n_refs * 4, cudaMemcpyDeviceToDevice, c->stream));
+  csr_offsets_kernel<<<(unsigned)((n_refs + 1 + 255) / 256), 256, 0, c->stream>>>((int)n_refs, (int)c->N, ok_keys,
+                                                                                  c->csr_off.as<uint32_t>());
+  CKL();
+  CK(cudaStreamSynchronize(c->stream));
+  Counters h;
+  CK(cudaMemcpy(&h, c->counters_d.p, sizeof(Counters), cudaMemcpyDeviceToHost));
+  if (h.err) return fail(c, RMESH_ERR_TIMEOUT, "vertex map sort failed");
+  return RMESH_OK;
+}
+
+}  // namespace
+
+// ===================================================================== C ABI
+extern "C" {
+
+int rmesh_abi_version(void) { return RMESH_ABI_VERSION; }
+
+const char* rmesh_last_error(const RmeshCtx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+int rmesh_create(const RmeshSceneDesc* d, RmeshCtx** out) {
+  RmeshCtx* c = nullptr;
+  if (!d || !out) return RMESH_ERR_INVALID_ARG;
+  *out = nullptr;
+  if (d->n_vertices <= 0 || d->n_tets <= 0 || !d->vertices || !d->indices || !d->base_colors || !d->densities ||
+      !d->color_grads || !d->circumdata)
+    return RMESH_ERR_INVALID_ARG;
+  if (d->n_tets > (int64_t)(1u << 29) || d->n_vertices > (int64_t)(1u << 30)) return RMESH_ERR_INVALID_ARG;
+  if (d->aux_dim != 0) return RMESH_ERR_INVALID_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return RMESH_ERR_NO_DEVICE;
+  }
+  c = new RmeshCtx();
+  c->N = d->n_vertices;
+  c->M = d->n_tets;
+  c->width = d->width;
+  c->height = d->height;
+  c->tile_size = d->tile_size > 0 ? d->tile_size : 12;
+  if (c->tile_size != 8 && c->tile_size != 12 && c->tile_size != 16) {
+    delete c;
+    return RMESH_ERR_INVALID_ARG;
+  }
+  if (d->device >= 0) {
+    if (cudaSetDevice(d->device) != cudaSuccess) {
+      delete c;
+      return RMESH_ERR_NO_DEVICE;
+    }
+  }
+  cudaGetDevice(&c->device);
+  cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, c->device);
+  if (setup_sort_attrs() != 0) {
+    delete c;
+    return RMESH_ERR_NO_DEVICE;
+  }
+  int r = RMESH_OK;
+  auto init = [&]() -> int {
+    CK(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    c->own_stream = true;
+    CK(cudaMallocHost(&c->views_h, sizeof(ViewParams) * kMaxViews));
+    CK(cudaMallocHost(&c->counters_h, sizeof(Counters) * kMaxViews));
+    CK(cudaMallocHost(&c->hp_h, sizeof(AdamParams)));
+    const size_t N = (size_t)c->N, M = (size_t)c->M;
+    CKR(ensure_buf(c, c->verts, 3 * N * 4));
+    CKR(ensure_buf(c, c->idx, 4 * M * 4));
+    CKR(ensure_buf(c, c->dens, M * 4));
+    CKR(ensure_buf(c, c->cgrad, 3 * M * 4));
+    CKR(ensure_buf(c, c->base, 3 * M * 4));
+    CKR(ensure_buf(c, c->circ, 4 * M * 4));
+    DevBuf* zeros[] = {&c->m_verts, &c->v_verts, &c->m_dens, &c->v_dens, &c->m_cgrad, &c->v_cgrad, &c->m_base, &c->v_base};
+    size_t zsz[] = {3 * N, 3 * N, M, M, 3 * M, 3 * M, 3 * M, 3 * M};
+    for (int i = 0; i < 8; ++i) {
+      CKR(ensure_buf(c, *zeros[i], zsz[i] * 4));
+      CK(cudaMemsetAsync(zeros[i]->p, 0, zsz[i] * 4, c->stream));
+    }
+    CKR(ensure_buf(c, c->rec, M * sizeof(TetRec)));
+    CKR(ensure_buf(c, c->color4, M * 16));
+    CKR(ensure_buf(c, c->grad_slot, M * kGradSlot * 4));
+    CKR(ensure_buf(c, c->views_d, sizeof(ViewParams) * kMaxViews));
+    CKR(ensure_buf(c, c->counters_d, sizeof(Counters) * kMaxViews));
+    CKR(ensure_buf(c, c->hp_d, sizeof(AdamParams)));
+    CKR(ensure_buf(c, c->sort_state, sizeof(SortState)));
+    CK(cudaMemsetAsync(c->sort_state.p, 0, sizeof(SortState), c->stream));
+    CKR(copy_in(c, c->verts, d->vertices, 3 * N * 4));
+    CKR(copy_in(c, c->idx, d->indices, 4 * M * 4));
+    CKR(copy_in(c, c->dens, d->densities, M * 4));
+    CKR(copy_in(c, c->cgrad, d->color_grads, 3 * M * 4));
+    CKR(copy_in(c, c->base, d->base_colors, 3 * M * 4));
+    CKR(copy_in(c, c->circ, d->circumdata, 4 * M * 4));
+    CKR(build_csr(c));
+    return RMESH_OK;
+  };
+  r = init();
+  if (r != RMESH_OK) {
+    rmesh_destroy(c);
+    return r;
+  }
+  *out = c;
+  return RMESH_OK;
+}
+
+int rmesh_destroy(RmeshCtx* c) {
+  if (!c) return RMESH_OK;
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->graph) cudaGraphExecDestroy(c->graph);
+  for (auto& e : c->events) {
+    cudaEventDestroy(e.a);
+    cudaEventDestroy(e.b);
+  }
+  for (auto e : c->event_pool) cudaEventDestroy(e);
+  if (c->views_h) cudaFreeHost(c->views_h);
+  if (c->counters_h) cudaFreeHost(c->counters_h);
+  if (c->hp_h) cudaFreeHost(c->hp_h);
+  if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+  return RMESH_OK;
+}
+
+int rmesh_set_stream(RmeshCtx* c, void* s) {
+  if (!c) return RMESH_ERR_INVALID_ARG;
+  CK(cudaStreamSynchronize(c->stream));
+  if (c->own_stream) cudaStreamDestroy(c->stream);
+  c->own_stream = false;
+  c->stream = (cudaStream_t)s;
+  if (c->graph) {
+    cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+  }
+  return RMESH_OK;
+}
+
+int rmesh_set_min_t(RmeshCtx* c, float t) {
+  if (!c) return RMESH_ERR_INVALID_ARG;
+  c->min_t = t;
+  return RMESH_OK;
+}
+
+int rmesh_set_tile_size(RmeshCtx* c, int32_t ts) {
+  if (!c) return RMESH_ERR_INVALID_ARG;
+  if (ts != 8 && ts != 12 && ts != 16) return fail(c, RMESH_ERR_INVALID_ARG, "tile size must be 8, 12 or 16");
+  c->tile_size = ts;
+  c->have_forward = false;
+  return RMESH_OK;
+}
+
+int rmesh_update_params(RmeshCtx* c, const float* v, const float* b, const float* d, const float* g) {
+  if (!c) return RMESH_ERR_INVALID_ARG;
+  CKR(copy_in(c, c->verts, v, 3 * (size_t)c->N * 4));
+  CKR(copy_in(c, c->base, b, 3 * (size_t)c->M * 4));
+  CKR(copy_in(c, c->dens, d, (size_t)c->M * 4));
+  CKR(copy_in(c, c->cgrad, g, 3 * (size_t)c->M * 4));
+  return RMESH_OK;
+}
+
+int rmesh_get_params(RmeshCtx* c, float* v, float* b, float* d, float* g) {
+  if (!c) return RMESH_ERR_INVALID_ARG;
+  if (v) CK(cudaMemcpyAsync(v, c->verts.p, 3 * (size_t)c->N * 4, cudaMemcpyDefault, c->stream));
+  if (b) CK(cudaMemcpyAsync(b, c->base.p, 3 * (size_t)c->M * 4, cudaMemcpyDefault, c->stream));
+  if (d) CK(cudaMemcpyAsync(d, c->dens.p, (size_t)c->M * 4, cudaMemcpyDefault, c->stream));
+  if (g) CK(cudaMemcpyAsync(g, c->cgrad.p, 3 * (size_t)c->M * 4, cudaMemcpyDefault, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return RMESH_OK;
+}
+
+int rmesh_get_info(RmeshCtx* c, RmeshInfo* info) {
+  if (!c || !info) return RMESH_ERR_INVALID_ARG;
+  memset(info, 0, sizeof(*info));
+  info->n_vertices = c->N;
+  info->n_tets = c->M;
+  info->width = c->width;
+  info->height = c->height;
+  info->tile_size = c->tile_size;
+  info->n_views_last = c->last_views;
+  info->step = c->step;
+  info->last_error_bits = c->last_err_bits;
+  info->n_visible_last = c->last_n_vis;
+  info->n_pairs_last = c->last_n_pairs;
+  info->pair_capacity = c->cap_pairs;
+  DevBuf* all[] = {&c->verts, &c->idx, &c->dens, &c->cgrad, &c->base, &c->circ, &c->m_verts, &c->v_verts,
+                   &c->m_dens, &c->v_dens, &c->m_cgrad, &c->v_cgrad, &c->m_base, &c->v_base, &c->rec,
+                   &c->color4, &c->grad_slot, &c->csr_off, &c->csr_ref, &c->views_d, &c->counters_d, &c->hp_d,
+                   &c->sort_state, &c->sort_status, &c->scan_status, &c->vis_key, &c->vis_val, &c->vis_tet,
+                   &c->vis_cnt, &c->vis_proj, &c->vis_key_alt, &c->vis_val_alt, &c->tiles_touched, &c->pair_key,
+                   &c->pair_val, &c->pair_key_alt, &c->pair_val_alt, &c->ranges, &c->rgba, &c->aux, &c->dl,
+                   &c->gt, &c->out_a, &c->out_b, &c->out_c, &c->out_d};
+  for (DevBuf* b : all) info->device_bytes += b->bytes;
+  return RMESH_OK;
+}
+
+int rmesh_forward_tiled(RmeshCtx* c, const RmeshCamera* cam, float* rgba_out, float* aux_out) {
+  if (!c || !cam || !rgba_out) return RMESH_ERR_INVALID_ARG;
+  const uint64_t npix = (uint64_t)cam->width * cam->height;
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    CKR(fill_view(c, *cam, c->views_h[0], 0, 0));
+    const uint32_t tiles = (uint32_t)(c->views_h[0].tiles_x * c->views_h[0].tiles_y);
+    CKR(ensure_run_buffers(c, 1, npix, tiles));
+    if (aux_out) CKR(ensure_buf(c, c->aux, npix * 32));
+    CKR(upload_views(c, 1));
+    Counters* cnt = c->counters_d.as<Counters>();
+    CK(cudaMemsetAsync(cnt, 0, sizeof(Counters), c->stream));
+    CKR(run_records(c, false));
+    ViewParams* vd = c->views_d.as<ViewParams>();
+    CKR(run_bin(c, vd, 1, tiles, cnt, false));
+    {
+      StageScope sc(c, kStComposite, false);
+      TileArgs ta = base_tile_args(c, vd, 1, tiles, cnt);
+      ta.rgba = c->rgba.as<float>();
+      if (aux_out) {
+        ta.aux = c->aux.as<float>();
+        CKR((launch_tile_m<kModeForward, true>(c, ta, tiles, true)));
+      } else {
+        CKR((launch_tile_m<kModeForward, false>(c, ta, tiles, true)));
+      }
+    }
+    CKR(sync_counters(c, 1));
+    if ((c->last_err_bits & kErrPairOverflow) && grow_pairs(c)) continue;
+    CKR(status_from_bits(c));
+    CK(cudaMemcpyAsync(rgba_out, c->rgba.p, npix * 16, cudaMemcpyDefault, c->stream));
+    if (aux_out) CK(cudaMemcpyAsync(aux_out, c->aux.p, npix * 32, cudaMemcpyDefault, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_forward = true;
+    c->last_tiles = tiles;
+    c->last_views = 1;
+    return RMESH_OK;
+  }
+  return fail(c, RMESH_ERR_PAIR_OVERFLOW, "pair buffers could not be grown enough");
+}
+
+int rmesh_backward(RmeshCtx* c, const float* dl, float* d_verts, float* d_dens, float* d_base, float* d_cgrad) {
+  if (!c || !dl) return RMESH_ERR_INVALID_ARG;
+  if (!c->have_forward) return fail(c, RMESH_ERR_STATE, "backward() must follow forward_tiled()");
+  const ViewParams& v = c->views_h[0];
+  const uint64_t npix = (uint64_t)v.W * v.H;
+  CKR(ensure_buf(c, c->dl, npix * 16));
+  CK(cudaMemcpyAsync(c->dl.p, dl, npix * 16, cudaMemcpyDefault, c->stream));
+  CK(cudaMemsetAsync(c->grad_slot.p, 0, (size_t)c->M * kGradSlot * 4, c->stream));
+  Counters* cnt = c->counters_d.as<Counters>();
+  CK(cudaMemsetAsync(&cnt->tile_ticket, 0, sizeof(uint32_t), c->stream));
+  ViewParams* vd = c->views_d.as<ViewParams>();
+  {
+    StageScope sc(c, kStComposite, false);
+    TileArgs ta = base_tile_args(c, vd, 1, c->last_tiles, cnt);
+    ta.rgba = c->rgba.as<float>();
+    ta.dl_rgba = c->dl.as<float>();
+    CKR((launch_tile_m<kModeBackward, false>(c, ta, c->last_tiles, true)));
+  }
+  const size_t N = (size_t)c->N, M = (size_t)c->M;
+  CKR(ensure_buf(c, c->out_a, 3 * N * 4));
+  CKR(ensure_buf(c, c->out_b, M * 4));
+  CKR(ensure_buf(c, c->out_c, 3 * M * 4));
+  CKR(ensure_buf(c, c->out_d, 3 * M * 4));
+  const int blocks = (int)std::min<int64_t>((c->N + c->M + 255) / 256, (int64_t)c->num_sms * 16);
+  unpack_grads_kernel<<<std::max(1, blocks), 256, 0, c->stream>>>(
+      (int)c->N, (int)c->M, c->grad_slot.as<float>(), c->csr_off.as<uint32_t>(), c->csr_ref.as<uint32_t>(),
+      c->out_a.as<float>(), c->out_b.as<float>(), c->out_c.as<float>(), c->out_d.as<float>());
+  CKL();
+  if (d_verts) CK(cudaMemcpyAsync(d_verts, c->out_a.p, 3 * N * 4, cudaMemcpyDefault, c->stream));
+  if (d_dens) CK(cudaMemcpyAsync(d_dens, c->out_b.p, M * 4, cudaMemcpyDefault, c->stream));
+  if (d_base) CK(cudaMemcpyAsync(d_base, c->out_c.p, 3 * M * 4, cudaMemcpyDefault, c->stream));
+  if (d_cgrad) CK(cudaMemcpyAsync(d_cgrad, c->out_d.p, 3 * M * 4, cudaMemcpyDefault, c->stream));
+  CKR(sync_counters(c, 1));
+  return status_from_bits(c);
+}
+
+int rmesh_train_step(RmeshCtx* c, const RmeshCamera* cam, const float* gt, float lr_verts, float lr_dens,
+                     float lr_grads, int32_t loss_type, float* loss_out) {
+  if (!c) return RMESH_ERR_INVALID_ARG;
+  RmeshTrainOpts o;
+  memset(&o, 0, sizeof(o));
+  o.lr_verts = lr_verts;
+  o.lr_dens = lr_dens;
+  o.lr_grads = lr_grads;
+  o.lr_base = 0.0f;
+  o.loss_type = loss_type;
+  o.mode = RMESH_MODE_BATCHED;
+  return train_views(c, cam, 1, gt, &o, loss_out);
+}
+
+int rmesh_train_step_views(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views, const float* gt,
+                           const RmeshTrainOpts* opts, float* loss_out) {
+  if (!c) return RMESH_ERR_INVALID_ARG;
+  if (!opts || opts->mode < 0 || opts->mode > 2) return fail(c, RMESH_ERR_INVALID_ARG, "bad mode");
+  return train_views(c, cams, n_views, gt, opts, loss_out);
+}
+
+int rmesh_accumulate_views(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views, const float* gt,
+                           const RmeshTrainOpts* opts, float* loss_out) {
+  if (!c) return RMESH_ERR_INVALID_ARG;
+  if (!opts || opts->mode < 0 || opts->mode > 2) return fail(c, RMESH_ERR_INVALID_ARG, "bad mode");
+  return train_views(c, cams, n_views, gt, opts, loss_out, false);
+}
+
+int rmesh_grad_slots(RmeshCtx* c, float** ptr, uint64_t* n_floats) {
+  if (!c || !ptr || !n_floats) return RMESH_ERR_INVALID_ARG;
+  *ptr = c->grad_slot.as<float>();
+  *n_floats = (uint64_t)c->M * kGradSlot;
+  return RMESH_OK;
+}
+
+int rmesh_apply_adam(RmeshCtx* c, const RmeshTrainOpts* o) {
+  if (!c || !o) return RMESH_ERR_INVALID_ARG;
+  AdamParams& hp = *c->hp_h;
+  hp.step = c->step + 1;
+  hp.lr_verts = o->lr_verts;
+  hp.lr_dens = o->lr_dens;
+  hp.lr_grads = o->lr_grads;
+  hp.lr_base = o->lr_base;
+  hp.lr_sh = 0.0f;
+  hp.beta1 = 0.9f;
+  hp.beta2 = 0.999f;
+  hp.eps = 1e-8f;
+  hp.loss_type = o->loss_type;
+  CK(cudaMemcpyAsync(c->hp_d.p, c->hp_h, sizeof(AdamParams), cudaMemcpyHostToDevice, c->stream));
+  CKR(launch_adam(c, c->last_cnt, false));
+  CK(cudaStreamSynchronize(c->stream));
+  c->step += 1;
+  return RMESH_OK;
+}
+
+int rmesh_debug_tiles_touched(RmeshCtx* c, uint32_t* out) {
+  if (!c || !out) return RMESH_ERR_INVALID_ARG;
+  if (!c->have_forward) return fail(c, RMESH_ERR_STATE, "no forward yet");
+  CK(cudaMemcpyAsync(out, c->tiles_touched.p, (size_t)c->M * 4, cudaMemcpyDefault, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return RMESH_OK;
+}
+
+int rmesh_debug_pairs(RmeshCtx* c, uint32_t* tiles, uint32_t* tets, uint64_t cap, uint64_t* n) {
+  if (!c || !n) return RMESH_ERR_INVALID_ARG;
+  if (!c->have_forward) return fail(c, RMESH_ERR_STATE, "no forward yet");
+  *n = c->last_n_pairs;
+  const uint64_t k = std::min<uint64_t>(cap, c->last_n_pairs);
+  if (k && tiles) CK(cudaMemcpyAsync(tiles, c->sorted_pair_key, k * 4, cudaMemcpyDefault, c->stream));
+  if (k && tets) CK(cudaMemcpyAsync(tets, c->sorted_pair_val, k * 4, cudaMemcpyDefault, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return RMESH_OK;
+}
+
+int rmesh_debug_ranges(RmeshCtx* c, uint32_t* ranges, uint64_t n_tiles) {
+  if (!c || !ranges) return RMESH_ERR_INVALID_ARG;
+  if (!c->have_forward) return fail(c, RMESH_ERR_STATE, "no forward yet");
+  const uint64_t k = std::min<uint64_t>(n_tiles, c->last_tiles);
+  CK(cudaMemcpyAsync(ranges, c->ranges.p, k * 8, cudaMemcpyDefault, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return RMESH_OK;
+}
+
+int rmesh_set_profiling(RmeshCtx* c, int32_t on) {
+  if (!c) return RMESH_ERR_INVALID_ARG;
+  c->profiling = on != 0;
+  return RMESH_OK;
+}
+
+int rmesh_stage_times(RmeshCtx* c, float* ms_out, int32_t* launches_out) {
+  if (!c) return RMESH_ERR_INVALID_ARG;
+  CK(cudaStreamSynchronize(c->stream));
+  for (auto& e : c->events) {
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) {
+      c->stage_ms[e.stage] += ms;
+      c->stage_launches[e.stage] += 1;
+    }
+    c->event_pool.push_back(e.a);
+    c->event_pool.push_back(e.b);
+  }
+  c->events.clear();
+  if (ms_out)
+    for (int i = 0; i < RMESH_N_STAGES; ++i) ms_out[i] = c->stage_ms[i];
+  if (launches_out) {
+    for (int i = 0; i < RMESH_N_STAGES; ++i) launches_out[i] = c->stage_launches[i];
+    launches_out[RMESH_N_STAGES] = c->kernel_launches;
+  }
+  for (int i = 0; i < RMESH_N_STAGES; ++i) {
+    c->stage_ms[i] = 0.f;
+    c->stage_launches[i] = 0;
+  }
+  c->kernel_launches = 0;
+  return RMESH_OK;
+}
+
+}  // extern "C"

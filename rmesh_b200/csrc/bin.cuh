@@ -1,0 +1,139 @@
+// Tile binning: emit (tile, tet) pairs in depth order, then per-tile ranges.
+//
+// Order of work (B200 design): tets are first sorted by (view, ~depth) at tet
+// granularity (onesweep, 32 + view bits), then each tet emits its tiles at
+// offsets given by a chained scan of tiles_touched in that order, and a short
+// stable sort on the global tile id (ceil(log2 tiles) bits) finishes the job.
+// Per tile this yields exactly the reference's order -- ascending 64-bit key
+// (tile << 32 | ~depth) with ties broken by tet id -- while the pair-level sort
+// touches 2-3 digits instead of the reference's 6-7
+// (crates/rmesh-sort/src/drs.rs:23-26).
+//
+// Emission restates crates/rmesh-tile/src/wgsl/tile_gen_scan_compute.wgsl:61-203:
+// division-projected vertices, at most tiles_touched pairs per tet (the count
+// project_compute.wgsl made with multiply-by-reciprocal projection), and a
+// sentinel (tile 0xFFFFFFFF, value 0) for every slot the tet leaves unfilled
+// (tile_fill_compute.wgsl:9-19).  Sentinels sort after every real tile.
+#pragma once
+#include "common.cuh"
+#include "project.cuh"
+
+namespace rm {
+
+struct EmitArgs {
+  const ViewParams* views;
+  const unsigned long long* tet_key_sorted;  // (view << 32) | ~depth, sorted
+  const uint32_t* tet_val_sorted;            // compact index j
+  const uint32_t* vis_tet;
+  const uint32_t* vis_cnt;
+  const float4* vis_proj;
+  const uint32_t* n_vis_ptr;
+  uint32_t* pair_key;   // global tile id
+  uint32_t* pair_val;   // tet id
+  unsigned long long cap;
+  unsigned long long* status;
+  uint32_t* ticket;
+  Counters* counters;
+};
+
+__global__ void __launch_bounds__(256) emit_kernel(EmitArgs a) {
+  __shared__ uint32_t s_blk;
+  __shared__ unsigned long long s_wsum[8];
+  __shared__ unsigned long long s_prefix;
+  if (threadIdx.x == 0) s_blk = atomicAdd(a.ticket, 1u);
+  __syncthreads();
+  const uint32_t blk = s_blk;
+  const uint32_t n = *a.n_vis_ptr;
+  if ((unsigned long long)blk * 256ull >= n) return;  // later blocks never wait on this one
+  const uint32_t k = blk * 256u + threadIdx.x;
+  const bool in = k < n;
+  uint32_t j = 0, cnt = 0;
+  if (in) {
+    j = a.tet_val_sorted[k];
+    cnt = a.vis_cnt[j];
+  }
+  // block exclusive scan of cnt (64-bit)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned long long x = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_wsum[warp] = x;
+  __syncthreads();
+  unsigned long long woff = 0, btot = 0;
+#pragma unroll
+  for (int w = 0; w < 8; ++w) {
+    if (w < warp) woff += s_wsum[w];
+    btot += s_wsum[w];
+  }
+  if (warp == 0) {
+    const unsigned long long pre = chained_lookback(a.status, blk, btot, &a.counters->err);
+    if (lane == 0) s_prefix = pre;
+  }
+  __syncthreads();
+  const unsigned long long off = s_prefix + woff + x - cnt;
+  if (!in) return;
+  if (k == n - 1) a.counters->n_pairs = off + cnt;
+  if (cnt == 0) return;
+
+  const uint32_t view = (uint32_t)(a.tet_key_sorted[k] >> 32);
+  const ViewParams& V = a.views[view];
+  const uint32_t tet = a.vis_tet[j];
+  const float4 q0 = a.vis_proj[2 * j], q1 = a.vis_proj[2 * j + 1];
+  const float px[4] = {q0.x, q0.z, q1.x, q1.z};
+  const float py[4] = {q0.y, q0.w, q1.y, q1.w};
+  uint32_t local = 0;
+  bool overflow = false;
+  scanline_tiles(px, py, V.Wf, V.Hf, (uint32_t)V.TS, [&](uint32_t ty, uint32_t tx0, uint32_t tx1) {
+    for (uint32_t tx = tx0; tx <= tx1 && local < cnt; ++tx, ++local) {
+      const unsigned long long w = off + local;
+      if (w < a.cap) {
+        a.pair_key[w] = V.tile_base + ty * (uint32_t)V.tiles_x + tx;
+        a.pair_val[w] = tet;
+      } else {
+        overflow = true;
+      }
+    }
+  });
+  if (local < cnt) atomicOr(&a.counters->shortfall[view], 1u);
+  for (; local < cnt; ++local) {
+    const unsigned long long w = off + local;
+    if (w < a.cap) {
+      a.pair_key[w] = kSentinel;
+      a.pair_val[w] = 0u;
+    } else {
+      overflow = true;
+    }
+  }
+  if (overflow) atomicOr(&a.counters->err, kErrPairOverflow);
+}
+
+// Per-tile [start, end) over the sorted pair keys.  Restates
+// tile_ranges_compute.wgsl:10-45 per view: the end of a view's last non-empty
+// tile is only written when the view had no sentinel slots (in the reference
+// the sentinels follow that tile and the idx == count-1 rule never fires for
+// it, leaving end = 0 from the clear).  ranges must be zeroed beforehand.
+__global__ void __launch_bounds__(256) ranges_kernel(const uint32_t* __restrict__ keys,
+                                                     const unsigned long long* n_ptr, unsigned long long cap,
+                                                     uint2* __restrict__ ranges,
+                                                     const ViewParams* views, int n_views,
+                                                     const Counters* counters) {
+  const unsigned long long n = *n_ptr < cap ? *n_ptr : cap;
+  for (unsigned long long idx = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; idx < n;
+       idx += (unsigned long long)gridDim.x * blockDim.x) {
+    const uint32_t key = keys[idx];
+    if (key == kSentinel) continue;
+    const uint32_t prev = idx > 0 ? keys[idx - 1] : kSentinel;
+    const uint32_t next = idx + 1 < n ? keys[idx + 1] : kSentinel;
+    if (idx == 0 || key != prev) ranges[key].x = (uint32_t)idx;
+    if (next != key) {
+      const int v = view_of_tile(views, n_views, key);
+      const bool last_of_view = (next == kSentinel) || view_of_tile(views, n_views, next) != v;
+      if (!(last_of_view && counters->shortfall[v])) ranges[key].y = (uint32_t)(idx + 1);
+    }
+  }
+}
+
+}  // namespace rm

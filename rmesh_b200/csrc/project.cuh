@@ -1,0 +1,226 @@
+// Per-tet stage: record packing, projection, culling, tile counting, depth keys
+// and deterministic compaction of the tile-touching tets of every view.
+//
+// Reference: crates/rmesh-render/src/wgsl/project_compute.wgsl:88-325 (cull,
+// tiles_touched, colours) and tile_gen_scan_compute.wgsl:135-143 (the
+// circumsphere depth key used for the tile sort).  The reference compacts with
+// atomicAdd (project_compute.wgsl:181); here compaction is a single-pass
+// chained scan in (view, tet) order, so downstream order is deterministic.
+#pragma once
+#include "common.cuh"
+
+namespace rm {
+
+// Per-tet record, view independent, rebuilt whenever parameters change.
+// 64 bytes: a = (v0, density), b = (v1, g.x), c = (v2, g.y), d = (v3, g.z).
+struct __align__(16) TetRec {
+  float4 a, b, c, d;
+};
+
+__global__ void __launch_bounds__(256) build_records_kernel(int M, const float* __restrict__ verts,
+                                                            const uint4* __restrict__ idx4,
+                                                            const float* __restrict__ dens,
+                                                            const float* __restrict__ cgrad,
+                                                            const float* __restrict__ base,
+                                                            TetRec* __restrict__ rec, float4* __restrict__ color4) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= M) return;
+  uint4 q = idx4[t];
+  float g0 = cgrad[3 * t], g1 = cgrad[3 * t + 1], g2 = cgrad[3 * t + 2];
+  TetRec r;
+  r.a = make_float4(verts[3 * q.x], verts[3 * q.x + 1], verts[3 * q.x + 2], dens[t]);
+  r.b = make_float4(verts[3 * q.y], verts[3 * q.y + 1], verts[3 * q.y + 2], g0);
+  r.c = make_float4(verts[3 * q.z], verts[3 * q.z + 1], verts[3 * q.z + 2], g1);
+  r.d = make_float4(verts[3 * q.w], verts[3 * q.w + 1], verts[3 * q.w + 2], g2);
+  rec[t] = r;
+  if (color4) color4[t] = make_float4(base[3 * t], base[3 * t + 1], base[3 * t + 2], 0.0f);
+}
+
+// Conservative scanline over tile rows (project_compute.wgsl:202-259 ==
+// tile_gen_scan_compute.wgsl:119-201), exact arithmetic.  Calls
+// f(ty, tx0, tx1) for every tile row with a non-empty clamped span.
+template <class F>
+__device__ __forceinline__ void scanline_tiles(const float px[4], const float py[4], float W, float H, uint32_t TS,
+                                               F&& f) {
+  const float pix_min_x = fmaxf(fminf(fminf(px[0], px[1]), fminf(px[2], px[3])), 0.0f);
+  const float pix_max_x = fminf(fmaxf(fmaxf(px[0], px[1]), fmaxf(px[2], px[3])), fs(W, 1.0f));
+  const float pix_min_y = fmaxf(fminf(fminf(py[0], py[1]), fminf(py[2], py[3])), 0.0f);
+  const float pix_max_y = fminf(fmaxf(fmaxf(py[0], py[1]), fmaxf(py[2], py[3])), fs(H, 1.0f));
+  if (pix_min_x > pix_max_x || pix_min_y > pix_max_y) return;
+  const float T = (float)TS;
+  const uint32_t tiles_x_total = __float2uint_rz(ceilf(fdv(W, T)));
+  const uint32_t tile_min_x = __float2uint_rz(fdv(pix_min_x, T));
+  const uint32_t tile_max_x = min(__float2uint_rz(fdv(pix_max_x, T)), tiles_x_total - 1u);
+  const uint32_t tile_min_y = __float2uint_rz(fdv(pix_min_y, T));
+  const uint32_t tile_max_y = min(__float2uint_rz(fdv(pix_max_y, T)), __float2uint_rz(ceilf(fdv(H, T))) - 1u);
+  const int ei[6] = {0, 0, 0, 1, 1, 2};
+  const int ej[6] = {1, 2, 3, 2, 3, 3};
+  for (uint32_t ty = tile_min_y; ty <= tile_max_y; ++ty) {
+    float xl = 1e10f, xr = -1e10f;
+#pragma unroll
+    for (int e = 0; e < 6; ++e) {
+      const float yi = py[ei[e]], yj = py[ej[e]], xi = px[ei[e]], xj = px[ej[e]];
+#pragma unroll
+      for (uint32_t b = 0; b < 2; ++b) {
+        const float ytest = fm((float)(ty + b), T);
+        if ((yi <= ytest && yj > ytest) || (yj <= ytest && yi > ytest)) {
+          const float t = fdv(fs(ytest, yi), fs(yj, yi));
+          const float x = fa(xi, fm(t, fs(xj, xi)));
+          xl = fminf(xl, x);
+          xr = fmaxf(xr, x);
+        }
+      }
+    }
+    const float band_lo = fm((float)ty, T), band_hi = fm((float)(ty + 1u), T);
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      if (py[v] >= band_lo && py[v] <= band_hi) {
+        xl = fminf(xl, px[v]);
+        xr = fmaxf(xr, px[v]);
+      }
+    }
+    if (xl <= xr) {
+      uint32_t tx0 = __float2uint_rz(fmaxf(floorf(fdv(xl, T)), 0.0f));
+      uint32_t tx1 = __float2uint_rz(fmaxf(floorf(fdv(xr, T)), 0.0f));
+      tx0 = min(max(tx0, tile_min_x), tile_max_x);
+      tx1 = min(max(tx1, tile_min_x), tile_max_x);
+      f(ty, tx0, tx1);
+    }
+  }
+}
+
+struct ProjectArgs {
+  int M;
+  int n_views;
+  const ViewParams* views;
+  const TetRec* rec;
+  const float4* circ;
+  // compaction outputs (index j in (view, tet) order of tile-touching tets)
+  unsigned long long* vis_key;  // (view << 32) | ~bits(depth)
+  uint32_t* vis_val;            // j (sort payload)
+  uint32_t* vis_tet;
+  uint32_t* vis_cnt;            // tiles_touched
+  float4* vis_proj;             // 2 per entry: division-projected pixel coords (emission)
+  uint32_t* tiles_touched;      // optional [n_views*M], indexed by (view, tet id)
+  unsigned long long* status;   // chained-scan status, one word per block (zeroed)
+  uint32_t* ticket;             // block ticket (zeroed)
+  Counters* counters;
+};
+
+__global__ void __launch_bounds__(256) project_kernel(ProjectArgs a) {
+  __shared__ uint32_t s_blk;
+  __shared__ uint32_t s_warp[8];
+  __shared__ unsigned long long s_prefix;
+  if (threadIdx.x == 0) s_blk = atomicAdd(a.ticket, 1u);
+  __syncthreads();
+  const uint32_t blk = s_blk;
+  const unsigned long long total_items = (unsigned long long)a.M * (unsigned long long)a.n_views;
+  const unsigned long long i = (unsigned long long)blk * 256ull + threadIdx.x;
+
+  bool flag = false;
+  uint32_t count = 0, inv_depth = 0, view = 0, tet = 0;
+  float qx[4], qy[4];
+  if (i < total_items) {
+    view = (uint32_t)(i / (unsigned long long)a.M);
+    tet = (uint32_t)(i - (unsigned long long)view * a.M);
+    const ViewParams& V = a.views[view];
+    const TetRec r = a.rec[tet];
+    const float vx[4] = {r.a.x, r.b.x, r.c.x, r.d.x};
+    const float vy[4] = {r.a.y, r.b.y, r.c.y, r.d.y};
+    const float vz[4] = {r.a.z, r.b.z, r.c.z, r.d.z};
+    float p[4][4], c[4][4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      clip_exact(V.vp, vx[k], vy[k], vz[k], c[k]);
+      const float inv_w = fdv(1.0f, fa(c[k][3], 1e-6f));
+      p[k][0] = fm(c[k][0], inv_w);
+      p[k][1] = fm(c[k][1], inv_w);
+      p[k][2] = fm(c[k][2], inv_w);
+      p[k][3] = c[k][3];
+    }
+    const bool any_behind = (p[0][3] <= 0.0f) || (p[1][3] <= 0.0f) || (p[2][3] <= 0.0f) || (p[3][3] <= 0.0f);
+    bool visible = true;
+    if (!any_behind) {
+      const float min_x = fminf(fminf(p[0][0], p[1][0]), fminf(p[2][0], p[3][0]));
+      const float max_x = fmaxf(fmaxf(p[0][0], p[1][0]), fmaxf(p[2][0], p[3][0]));
+      const float min_y = fminf(fminf(p[0][1], p[1][1]), fminf(p[2][1], p[3][1]));
+      const float max_y = fmaxf(fmaxf(p[0][1], p[1][1]), fmaxf(p[2][1], p[3][1]));
+      const float min_z = fminf(fminf(p[0][2], p[1][2]), fminf(p[2][2], p[3][2]));
+      if (max_x < -1.0f || min_x > 1.0f || max_y < -1.0f || min_y > 1.0f || min_z > 1.0f) visible = false;
+      const float ext_x = fm(fs(max_x, min_x), V.Wf);
+      const float ext_y = fm(fs(max_y, min_y), V.Hf);
+      if (fm(ext_x, ext_y) < 1.0f) visible = false;
+    }
+    if (visible) {  // optical-depth cull (project_compute.wgsl:146-162)
+      float e2[6];
+      const int ei[6] = {1, 2, 3, 2, 3, 3};
+      const int ej[6] = {0, 0, 0, 1, 1, 2};
+#pragma unroll
+      for (int e = 0; e < 6; ++e) {
+        const float dx = fs(vx[ei[e]], vx[ej[e]]), dy = fs(vy[ei[e]], vy[ej[e]]), dz = fs(vz[ei[e]], vz[ej[e]]);
+        e2[e] = dot3x(dx, dy, dz, dx, dy, dz);
+      }
+      const float m = fmaxf(fmaxf(e2[0], fmaxf(e2[1], e2[2])), fmaxf(e2[3], fmaxf(e2[4], e2[5])));
+      if (fm(r.a.w, __fsqrt_rn(m)) < 0.01f) visible = false;
+    }
+    if (visible && !any_behind) {
+      float px[4], py[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        px[k] = fm(fm(fa(p[k][0], 1.0f), 0.5f), V.Wf);
+        py[k] = fm(fm(fs(1.0f, p[k][1]), 0.5f), V.Hf);
+      }
+      scanline_tiles(px, py, V.Wf, V.Hf, (uint32_t)V.TS,
+                     [&](uint32_t, uint32_t tx0, uint32_t tx1) { count += tx1 - tx0 + 1u; });
+    }
+    if (a.tiles_touched) a.tiles_touched[i] = (visible ? count : 0u);
+    flag = visible && count > 0u;
+    if (flag) {
+      // depth key (tile_gen_scan_compute.wgsl:136-143)
+      const float4 C = a.circ[tet];
+      const float dx = fs(C.x, V.cam[0]), dy = fs(C.y, V.cam[1]), dz = fs(C.z, V.cam[2]);
+      const float depth = fs(dot3x(dx, dy, dz, dx, dy, dz), C.w);
+      inv_depth = ~__float_as_uint(depth);
+      // division-projected coords used by the emission stage (:108-117)
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const float w = fa(c[k][3], 1e-6f);
+        qx[k] = fm(fm(fa(fdv(c[k][0], w), 1.0f), 0.5f), V.Wf);
+        qy[k] = fm(fm(fs(1.0f, fdv(c[k][1], w)), 0.5f), V.Hf);
+      }
+    }
+  }
+  // block-level exclusive scan of flags
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned ballot = __ballot_sync(0xffffffffu, flag);
+  if (lane == 0) s_warp[warp] = __popc(ballot);
+  __syncthreads();
+  uint32_t warp_off = 0, block_total = 0;
+#pragma unroll
+  for (int w = 0; w < 8; ++w) {
+    const uint32_t c = s_warp[w];
+    if (w < warp) warp_off += c;
+    block_total += c;
+  }
+  if (warp == 0) {
+    const unsigned long long pre = chained_lookback(a.status, blk, block_total, &a.counters->err);
+    if (lane == 0) s_prefix = pre;
+  }
+  __syncthreads();
+  const unsigned long long base = s_prefix;
+  if (flag) {
+    const unsigned long long j = base + warp_off + __popc(ballot & ((1u << lane) - 1u));
+    a.vis_key[j] = ((unsigned long long)view << 32) | inv_depth;
+    a.vis_val[j] = (uint32_t)j;
+    a.vis_tet[j] = tet;
+    a.vis_cnt[j] = count;
+    a.vis_proj[2 * j] = make_float4(qx[0], qy[0], qx[1], qy[1]);
+    a.vis_proj[2 * j + 1] = make_float4(qx[2], qy[2], qx[3], qy[3]);
+  }
+  // the block holding the last item publishes the visible count
+  if (threadIdx.x == 0 && (unsigned long long)(blk + 1) * 256ull >= total_items &&
+      (unsigned long long)blk * 256ull < total_items)
+    a.counters->n_vis = (uint32_t)(base + block_total);
+}
+
+}  // namespace rm

@@ -1,0 +1,362 @@
+"""``RMeshRenderer``: the reference binding's class, backed by the B200 C ABI.
+
+Method names, argument meaning, dict keys and return shapes follow the PyO3
+class of the reference (crates/rmesh-python/src/lib.rs):
+
+* ``RMeshRenderer(vertices, indices, base_colors, densities, color_grads,
+  circumdata, width, height, aux_dim=0)``                       lib.rs:265-277
+* ``set_min_t(min_t)``                                          lib.rs:873-875
+* ``forward_tiled(cam_pos, vp, c2w_intrinsics, render_aux=False)`` lib.rs:1040-1204
+* ``backward(dl_d_image) -> dict``                              lib.rs:1894-2031
+* ``train_step(cam_pos, vp, c2w_intrinsics, gt_image, lr_verts, lr_dens,
+  lr_grads, loss_type) -> float``                               lib.rs:2405-2636
+* ``update_params(...)`` / ``get_params()``                     lib.rs:2641-2686
+* ``step`` / ``width`` / ``height``                             lib.rs:2688-2705
+
+Differences, all additive: ``train_step`` returns the actual loss (the
+reference returns 0.0 because its loss buffer is never written); inputs may
+also be torch tensors, and CUDA tensors are passed to the device without a
+host round trip; ``train_step_views`` trains on several cameras per step.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib
+
+__all__ = ["RMeshRenderer", "RMeshError"]
+
+
+class RMeshError(RuntimeError):
+    """A failing C-ABI call (status code and message attached)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"rmesh_b200 error {code}: {msg}")
+        self.code = code
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _as_array(x, dtype, name: str):
+    """Returns (object to keep alive, pointer as int) for a flat C-contiguous array."""
+    if _is_torch(x):
+        import torch
+
+        tdt = torch.float32 if dtype == np.float32 else torch.int32
+        if x.dtype not in (tdt, torch.uint32 if dtype == np.uint32 else tdt):
+            if dtype == np.uint32 and x.dtype in (torch.int32, torch.int64):
+                x = x.to(torch.int32)
+            else:
+                raise TypeError(f"{name}: expected a {tdt} tensor, got {x.dtype}")
+        if x.is_cuda:
+            torch.cuda.current_stream(x.device).synchronize()
+        x = x.contiguous()
+        return x, x.data_ptr()
+    a = np.asarray(x)
+    if a.dtype != dtype:
+        if dtype == np.uint32 and a.dtype.kind in "iu":
+            a = a.astype(np.uint32)
+        elif dtype == np.float32 and a.dtype.kind == "f":
+            a = a.astype(np.float32)
+        else:
+            raise TypeError(f"{name}: expected {np.dtype(dtype).name}, got {a.dtype}")
+    a = np.ascontiguousarray(a)
+    return a, a.ctypes.data
+
+
+def _camera_struct(cam_pos, vp, c2w_intrinsics, width: int, height: int) -> _lib.Camera:
+    c = _lib.Camera()
+    cp = np.asarray(_to_numpy(cam_pos), dtype=np.float32).ravel()
+    v = np.asarray(_to_numpy(vp), dtype=np.float32).ravel()
+    ci = np.asarray(_to_numpy(c2w_intrinsics), dtype=np.float32).ravel()
+    if cp.size != 3 or v.size != 16 or ci.size != 16:
+        raise ValueError("cam_pos must have 3 values, vp and c2w_intrinsics 16")
+    c.cam_pos[:] = cp.tolist()
+    c.vp[:] = v.tolist()
+    c.c2w_intrinsics[:] = ci.tolist()
+    c.width = int(width)
+    c.height = int(height)
+    return c
+
+
+def _to_numpy(x):
+    if _is_torch(x):
+        return x.detach().cpu().numpy()
+    return x
+
+
+class RMeshRenderer:
+    """Tiled differentiable tet-mesh volume renderer on one CUDA device."""
+
+    def __init__(self, vertices, indices, base_colors, densities, color_grads, circumdata, width: int,
+                 height: int, aux_dim: int = 0, *, tile_size: int = 12, device: int | None = None):
+        self._lib = _lib.load()
+        if int(aux_dim) != 0:
+            raise ValueError("aux_dim > 0 is not supported by this build")
+        keep = []
+        ptrs = {}
+        for name, arr, dt in (("vertices", vertices, np.float32), ("indices", indices, np.uint32),
+                              ("base_colors", base_colors, np.float32), ("densities", densities, np.float32),
+                              ("color_grads", color_grads, np.float32), ("circumdata", circumdata, np.float32)):
+            obj, p = _as_array(arr, dt, name)
+            keep.append(obj)
+            ptrs[name] = (obj, p)
+        n_v = _numel(ptrs["vertices"][0])
+        n_i = _numel(ptrs["indices"][0])
+        if n_v % 3 or n_i % 4 or n_i == 0:
+            raise ValueError("vertices must hold 3N floats and indices 4M (M > 0) integers")
+        self._N, self._M = n_v // 3, n_i // 4
+        for name, per in (("base_colors", 3), ("densities", 1), ("color_grads", 3), ("circumdata", 4)):
+            if _numel(ptrs[name][0]) != per * self._M:
+                raise ValueError(f"{name} must hold {per}*M = {per * self._M} values")
+        d = _lib.SceneDesc()
+        d.n_vertices, d.n_tets = self._N, self._M
+        d.vertices, d.indices = ptrs["vertices"][1], ptrs["indices"][1]
+        d.base_colors, d.densities = ptrs["base_colors"][1], ptrs["densities"][1]
+        d.color_grads, d.circumdata = ptrs["color_grads"][1], ptrs["circumdata"][1]
+        d.width, d.height, d.aux_dim, d.tile_size = int(width), int(height), 0, int(tile_size)
+        d.device = -1 if device is None else int(device)
+        ctx = ctypes.c_void_p()
+        rc = self._lib.rmesh_create(ctypes.byref(d), ctypes.byref(ctx))
+        if rc != 0:
+            raise RMeshError(rc, "rmesh_create failed (no CUDA device, bad sizes or out of memory)")
+        self._ctx = ctx
+        self._width, self._height = int(width), int(height)
+        self._tile_size = int(tile_size)
+
+    # ------------------------------------------------------------------ utils
+    def _check(self, rc: int):
+        if rc != 0:
+            msg = self._lib.rmesh_last_error(self._ctx)
+            raise RMeshError(rc, msg.decode() if msg else "")
+
+    def close(self):
+        if getattr(self, "_ctx", None):
+            self._lib.rmesh_destroy(self._ctx)
+            self._ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _cam(self, cam_pos, vp, c2w_intrinsics, width=None, height=None):
+        return _camera_struct(cam_pos, vp, c2w_intrinsics, self._width if width is None else width,
+                              self._height if height is None else height)
+
+    # ---------------------------------------------------------------- getters
+    @property
+    def step(self) -> int:
+        return int(self.info().step)
+
+    @property
+    def width(self) -> int:
+        return self._width
+
+    @property
+    def height(self) -> int:
+        return self._height
+
+    @property
+    def n_vertices(self) -> int:
+        return self._N
+
+    @property
+    def n_tets(self) -> int:
+        return self._M
+
+    def info(self) -> _lib.Info:
+        inf = _lib.Info()
+        self._check(self._lib.rmesh_get_info(self._ctx, ctypes.byref(inf)))
+        return inf
+
+    # --------------------------------------------------------------- settings
+    def set_min_t(self, min_t: float):
+        self._check(self._lib.rmesh_set_min_t(self._ctx, float(min_t)))
+
+    def set_tile_size(self, tile_size: int):
+        self._check(self._lib.rmesh_set_tile_size(self._ctx, int(tile_size)))
+        self._tile_size = int(tile_size)
+
+    def set_stream(self, stream_handle: int):
+        self._check(self._lib.rmesh_set_stream(self._ctx, ctypes.c_void_p(int(stream_handle))))
+
+    # ------------------------------------------------------------- parameters
+    def update_params(self, vertices, base_colors, densities, color_grads):
+        keep = []
+        ps = []
+        for name, arr, n in (("vertices", vertices, 3 * self._N), ("base_colors", base_colors, 3 * self._M),
+                             ("densities", densities, self._M), ("color_grads", color_grads, 3 * self._M)):
+            if arr is None:
+                ps.append(None)
+                continue
+            obj, p = _as_array(arr, np.float32, name)
+            if _numel(obj) != n:
+                raise ValueError(f"{name} must hold {n} values, got {_numel(obj)}")
+            keep.append(obj)
+            ps.append(p)
+        self._check(self._lib.rmesh_update_params(self._ctx, *ps))
+
+    def get_params(self) -> dict:
+        out = {"vertices": np.empty(3 * self._N, np.float32), "base_colors": np.empty(3 * self._M, np.float32),
+               "densities": np.empty(self._M, np.float32), "color_grads": np.empty(3 * self._M, np.float32)}
+        self._check(self._lib.rmesh_get_params(self._ctx, out["vertices"].ctypes.data,
+                                               out["base_colors"].ctypes.data, out["densities"].ctypes.data,
+                                               out["color_grads"].ctypes.data))
+        return out
+
+    # -------------------------------------------------------------- the path
+    def forward_tiled(self, cam_pos, vp, c2w_intrinsics, render_aux: bool = False):
+        """[H, W, 4] premultiplied RGBA (and [H, W, 8] aux when ``render_aux``)."""
+        cam = self._cam(cam_pos, vp, c2w_intrinsics)
+        rgba = np.empty((self._height, self._width, 4), np.float32)
+        aux = np.empty((self._height, self._width, 8), np.float32) if render_aux else None
+        self._check(self._lib.rmesh_forward_tiled(self._ctx, ctypes.byref(cam), rgba.ctypes.data,
+                                                  aux.ctypes.data if render_aux else None))
+        return (rgba, aux) if render_aux else rgba
+
+    def forward_tiled_into(self, cam_pos, vp, c2w_intrinsics, out, aux_out=None):
+        """Device-tensor variant: writes into ``out`` ([H,W,4] float32, host or CUDA)."""
+        cam = self._cam(cam_pos, vp, c2w_intrinsics)
+        _, p = _as_array(out, np.float32, "out")
+        pa = None if aux_out is None else _as_array(aux_out, np.float32, "aux_out")[1]
+        self._check(self._lib.rmesh_forward_tiled(self._ctx, ctypes.byref(cam), p, pa))
+        return out
+
+    def backward(self, dl_d_image) -> dict:
+        """dict of 1-D float32 arrays d_vertices, d_densities, d_base_colors, d_color_grads."""
+        obj, p = _as_array(dl_d_image, np.float32, "dl_d_image")
+        if _numel(obj) != 4 * self._width * self._height:
+            raise ValueError("dl_d_image must be [H, W, 4]")
+        out = {"d_vertices": np.empty(3 * self._N, np.float32), "d_densities": np.empty(self._M, np.float32),
+               "d_base_colors": np.empty(3 * self._M, np.float32),
+               "d_color_grads": np.empty(3 * self._M, np.float32)}
+        self._check(self._lib.rmesh_backward(self._ctx, p, out["d_vertices"].ctypes.data,
+                                             out["d_densities"].ctypes.data, out["d_base_colors"].ctypes.data,
+                                             out["d_color_grads"].ctypes.data))
+        return out
+
+    def backward_into(self, dl_d_image, d_vertices, d_densities, d_base_colors, d_color_grads):
+        """Device-tensor variant of ``backward`` writing into the given buffers."""
+        _, p = _as_array(dl_d_image, np.float32, "dl_d_image")
+        ptrs = [_as_array(t, np.float32, "grad")[1] if t is not None else None
+                for t in (d_vertices, d_densities, d_base_colors, d_color_grads)]
+        self._check(self._lib.rmesh_backward(self._ctx, p, *ptrs))
+
+    def train_step(self, cam_pos, vp, c2w_intrinsics, gt_image, lr_verts: float, lr_dens: float,
+                   lr_grads: float, loss_type: int) -> float:
+        cam = self._cam(cam_pos, vp, c2w_intrinsics)
+        obj, p = _as_array(gt_image, np.float32, "gt_image")
+        if _numel(obj) != 3 * self._width * self._height:
+            raise ValueError("gt_image must be [H, W, 3]")
+        loss = ctypes.c_float(0.0)
+        self._check(self._lib.rmesh_train_step(self._ctx, ctypes.byref(cam), p, float(lr_verts), float(lr_dens),
+                                               float(lr_grads), int(loss_type), ctypes.byref(loss)))
+        return float(loss.value)
+
+    def _views_args(self, cameras, gt_images, lr_verts, lr_dens, lr_grads, loss_type, lr_base, mode):
+        n = len(cameras)
+        cams = (_lib.Camera * n)()
+        total = 0
+        for i, c in enumerate(cameras):
+            cams[i] = _camera_struct(c.cam_pos, c.vp, c.c2w_intrinsics, c.width, c.height)
+            total += 3 * c.width * c.height
+        if isinstance(gt_images, (list, tuple)):
+            flat = np.concatenate([np.asarray(_to_numpy(g), np.float32).ravel() for g in gt_images])
+            obj, p = flat, flat.ctypes.data
+        else:
+            obj, p = _as_array(gt_images, np.float32, "gt_images")
+        if _numel(obj) != total:
+            raise ValueError("gt images do not match the cameras' sizes")
+        o = _lib.TrainOpts()
+        o.lr_verts, o.lr_dens, o.lr_grads, o.lr_base = float(lr_verts), float(lr_dens), float(lr_grads), float(lr_base)
+        o.loss_type = int(loss_type)
+        o.mode = {"plain": _lib.MODE_PLAIN, "batched": _lib.MODE_BATCHED, "graph": _lib.MODE_GRAPH}[mode]
+        return n, cams, obj, p, o
+
+    def train_step_views(self, cameras: Sequence, gt_images, lr_verts: float, lr_dens: float, lr_grads: float,
+                         loss_type: int = 1, lr_base: float = 0.0, mode: str = "graph") -> np.ndarray:
+        """One step over several cameras (``rmesh_b200.camera.Camera`` objects) with
+        one Adam update.  ``gt_images``: list of [H,W,3] arrays or one flat
+        array/tensor holding them back to back.  ``mode``: plain | batched | graph.
+        Returns the per-view losses."""
+        n, cams, keep, p, o = self._views_args(cameras, gt_images, lr_verts, lr_dens, lr_grads, loss_type,
+                                               lr_base, mode)
+        losses = np.zeros(n, np.float32)
+        self._check(self._lib.rmesh_train_step_views(self._ctx, cams, n, p, ctypes.byref(o), losses.ctypes.data))
+        return losses
+
+    def accumulate_views(self, cameras: Sequence, gt_images, loss_type: int = 1, mode: str = "graph") -> np.ndarray:
+        """Forward + loss + adjoint over ``cameras``; gradients land in the
+        per-tet slots (see ``grad_slots``), no parameter update."""
+        n, cams, keep, p, o = self._views_args(cameras, gt_images, 0.0, 0.0, 0.0, loss_type, 0.0, mode)
+        losses = np.zeros(n, np.float32)
+        self._check(self._lib.rmesh_accumulate_views(self._ctx, cams, n, p, ctypes.byref(o), losses.ctypes.data))
+        return losses
+
+    def grad_slots(self):
+        """The device gradient slots as a torch CUDA tensor view [M, 20]
+        (density, base rgb, colour-gradient xyz, 4 x vertex xyz, pad)."""
+        import torch
+
+        ptr = ctypes.c_void_p()
+        n = ctypes.c_uint64()
+        self._check(self._lib.rmesh_grad_slots(self._ctx, ctypes.byref(ptr), ctypes.byref(n)))
+
+        class _View:
+            __cuda_array_interface__ = {"shape": (int(n.value),), "typestr": "<f4", "data": (ptr.value, False),
+                                        "version": 3, "strides": None}
+
+        return torch.as_tensor(_View(), device="cuda").view(-1, 20)
+
+    def apply_adam(self, lr_verts: float, lr_dens: float, lr_grads: float, lr_base: float = 0.0,
+                   loss_type: int = 1):
+        o = _lib.TrainOpts()
+        o.lr_verts, o.lr_dens, o.lr_grads, o.lr_base = float(lr_verts), float(lr_dens), float(lr_grads), float(lr_base)
+        o.loss_type = int(loss_type)
+        self._check(self._lib.rmesh_apply_adam(self._ctx, ctypes.byref(o)))
+
+    # ---------------------------------------------------------- inspection
+    def debug_tiles_touched(self) -> np.ndarray:
+        out = np.empty(self._M, np.uint32)
+        self._check(self._lib.rmesh_debug_tiles_touched(self._ctx, out.ctypes.data))
+        return out
+
+    def debug_pairs(self):
+        n = ctypes.c_uint64(0)
+        self._check(self._lib.rmesh_debug_pairs(self._ctx, None, None, 0, ctypes.byref(n)))
+        tiles = np.empty(max(n.value, 1), np.uint32)
+        tets = np.empty(max(n.value, 1), np.uint32)
+        self._check(self._lib.rmesh_debug_pairs(self._ctx, tiles.ctypes.data, tets.ctypes.data, n.value,
+                                                ctypes.byref(n)))
+        return tiles[:n.value], tets[:n.value]
+
+    def debug_ranges(self) -> np.ndarray:
+        ts = self._tile_size
+        nt = ((self._width + ts - 1) // ts) * ((self._height + ts - 1) // ts)
+        out = np.empty(2 * nt, np.uint32)
+        self._check(self._lib.rmesh_debug_ranges(self._ctx, out.ctypes.data, nt))
+        return out
+
+    # ----------------------------------------------------------- profiling
+    def set_profiling(self, on: bool = True):
+        self._check(self._lib.rmesh_set_profiling(self._ctx, 1 if on else 0))
+
+    def stage_times(self):
+        ms = np.zeros(_lib.N_STAGES, np.float32)
+        launches = np.zeros(_lib.N_STAGES + 1, np.int32)
+        self._check(self._lib.rmesh_stage_times(self._ctx, ms.ctypes.data, launches.ctypes.data))
+        return ({k: float(v) for k, v in zip(_lib.STAGE_NAMES, ms)},
+                {k: int(v) for k, v in zip(_lib.STAGE_NAMES, launches[:-1])}, int(launches[-1]))
+
+
+def _numel(x) -> int:
+    if _is_torch(x):
+        return int(x.numel())
+    return int(np.asarray(x).size)
