@@ -10,7 +10,8 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "lib", "librmesh_b200.so")
+# RMESH_B200_LIB selects another build of the same ABI (e.g. a profiling build)
+LIB_PATH = os.environ.get("RMESH_B200_LIB") or os.path.join(_HERE, "lib", "librmesh_b200.so")
 
 RMESH_OK = 0
 RMESH_ERR_INVALID_ARG = 1

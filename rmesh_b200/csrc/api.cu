@@ -350,6 +350,9 @@ int run_bin(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t tota
     pa.vis_tet = c->vis_tet.as<uint32_t>();
     pa.vis_cnt = c->vis_cnt.as<uint32_t>();
     pa.vis_proj = c->vis_proj.as<float4>();
+    pa.vis_view = nullptr;
+    pa.color4 = nullptr;
+    pa.color_view_stride = 0;
     pa.tiles_touched = c->tiles_touched.as<uint32_t>();
     pa.status = status;
     pa.ticket = ticket;
@@ -406,17 +409,23 @@ int run_bin(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t tota
 
 template <int TS, int MODE, bool AUX>
 int launch_tile_t(RmeshCtx* c, TileArgs& ta, uint32_t n_tiles, bool persistent) {
-  constexpr int NT = ((TS * TS + 31) / 32) * 32;
+  constexpr int NT = TileCfg<TS, AUX>::NT;
+  constexpr size_t smem = sizeof(TileSmem<TS, AUX>);
+  static bool attr_done = false;  // per instantiation
+  if (!attr_done) {
+    CK(cudaFuncSetAttribute(tile_kernel<TS, MODE, AUX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    attr_done = true;
+  }
   unsigned grid = n_tiles;
   if (persistent) {
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tile_kernel<TS, MODE, AUX>, NT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tile_kernel<TS, MODE, AUX>, NT, smem);
     grid = (unsigned)std::max(1, occ) * (unsigned)c->num_sms;
     grid = std::min<unsigned>(grid, std::max<uint32_t>(n_tiles, 1));
   }
   ta.persistent = persistent ? 1 : 0;
   if (grid == 0) return RMESH_OK;
-  tile_kernel<TS, MODE, AUX><<<grid, NT, 0, c->stream>>>(ta);
+  tile_kernel<TS, MODE, AUX><<<grid, NT, smem, c->stream>>>(ta);
   CKL();
   return RMESH_OK;
 }

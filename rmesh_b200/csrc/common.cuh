@@ -96,6 +96,8 @@ __device__ __forceinline__ float dphi_f(float x) {
 
 // FACES (crates/rmesh-util/src/wgsl/intersect.wgsl:4-10): (a, b, c, opposite).
 __constant__ int8_t kFaces[4][4] = {{0, 2, 1, 3}, {1, 2, 3, 0}, {0, 3, 2, 1}, {3, 0, 1, 2}};
+// the same table for compile-time-unrolled loops
+__device__ constexpr int kFacesH[4][4] = {{0, 2, 1, 3}, {1, 2, 3, 0}, {0, 3, 2, 1}, {3, 0, 1, 2}};
 
 // ---- bounded spin helpers --------------------------------------------------
 constexpr uint32_t kSpinLimit = 1u << 22;

@@ -89,6 +89,67 @@ __device__ __forceinline__ void scanline_tiles(const float px[4], const float py
   }
 }
 
+// Per-(view, visible tet) record consumed by the tile kernel: everything a
+// tile needs about a tet that depends only on the tet and the view, computed
+// once per view instead of once per (tile, tet) pair.  144 bytes (TMA-sized).
+//   nrm[f]  inward normal of face f, n = cross(vc - va, vb - va) flipped toward
+//           the opposite vertex, and num = dot(n, va - cam), explicitly rounded
+//           (rasterize_compute.wgsl:301-314, 360-372)
+//   cb      colour + dot(g, cam - v0) (the base colour at the camera, :395-396), density
+//   gm      colour gradient g; w = face flip bits (bit f) | behind (bit 4)
+//   px, py  pixel-space vertex projections (c.x/c.w+1)*W/2, (1-c.y/c.w)*H/2 (:163-166)
+//   meta    tet id
+struct __align__(16) TetView {
+  float4 nrm[4];
+  float4 cb;
+  float4 gm;
+  float4 px;
+  float4 py;
+  uint4 meta;
+};
+
+__device__ __forceinline__ void write_tet_view(TetView* dst, const TetRec& r, const float4 col, const ViewParams& V,
+                                               uint32_t tet) {
+  const float4 vs[4] = {r.a, r.b, r.c, r.d};
+  const float camx = V.cam[0], camy = V.cam[1], camz = V.cam[2];
+  uint32_t flags = 0u;
+  TetView out;
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    const float4 va = vs[kFacesH[f][0]], vb = vs[kFacesH[f][1]], vc = vs[kFacesH[f][2]], vo = vs[kFacesH[f][3]];
+    const float e1x = fs(vc.x, va.x), e1y = fs(vc.y, va.y), e1z = fs(vc.z, va.z);
+    const float e2x = fs(vb.x, va.x), e2y = fs(vb.y, va.y), e2z = fs(vb.z, va.z);
+    float nx = fs(fm(e1y, e2z), fm(e1z, e2y));
+    float ny = fs(fm(e1z, e2x), fm(e1x, e2z));
+    float nz = fs(fm(e1x, e2y), fm(e1y, e2x));
+    if (dot3x(nx, ny, nz, fs(vo.x, va.x), fs(vo.y, va.y), fs(vo.z, va.z)) < 0.0f) {
+      nx = -nx; ny = -ny; nz = -nz;
+      flags |= 1u << f;
+    }
+    out.nrm[f] = make_float4(nx, ny, nz, dot3x(nx, ny, nz, fs(va.x, camx), fs(va.y, camy), fs(va.z, camz)));
+  }
+  const float gx = r.b.w, gy = r.c.w, gz = r.d.w;
+  const float boff = dot3x(gx, gy, gz, fs(camx, r.a.x), fs(camy, r.a.y), fs(camz, r.a.z));
+  out.cb = make_float4(fa(col.x, boff), fa(col.y, boff), fa(col.z, boff), r.a.w);
+  float qx[4], qy[4];
+  bool behind = false;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    float c[4];
+    clip_exact(V.vp, vs[k].x, vs[k].y, vs[k].z, c);
+    behind = behind || (c[3] <= 0.0f);
+    const float iw = __fdividef(1.0f, c[3]);
+    qx[k] = (c[0] * iw + 1.0f) * 0.5f * V.Wf;
+    qy[k] = (1.0f - c[1] * iw) * 0.5f * V.Hf;
+  }
+  if (behind) flags |= 1u << 4;
+  out.gm = make_float4(gx, gy, gz, __uint_as_float(flags));
+  out.px = make_float4(qx[0], qx[1], qx[2], qx[3]);
+  out.py = make_float4(qy[0], qy[1], qy[2], qy[3]);
+  out.meta = make_uint4(tet, 0u, 0u, 0u);
+  *dst = out;
+}
+
 struct ProjectArgs {
   int M;
   int n_views;
@@ -101,6 +162,9 @@ struct ProjectArgs {
   uint32_t* vis_tet;
   uint32_t* vis_cnt;            // tiles_touched
   float4* vis_proj;             // 2 per entry: division-projected pixel coords (emission)
+  TetView* vis_view;            // per entry: the tile kernel's per-(view, tet) record
+  const float4* color4;         // tet colours, [view * color_view_stride + tet]
+  uint32_t color_view_stride;
   uint32_t* tiles_touched;      // optional [n_views*M], indexed by (view, tet id)
   unsigned long long* status;   // chained-scan status, one word per block (zeroed)
   uint32_t* ticket;             // block ticket (zeroed)
@@ -216,6 +280,9 @@ __global__ void __launch_bounds__(256) project_kernel(ProjectArgs a) {
     a.vis_cnt[j] = count;
     a.vis_proj[2 * j] = make_float4(qx[0], qy[0], qx[1], qy[1]);
     a.vis_proj[2 * j + 1] = make_float4(qx[2], qy[2], qx[3], qy[3]);
+    if (a.vis_view)
+      write_tet_view(a.vis_view + j, a.rec[tet], a.color4[(size_t)a.color_view_stride * view + tet], a.views[view],
+                   tet);
   }
   // the block holding the last item publishes the visible count
   if (threadIdx.x == 0 && (unsigned long long)(blk + 1) * 256ull >= total_items &&

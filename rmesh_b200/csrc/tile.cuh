@@ -5,27 +5,40 @@
 //   loss      crates/rmesh-train/src/wgsl/loss_compute.wgsl:24-72
 //   adjoint   crates/rmesh-backward/src/wgsl/backward_tiled_compute.wgsl:154-587
 //
-// B200 layout: one CTA per tile with ONE THREAD PER PIXEL (TS*TS pixels,
-// rounded up to whole warps), per-pixel state in registers instead of shared
-// memory, and the tile's tets processed in batches of kBatch.  For each batch
-// warp 0 stages the 64-byte tet records and 16-byte colours into shared memory
-// with TMA bulk copies (double buffered: batch b+1 is in flight while batch b
-// is composited), one thread per tet derives the per-tet quantities (tile-local
-// projection, inward face planes, colour base), kBatch*TS threads derive the
-// per-row pixel spans exactly as the reference scanline does, and every pixel
-// thread then walks the batch.  Barriers: 3 per batch instead of 3 per tet.
+// B200 layout.  One CTA per tile (or a persistent CTA pulling tiles from a
+// queue), one thread owning each pixel's compositing state in registers, and
+// the tile's tets processed in batches of kBatch = 32:
 //
-// Coverage semantics kept from the reference: the forward includes vertices
-// inside a pixel row (rasterize_compute.wgsl:236-242) and skips pixels whose
+//   stage    warp 0 stages the batch's 64-byte tet records and 16-byte colours
+//            into shared memory with TMA bulk copies (double buffered: batch
+//            b+1 is in flight while batch b is composited);
+//   setup    four threads per tet derive the per-tet quantities (tile-local
+//            vertex projections, inward face planes, colour base);
+//   spans    (tet, row) tasks derive each row's pixel span exactly as the
+//            reference scanline does; every covered (pixel, tet) pair is an
+//            "item", numbered tet-major through per-tet / per-row prefix sums,
+//            and each pixel gets a 32-bit mask of the tets covering it;
+//   phase 0  item-parallel (every thread busy): ray-tet intersection and the
+//            segment integral of each item -> premultiplied colour, depth;
+//   phase 1  pixel-sequential (the only order-dependent part, a few
+//            instructions per item): the pixel's owner walks its mask and
+//            composites front to back (forward) or undoes back to front and
+//            records the restored transmittance and d(logT) (adjoint);
+//   phase 2  adjoint only, item-parallel: the gradient of each item, then a
+//            warp-segmented reduction by tet (items are tet-major, so each
+//            warp's 32 items form contiguous per-tet segments) into a shared
+//            20-float slot per tet, flushed to global memory with five 16-byte
+//            vector atomics per tet and batch.
+// A tet covers ~5-20 of a tile's 144-256 pixels, so working on items keeps
+// all lanes busy where a thread-per-pixel sweep would idle most of them.
+// Batches whose item count exceeds the item buffer run in several sub-batches.
+//
+// Semantics kept from the reference: the forward includes vertices inside a
+// pixel row (rasterize_compute.wgsl:236-242) and skips pixels whose
 // log-transmittance fell below -13.8 (:257-262, :338); the adjoint uses edge
 // crossings only (backward_tiled_compute.wgsl:241-299), takes the ray origin at
 // the camera, undoes every covered tet (clamping log T at 0) and skips the
 // gradient when the restored transmittance is below 1e-6 (:424-437).
-//
-// Adjoint reduction: per tet, each warp sums its lanes' 19 partials with a
-// butterfly reduce-scatter (31 shuffles, lane l ends with partial l), adds them
-// into a shared-memory slot, and after the batch the CTA flushes each tet's
-// 20-float slot to global memory with five 16-byte vector atomics.
 #pragma once
 #include "common.cuh"
 #include "project.cuh"
@@ -34,6 +47,7 @@
 namespace rm {
 
 constexpr int kBatch = 32;
+constexpr int kMom = 24;  // adjoint moments per tet (see phase 2)
 
 enum TileMode : int { kModeForward = 0, kModeBackward = 1, kModeTrain = 2 };
 
@@ -57,97 +71,149 @@ struct TileArgs {
   int persistent;
 };
 
-template <int TS>
+template <int TS, bool AUX>
+struct TileCfg {
+  static constexpr int NT = ((TS * TS + 31) / 32) * 32;
+  static constexpr int NW = NT / 32;
+  static constexpr int CAP = 512;  // items per sub-batch
+  // resident CTAs per SM the register budget is sized for
+  static constexpr int MINB = TS == 16 ? 2 : (TS == 12 ? 4 : 8);
+};
+
+template <int TS, bool AUX>
 struct __align__(16) TileSmem {
   TetRec rec[2][kBatch];
   float4 col[2][kBatch];
   float4 nrm[kBatch][4];  // inward face normal xyz, num = dot(n, va - cam)
   float4 cb[kBatch];      // colour + dot(g, cam - v0), density
-  float4 gr[kBatch];      // g xyz, flip bits (as uint) in w
+  float4 gr[kBatch];      // colour gradient g
+  float mom[kBatch][kMom];  // adjoint moments per tet (phase 2)
+  float4 pdir[TS * TS];   // pixel ray direction
+  float4 pdl[TS * TS];    // pixel dL/dRGB (adjoint)
+  float4 item[TileCfg<TS, AUX>::CAP];   // (cp.rgb, od) -> adjoint: (t_prev, d_od_state, has, -)
+  float4 itemx[TileCfg<TS, AUX>::CAP];  // (t_min, t_max, packed faces | tet | pixel, alpha_t)
   float px[kBatch][4];
   float py[kBatch][4];
-  float4 acc[kBatch][5];  // adjoint partial sums (20 floats per tet)
+  float red[TileCfg<TS, AUX>::NW][32][kMom + 1];  // per-warp transpose (odd row stride)
+  uint32_t toff[kBatch + 1];   // tet-major item offsets
+  uint32_t pmask[TS * TS];
   uint32_t tet[2][kBatch];
   uint32_t behind[kBatch];
   short2 span[kBatch][TS];
+  uint16_t rowpref[kBatch][TS + 1];
+  uint8_t ipix[kBatch * TS * TS];  // pixel of each item of the batch (tet-major)
+  uint8_t flip[kBatch][4];
   uint64_t bar[2];
-  float red[16];
+  float lsum[16];
   uint32_t tile;
-  uint32_t flags;
 };
 
-// Butterfly reduce-scatter over 32 lanes: on return lane l holds the warp sum of v[l]
-// (v[l] for l >= N is taken as zero).
-template <int N>
-__device__ __forceinline__ float warp_reduce_scatter(const float (&v)[N], int lane) {
-  float a[16];
-  const bool b4 = (lane >> 4) & 1;
-#pragma unroll
-  for (int i = 0; i < 16; ++i) {
-    const float lo = i < N ? v[i] : 0.0f;
-    const float hi = (i + 16) < N ? v[i + 16] : 0.0f;
-    const float send = b4 ? lo : hi;
-    const float keep = b4 ? hi : lo;
-    a[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+// Pixel of thread tid: 8x4 pixel blocks per warp for 16x16 tiles, row-major
+// otherwise.  Threads past TS*TS (12x12 tiles use 160 threads) get a real
+// pixel's coordinates but are marked out of tile.
+template <int TS>
+__device__ __forceinline__ void pixel_of_thread(int tid, int& row, int& col, bool& in_tile) {
+  if (TS == 16) {
+    const int w = tid >> 5, l = tid & 31;
+    col = (w & 1) * 8 + (l & 7);
+    row = (w >> 1) * 4 + (l >> 3);
+    in_tile = true;
+  } else {
+    in_tile = tid < TS * TS;
+    const int t = in_tile ? tid : TS * TS - 1;
+    row = t / TS;
+    col = t - (t / TS) * TS;
   }
-  float b[8];
-  const bool b3 = (lane >> 3) & 1;
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const float send = b3 ? a[i] : a[i + 8];
-    const float keep = b3 ? a[i + 8] : a[i];
-    b[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
-  }
-  float c[4];
-  const bool b2 = (lane >> 2) & 1;
-#pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    const float send = b2 ? b[i] : b[i + 4];
-    const float keep = b2 ? b[i + 4] : b[i];
-    c[i] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
-  }
-  float d[2];
-  const bool b1 = (lane >> 1) & 1;
-#pragma unroll
-  for (int i = 0; i < 2; ++i) {
-    const float send = b1 ? c[i] : c[i + 2];
-    const float keep = b1 ? c[i + 2] : c[i];
-    d[i] = keep + __shfl_xor_sync(0xffffffffu, send, 2);
-  }
-  const bool b0 = lane & 1;
-  const float send = b0 ? d[0] : d[1];
-  const float keep = b0 ? d[1] : d[0];
-  return keep + __shfl_xor_sync(0xffffffffu, send, 1);
 }
 
-// dot(n, va - o) for face f of a staged record (ray origin o off the camera).
-__device__ __forceinline__ float face_num_offset(const TetRec& r, int f, const float4& n, float ox, float oy,
-                                                 float oz) {
-  const int ia = kFaces[f][0];
-  const float4 v = ia == 0 ? r.a : (ia == 1 ? r.b : (ia == 2 ? r.c : r.d));
-  return dot3x(n.x, n.y, n.z, fs(v.x, ox), fs(v.y, oy), fs(v.z, oz));
+__device__ __forceinline__ float4 rec_vertex(const TetRec& r, int i) {
+  return i == 0 ? r.a : (i == 1 ? r.b : (i == 2 ? r.c : r.d));
+}
+
+// Ray vs the four inward face planes with the reference's rules
+// (rasterize_compute.wgsl:355-390): |den| < 1e-20 is parallel (outside if
+// num > 0), entry = max t over den > 0 (strict), exit = min t over den < 0.
+// Exact arithmetic: t_max - t_min cancels for thin tets.
+__device__ __forceinline__ bool intersect4(const float4* nrm, const float* num_override, float dx, float dy, float dz,
+                                           float& t_min, float& t_max, int& fmin, int& fmax) {
+  t_min = -3.402823e38f;
+  t_max = 3.402823e38f;
+  fmin = 0;
+  fmax = 0;
+  bool ok = true;
+  int entry = 4;
+#pragma unroll
+  for (int f = 0; f < 4; ++f) {
+    const float4 n = nrm[f];
+    const float den = dot3x(n.x, n.y, n.z, dx, dy, dz);
+    const float num = num_override ? num_override[f] : n.w;
+    if (fabsf(den) < 1e-20f) {
+      if (num > 0.0f) ok = false;
+      continue;
+    }
+    const float t = fdv(num, den);
+    if (den > 0.0f) {
+      if (t > t_min) { t_min = t; fmin = f; entry = f; }
+    } else {
+      if (t < t_max) { t_max = t; fmax = f; }
+    }
+  }
+  if (entry == 4) fmin = 4;  // no entering face (the forward's entry normal is then zero)
+  return ok && t_min < t_max;
+}
+
+// Segment integral of one item (rasterize_compute.wgsl:394-410).
+struct Integral {
+  float csr, csg, csb, cer, ceg, ceb;  // ReLU'd colours at entry / exit
+  float csr_r, csg_r, csb_r, cer_r, ceg_r, ceb_r;
+  float dist, od_raw, od, alpha_t, ph, w0, w1;
+};
+__device__ __forceinline__ void integrate(const float4& cb, float dcdt, float t_min, float t_max, Integral& I,
+                                          float alpha_known = -1.0f) {
+  I.csr_r = cb.x + dcdt * t_min; I.csg_r = cb.y + dcdt * t_min; I.csb_r = cb.z + dcdt * t_min;
+  I.cer_r = cb.x + dcdt * t_max; I.ceg_r = cb.y + dcdt * t_max; I.ceb_r = cb.z + dcdt * t_max;
+  I.csr = fmaxf(I.csr_r, 0.f); I.csg = fmaxf(I.csg_r, 0.f); I.csb = fmaxf(I.csb_r, 0.f);
+  I.cer = fmaxf(I.cer_r, 0.f); I.ceg = fmaxf(I.ceg_r, 0.f); I.ceb = fmaxf(I.ceb_r, 0.f);
+  I.dist = t_max - t_min;
+  I.od_raw = cb.w * I.dist;
+  I.od = clipf(I.od_raw, 1e-8f, 88.0f);
+  I.alpha_t = alpha_known >= 0.0f ? alpha_known : __expf(-I.od);
+  I.ph = fabsf(I.od) < 0.02f ? 1.0f + I.od * (-0.5f + I.od * (1.0f / 6.0f + I.od * (-1.0f / 24.0f)))
+                             : clipf(__fdividef(1.0f - I.alpha_t, I.od), kMinVal, kMaxVal);
+  I.w0 = I.ph - I.alpha_t;
+  I.w1 = 1.0f - I.ph;
+}
+
+// itemx.z packs the adjoint's exit/entry faces, the tet's batch slot and the pixel
+__device__ __forceinline__ uint32_t pack_item(int fmin, int fmax, int k, int p) {
+  return (uint32_t)fmin | ((uint32_t)fmax << 3) | ((uint32_t)k << 5) | ((uint32_t)p << 10);
 }
 
 template <int TS, int MODE, bool AUX>
-__global__ void __launch_bounds__(((TS * TS + 31) / 32) * 32) tile_kernel(TileArgs a) {
-  constexpr int NT = ((TS * TS + 31) / 32) * 32;
-  constexpr int NW = NT / 32;
-  __shared__ TileSmem<TS> s;
+__global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) tile_kernel(TileArgs a) {
+  using Cfg = TileCfg<TS, AUX>;
+  constexpr int NT = Cfg::NT;
+  constexpr int NW = Cfg::NW;
+  constexpr int CAP = Cfg::CAP;
+  extern __shared__ __align__(16) unsigned char tile_smem_raw[];
+  TileSmem<TS, AUX>& s = *reinterpret_cast<TileSmem<TS, AUX>*>(tile_smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int prow = tid / TS < TS ? tid / TS : TS - 1;  // padding threads read a real row, never use it
-  const int pcol = tid - (tid / TS) * TS;
+  int prow, pcol;
+  bool in_tile;
+  pixel_of_thread<TS>(tid, prow, pcol, in_tile);
+  const int pl = prow * TS + pcol;
 
   if (tid == 0) {
     mbar_init(&s.bar[0], 1);
     mbar_init(&s.bar[1], 1);
     fence_mbar_init();
   }
-  for (int i = tid; i < kBatch * 5; i += NT) (&s.acc[0][0])[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+  for (int i = tid; i < kBatch * kMom; i += NT) (&s.mom[0][0])[i] = 0.0f;
   __syncthreads();
-  uint32_t phase[2] = {0u, 0u};
+  uint32_t phase_bits = 0u;  // parity of the next phase of bar[0] (bit 0) and bar[1] (bit 1)
   bool failed = false;
 
-  uint32_t first_tile = blockIdx.x;
+  const uint32_t first_tile = blockIdx.x;
   while (true) {
     if (tid == 0) s.tile = a.persistent ? atomicAdd(&a.counters->tile_ticket, 1u) : first_tile;
     __syncthreads();
@@ -161,14 +227,17 @@ __global__ void __launch_bounds__(((TS * TS + 31) / 32) * 32) tile_kernel(TileAr
     const float tile_ox = (float)(tile_x * (uint32_t)TS), tile_oy = (float)(tile_y * (uint32_t)TS);
     const uint32_t px = tile_x * (uint32_t)TS + (uint32_t)pcol;
     const uint32_t py = tile_y * (uint32_t)TS + (uint32_t)prow;
-    const bool valid = tid < TS * TS && px < (uint32_t)V.W && py < (uint32_t)V.H;
+    const bool valid = in_tile && px < (uint32_t)V.W && py < (uint32_t)V.H;
     const size_t pix = (size_t)V.pix_base + (size_t)py * (size_t)V.W + px;
     const uint2 range = a.ranges[g];
     const uint32_t rs = range.x, re = range.y;
+    // pixels of this tile inside the image
+    const int valid_cols = min(TS, V.W - (int)(tile_x * TS));
+    const int valid_rows = min(TS, V.H - (int)(tile_y * TS));
 
     // pixel ray (rasterize_compute.wgsl:343-349), explicitly rounded: the ray and
-    // the plane hits below feed t_max - t_min, which cancels for thin tets, so
-    // they are evaluated exactly as the reference's left-to-right float math.
+    // the plane hits feed t_max - t_min, which cancels for thin tets, so they
+    // are evaluated exactly as the reference's left-to-right float math.
     float dx, dy, dz;
     {
       float ux = fdv(fs(fa((float)px, 0.5f), V.cx), V.fx);
@@ -182,14 +251,14 @@ __global__ void __launch_bounds__(((TS * TS + 31) / 32) * 32) tile_kernel(TileAr
       l = __fsqrt_rn(dot3x(wx, wy, wz, wx, wy, wz));
       dx = fdv(wx, l); dy = fdv(wy, l); dz = fdv(wz, l);
     }
+    if (in_tile) s.pdir[pl] = make_float4(dx, dy, dz, 0.0f);
     const float camx = V.cam[0], camy = V.cam[1], camz = V.cam[2];
     // forward ray origin cam + dir * min_t (rasterize_compute.wgsl:352); the
     // adjoint keeps the origin at the camera (backward_tiled_compute.wgsl:377)
     const bool has_min_t = V.min_t != 0.0f;
-    const float ox = fa(camx, fm(dx, V.min_t)), oy = fa(camy, fm(dy, V.min_t)), oz = fa(camz, fm(dz, V.min_t));
 
-    // ---------------- per-tile batch machinery ----------------
-    // dir = -1: front-to-back from re-1 down to rs (forward); +1: rs up to re-1 (adjoint)
+    // ---------------- batch machinery ----------------
+    // dir = -1: front-to-back from `first` downwards (forward); +1: upwards (adjoint)
     auto issue = [&](int buf, uint32_t first, int nb, int dir) {
       if (warp == 0) {
         if (lane == 0) {
@@ -209,71 +278,75 @@ __global__ void __launch_bounds__(((TS * TS + 31) / 32) * 32) tile_kernel(TileAr
     };
     // every thread waits on the phase; the outcome is made block-uniform
     auto wait_buf = [&](int buf) {
-      const bool ok = mbar_wait_bounded(&s.bar[buf], phase[buf], 1u << 20);
-      phase[buf] ^= 1u;
+      const bool ok = mbar_wait_bounded(&s.bar[buf], (phase_bits >> buf) & 1u, 1u << 20);
+      phase_bits ^= 1u << buf;
       if (__syncthreads_or(!ok)) {
         failed = true;
         if (tid == 0) atomicOr(&a.counters->err, kErrSpinTimeout);
       }
     };
-    // per-tet setup (thread k < nb) from staged record
+    // per-tet setup, 4 threads per tet (thread q: vertex q and face q); mask clear
     auto setup = [&](int buf, int nb) {
-      if (tid < nb) {
-        const int k = tid;
-        const TetRec r = s.rec[buf][k];
-        const float4 col = s.col[buf][k];
-        const float vx[4] = {r.a.x, r.b.x, r.c.x, r.d.x};
-        const float vy[4] = {r.a.y, r.b.y, r.c.y, r.d.y};
-        const float vz[4] = {r.a.z, r.b.z, r.c.z, r.d.z};
-        float cl[4][4];
+      for (int i = tid; i < TS * TS; i += NT) s.pmask[i] = 0u;
+      for (int task = tid; task < 4 * nb; task += NT) {
+        const int k = task >> 2, q = task & 3;
+        const TetRec& r = s.rec[buf][k];
         bool behind = false;
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          clip_exact(V.vp, vx[q], vy[q], vz[q], cl[q]);
-          behind = behind || (cl[q][3] <= 0.0f);
+        for (int i = 0; i < 4; ++i) {
+          const float4 v = rec_vertex(r, i);
+          const float w = fa(fa(fa(fm(V.vp[3], v.x), fm(V.vp[7], v.y)), fm(V.vp[11], v.z)), V.vp[15]);
+          behind = behind || (w <= 0.0f);
         }
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          float ppx = 0.f, ppy = 0.f;
-          if (!behind) {
-            ppx = fs(fm(fm(fa(fdv(cl[q][0], cl[q][3]), 1.0f), 0.5f), V.Wf), tile_ox);
-            ppy = fs(fm(fm(fs(1.0f, fdv(cl[q][1], cl[q][3])), 0.5f), V.Hf), tile_oy);
-          }
-          s.px[k][q] = ppx;
-          s.py[k][q] = ppy;
+        // tile-local projection for the in-tile coverage (rasterize_compute.wgsl:152-167).
+        // Fast arithmetic is safe here: spans include pixels up to 0.001 px
+        // outside the silhouette, where the exact ray test misses anyway, so a
+        // last-bit difference in a span end changes no pixel value.
+        const float4 vq = rec_vertex(r, q);
+        float ppx = 0.f, ppy = 0.f;
+        if (!behind) {
+          const float cx_ = V.vp[0] * vq.x + V.vp[4] * vq.y + V.vp[8] * vq.z + V.vp[12];
+          const float cy_ = V.vp[1] * vq.x + V.vp[5] * vq.y + V.vp[9] * vq.z + V.vp[13];
+          const float cw_ = V.vp[3] * vq.x + V.vp[7] * vq.y + V.vp[11] * vq.z + V.vp[15];
+          const float iw = __fdividef(1.0f, cw_);
+          ppx = (cx_ * iw + 1.0f) * 0.5f * V.Wf - tile_ox;
+          ppy = (1.0f - cy_ * iw) * 0.5f * V.Hf - tile_oy;
         }
-        s.behind[k] = behind ? 1u : 0u;
-        uint32_t flips = 0u;
-#pragma unroll
-        for (int f = 0; f < 4; ++f) {
-          const int ia = kFaces[f][0], ib = kFaces[f][1], ic = kFaces[f][2], io = kFaces[f][3];
-          const float e1x = fs(vx[ic], vx[ia]), e1y = fs(vy[ic], vy[ia]), e1z = fs(vz[ic], vz[ia]);
-          const float e2x = fs(vx[ib], vx[ia]), e2y = fs(vy[ib], vy[ia]), e2z = fs(vz[ib], vz[ia]);
-          float nx = fs(fm(e1y, e2z), fm(e1z, e2y));
-          float ny = fs(fm(e1z, e2x), fm(e1x, e2z));
-          float nz = fs(fm(e1x, e2y), fm(e1y, e2x));
-          const float ox = fs(vx[io], vx[ia]), oy = fs(vy[io], vy[ia]), oz = fs(vz[io], vz[ia]);
-          if (dot3x(nx, ny, nz, ox, oy, oz) < 0.0f) {
-            nx = -nx; ny = -ny; nz = -nz;
-            flips |= 1u << f;
-          }
-          const float num = dot3x(nx, ny, nz, fs(vx[ia], camx), fs(vy[ia], camy), fs(vz[ia], camz));
-          s.nrm[k][f] = make_float4(nx, ny, nz, num);
+        s.px[k][q] = ppx;
+        s.py[k][q] = ppy;
+        // face q (intersect.wgsl FACES): normal cross(vc - va, vb - va), flipped inward
+        const float4 va = rec_vertex(r, kFaces[q][0]), vb = rec_vertex(r, kFaces[q][1]);
+        const float4 vc = rec_vertex(r, kFaces[q][2]), vo = rec_vertex(r, kFaces[q][3]);
+        const float e1x = fs(vc.x, va.x), e1y = fs(vc.y, va.y), e1z = fs(vc.z, va.z);
+        const float e2x = fs(vb.x, va.x), e2y = fs(vb.y, va.y), e2z = fs(vb.z, va.z);
+        float nx = fs(fm(e1y, e2z), fm(e1z, e2y));
+        float ny = fs(fm(e1z, e2x), fm(e1x, e2z));
+        float nz = fs(fm(e1x, e2y), fm(e1y, e2x));
+        const bool flip = dot3x(nx, ny, nz, fs(vo.x, va.x), fs(vo.y, va.y), fs(vo.z, va.z)) < 0.0f;
+        if (flip) { nx = -nx; ny = -ny; nz = -nz; }
+        s.nrm[k][q] = make_float4(nx, ny, nz, dot3x(nx, ny, nz, fs(va.x, camx), fs(va.y, camy), fs(va.z, camz)));
+        s.flip[k][q] = flip ? 1 : 0;
+        if (q == 0) {
+          s.behind[k] = behind ? 1u : 0u;
+          const float4 col = s.col[buf][k];
+          const float gx = r.b.w, gy = r.c.w, gz = r.d.w;
+          const float boff = dot3x(gx, gy, gz, fs(camx, r.a.x), fs(camy, r.a.y), fs(camz, r.a.z));
+          s.cb[k] = make_float4(fa(col.x, boff), fa(col.y, boff), fa(col.z, boff), r.a.w);
+          s.gr[k] = make_float4(gx, gy, gz, 0.0f);
         }
-        const float gx = r.b.w, gy = r.c.w, gz = r.d.w;
-        const float boff = dot3x(gx, gy, gz, fs(camx, vx[0]), fs(camy, vy[0]), fs(camz, vz[0]));
-        s.cb[k] = make_float4(fa(col.x, boff), fa(col.y, boff), fa(col.z, boff), r.a.w);
-        s.gr[k] = make_float4(gx, gy, gz, __uint_as_float(flips));
       }
     };
-    // per-(tet,row) pixel spans, exact arithmetic.  vertex_rows selects the
-    // forward rule (rasterize_compute.wgsl:170-275); without it this is the
-    // adjoint rule (backward_tiled_compute.wgsl:241-299).
+    // per-(tet,row) pixel spans -> span table.  vertex_rows selects the forward
+    // rule (rasterize_compute.wgsl:170-275); without it this is the adjoint rule
+    // (backward_tiled_compute.wgsl:241-299).
+    // Rows/columns outside the image are dropped (their pixels are skipped by
+    // the reference too, rasterize_compute.wgsl:332).
     auto spans = [&](int nb, bool vertex_rows) {
       for (int task = tid; task < nb * TS; task += NT) {
         const int k = task / TS, row = task - (task / TS) * TS;
-        float xl = 1e10f, xr = -1e10f;
-        if (!s.behind[k]) {
+        short2 sp = make_short2(0, -1);
+        if (!s.behind[k] && row < valid_rows) {
+          float xl = 1e10f, xr = -1e10f;
           const float yc = fa((float)row, 0.5f);
           const int ei[6] = {0, 0, 0, 1, 1, 2};
           const int ej[6] = {1, 2, 3, 2, 3, 3};
@@ -281,8 +354,8 @@ __global__ void __launch_bounds__(((TS * TS + 31) / 32) * 32) tile_kernel(TileAr
           for (int e = 0; e < 6; ++e) {
             const float yi = s.py[k][ei[e]], yj = s.py[k][ej[e]];
             if ((yi <= yc && yj > yc) || (yj <= yc && yi > yc)) {
-              const float t = fdv(fs(yc, yi), fs(yj, yi));
-              const float x = fa(s.px[k][ei[e]], fm(t, fs(s.px[k][ej[e]], s.px[k][ei[e]])));
+              const float t = __fdividef(yc - yi, yj - yi);
+              const float x = s.px[k][ei[e]] + t * (s.px[k][ej[e]] - s.px[k][ei[e]]);
               xl = fminf(xl, x);
               xr = fmaxf(xr, x);
             }
@@ -298,14 +371,122 @@ __global__ void __launch_bounds__(((TS * TS + 31) / 32) * 32) tile_kernel(TileAr
               }
             }
           }
-        }
-        short2 sp = make_short2(0, -1);
-        if (xl <= xr) {
-          const int32_t lo = max(__float2int_rz(ceilf(fs(fs(xl, 0.5f), 0.001f))), 0);
-          const int32_t hi = min(__float2int_rz(floorf(fa(fs(xr, 0.5f), 0.001f))), TS - 1);
-          if (lo <= hi) sp = make_short2((short)lo, (short)hi);
+          if (xl <= xr) {
+            const int32_t lo = max(__float2int_rz(ceilf(xl - 0.5f - 0.001f)), 0);
+            const int32_t hi = min(min(__float2int_rz(floorf(xr - 0.5f + 0.001f)), TS - 1), valid_cols - 1);
+            if (lo <= hi) sp = make_short2((short)lo, (short)hi);
+          }
         }
         s.span[k][row] = sp;
+      }
+    };
+    // per-tet row prefix sums and tet-major item offsets (after spans)
+    auto prefixes = [&](int nb) {
+      uint32_t cnt = 0;
+      if (tid < nb) {
+        const int k = tid;
+        uint32_t acc = 0;
+        s.rowpref[k][0] = 0;
+        for (int r = 0; r < TS; ++r) {
+          const short2 sp = s.span[k][r];
+          acc += (uint32_t)max(sp.y - sp.x + 1, 0);
+          s.rowpref[k][r + 1] = (uint16_t)acc;
+        }
+        cnt = acc;
+      }
+      if (warp == 0) {  // exclusive scan over the batch's tets (nb <= 32)
+        uint32_t x = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+          if (lane >= o) x += y;
+        }
+        if (lane < nb) s.toff[lane + 1] = x;
+        if (lane == 0) s.toff[0] = 0u;
+      }
+    };
+    // item pixel ids (tet-major) and per-pixel coverage masks
+    auto fill = [&](int nb) {
+      for (int task = tid; task < nb * TS; task += NT) {
+        const int k = task / TS, row = task - (task / TS) * TS;
+        const short2 sp = s.span[k][row];
+        if (sp.x > sp.y) continue;
+        const uint32_t base = s.toff[k] + s.rowpref[k][row];
+        for (int c = sp.x; c <= sp.y; ++c) {
+          s.ipix[base + (uint32_t)(c - sp.x)] = (uint8_t)(row * TS + c);
+          atomicOr(&s.pmask[row * TS + c], 1u << k);
+        }
+      }
+    };
+    // tet-major item gi -> (tet k, pixel index in tile)
+    auto decode = [&](uint32_t gi, int k0, int k1, int& k, int& p) {
+      int lo = k0, hi = k1 - 1;  // largest k with toff[k] <= gi
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s.toff[mid] <= gi) lo = mid; else hi = mid - 1;
+      }
+      k = lo;
+      p = s.ipix[gi];
+    };
+    // item index of (tet k, this thread's pixel) inside the current sub-batch
+    auto item_of = [&](int k, uint32_t base) -> uint32_t {
+      return s.toff[k] - base + s.rowpref[k][prow] + (uint32_t)(pcol - s.span[k][prow].x);
+    };
+    // greedy sub-batch end: largest k1 with toff[k1] - toff[k0] <= CAP (>= k0+1)
+    auto sub_end = [&](int k0, int nb) -> int {
+      int k1 = k0 + 1;
+      while (k1 < nb && s.toff[k1 + 1] - s.toff[k0] <= (uint32_t)CAP) ++k1;
+      return k1;
+    };
+    // phase 0: item-parallel intersection + integral.  clip_lo: 0 for the
+    // forward (rasterize_compute.wgsl:409), -1e20 for the adjoint (:411).
+    auto phase0 = [&](int buf, int k0, int k1, bool fwd) {
+      const uint32_t base = s.toff[k0];
+      const uint32_t n_items = s.toff[k1] - base;
+      for (uint32_t i = tid; i < n_items; i += NT) {
+        int k, p;
+        decode(base + i, k0, k1, k, p);
+        const float4 d = s.pdir[p];
+        float numo[4];
+        const float* nump = nullptr;
+        float bcr_o = 0.f, bcg_o = 0.f, bcb_o = 0.f;
+        if (fwd && has_min_t) {
+          // origin cam + d*min_t: num = dot(n, va - o), base offset dot(g, o - v0)
+          const float oxp = fa(camx, fm(d.x, V.min_t)), oyp = fa(camy, fm(d.y, V.min_t)),
+                      ozp = fa(camz, fm(d.z, V.min_t));
+          const TetRec& rr = s.rec[buf][k];
+#pragma unroll
+          for (int f = 0; f < 4; ++f) {
+            const float4 n = s.nrm[k][f];
+            const float4 v = rec_vertex(rr, kFaces[f][0]);
+            numo[f] = dot3x(n.x, n.y, n.z, fs(v.x, oxp), fs(v.y, oyp), fs(v.z, ozp));
+          }
+          nump = numo;
+          const float4 gg = s.gr[k];
+          const float bo = dot3x(gg.x, gg.y, gg.z, fs(oxp, rr.a.x), fs(oyp, rr.a.y), fs(ozp, rr.a.z));
+          const float4 cc = s.col[buf][k];
+          bcr_o = fa(cc.x, bo); bcg_o = fa(cc.y, bo); bcb_o = fa(cc.z, bo);
+        }
+        float t_min, t_max;
+        int fmin, fmax;
+        float4 out = make_float4(0.f, 0.f, 0.f, -1.0f);  // od < 0: the ray misses
+        float4 out2 = make_float4(0.f, 0.f, 0.f, 0.f);
+        const bool hit = intersect4(s.nrm[k], nump, d.x, d.y, d.z, t_min, t_max, fmin, fmax);
+        if (hit) {
+          float4 cb = s.cb[k];
+          if (fwd && has_min_t) cb = make_float4(bcr_o, bcg_o, bcb_o, cb.w);
+          const float4 gg = s.gr[k];
+          const float dcdt = dot3x(gg.x, gg.y, gg.z, d.x, d.y, d.z);
+          Integral I;
+          integrate(cb, dcdt, t_min, t_max, I);
+          const float lo = fwd ? 0.f : kMinVal;
+          out = make_float4(clipf(I.cer * I.w0 + I.csr * I.w1, lo, kMaxVal),
+                            clipf(I.ceg * I.w0 + I.csg * I.w1, lo, kMaxVal),
+                            clipf(I.ceb * I.w0 + I.csb * I.w1, lo, kMaxVal), I.od);
+          out2 = make_float4(t_min, t_max, __uint_as_float(pack_item(fmin, fmax, k, p)), I.alpha_t);
+        }
+        s.item[i] = out;
+        if (AUX || !fwd) s.itemx[i] = out2;
       }
     };
 
@@ -316,8 +497,7 @@ __global__ void __launch_bounds__(((TS * TS + 31) / 32) * 32) tile_kernel(TileAr
     if (MODE == kModeForward || MODE == kModeTrain) {
       bool alive = valid;
       if (re > rs) {
-        int nb0 = (int)min((uint32_t)kBatch, re - rs);
-        issue(0, re - 1u, nb0, -1);
+        issue(0, re - 1u, (int)min((uint32_t)kBatch, re - rs), -1);
         int b = 0;
         for (uint32_t hi = re; hi > rs;) {
           const int buf = b & 1;
@@ -330,85 +510,67 @@ __global__ void __launch_bounds__(((TS * TS + 31) / 32) * 32) tile_kernel(TileAr
           __syncthreads();
           spans(nb, true);
           __syncthreads();
-          if (alive) {
-            for (int k = 0; k < nb; ++k) {
-              const short2 sp = s.span[k][prow];
-              if (pcol < sp.x || pcol > sp.y) continue;
-              if (logT < -13.8f) { alive = false; break; }
-              float t_min = -3.402823e38f, t_max = 3.402823e38f;
-              int entry = 4;
-              bool ok = true;
-#pragma unroll
-              for (int f = 0; f < 4; ++f) {
-                const float4 n = s.nrm[k][f];
-                const float den = dot3x(n.x, n.y, n.z, dx, dy, dz);
-                const float num = has_min_t ? face_num_offset(s.rec[buf][k], f, n, ox, oy, oz) : n.w;
-                if (fabsf(den) < 1e-20f) {
-                  if (num > 0.0f) ok = false;
-                  continue;
-                }
-                const float t = fdv(num, den);
-                if (den > 0.0f) {
-                  if (t > t_min) { t_min = t; entry = f; }
-                } else {
-                  if (t < t_max) t_max = t;
-                }
-              }
-              if (!(ok && t_min < t_max)) continue;
-              const float4 cb = s.cb[k];
-              const float4 gg = s.gr[k];
-              const float dcdt = dot3x(gg.x, gg.y, gg.z, dx, dy, dz);
-              float bcr = cb.x, bcg = cb.y, bcb = cb.z;
-              if (has_min_t) {  // base offset at the shifted origin, dot(g, o - v0)
-                const TetRec& rr = s.rec[buf][k];
-                const float bo = dot3x(gg.x, gg.y, gg.z, fs(ox, rr.a.x), fs(oy, rr.a.y), fs(oz, rr.a.z));
-                const float4 cc = s.col[buf][k];
-                bcr = fa(cc.x, bo); bcg = fa(cc.y, bo); bcb = fa(cc.z, bo);
-              }
-              const float csr = fmaxf(bcr + dcdt * t_min, 0.f), csg = fmaxf(bcg + dcdt * t_min, 0.f),
-                          csb = fmaxf(bcb + dcdt * t_min, 0.f);
-              const float cer = fmaxf(bcr + dcdt * t_max, 0.f), ceg = fmaxf(bcg + dcdt * t_max, 0.f),
-                          ceb = fmaxf(bcb + dcdt * t_max, 0.f);
-              const float dist = t_max - t_min;
-              const float od = clipf(cb.w * dist, 1e-8f, 88.0f);
-              const float alpha_t = __expf(-od);
-              const float ph = fabsf(od) < 0.02f ? 1.0f + od * (-0.5f + od * (1.0f / 6.0f + od * (-1.0f / 24.0f)))
-                                                 : clipf(__fdividef(1.0f - alpha_t, od), kMinVal, kMaxVal);
-              const float w0 = ph - alpha_t, w1 = 1.0f - ph;
-              const float cpr = clipf(cer * w0 + csr * w1, 0.f, kMaxVal);
-              const float cpg = clipf(ceg * w0 + csg * w1, 0.f, kMaxVal);
-              const float cpb = clipf(ceb * w0 + csb * w1, 0.f, kMaxVal);
-              const float Tj = __expf(fmaxf(logT, -88.0f));
-              if (Tj >= 1e-6f) {
-                Cr += cpr * Tj; Cg += cpg * Tj; Cb += cpb * Tj;
-                logT -= od;
-                if (AUX) {
-                  const float alpha = 1.0f - alpha_t;
-                  float enx = 0.f, eny = 0.f, enz = 0.f;
-                  if (entry < 4) {
-                    const float4 n = s.nrm[k][entry];
-                    const float l = sqrtf(n.x * n.x + n.y * n.y + n.z * n.z);
-                    enx = -n.x / l; eny = -n.y / l; enz = -n.z / l;
+          prefixes(nb);
+          __syncthreads();
+          fill(nb);
+          __syncthreads();
+          for (int k0 = 0; k0 < nb;) {
+            const int k1 = sub_end(k0, nb);
+            phase0(buf, k0, k1, true);
+            __syncthreads();
+            // phase 1: composite this pixel's items nearest first
+            if (alive) {
+              const uint32_t base = s.toff[k0];
+              uint32_t m = s.pmask[pl] & ((k1 >= 32 ? 0xffffffffu : ((1u << k1) - 1u)) & ~((1u << k0) - 1u));
+              while (m) {
+                const int k = __ffs(m) - 1;
+                m &= m - 1u;
+                if (logT < -13.8f) { alive = false; break; }
+                const uint32_t it = item_of(k, base);
+                const float4 c = s.item[it];
+                if (c.w < 0.0f) continue;  // ray miss
+                const float Tj = __expf(fmaxf(logT, -88.0f));
+                if (Tj >= 1e-6f) {
+                  Cr += c.x * Tj; Cg += c.y * Tj; Cb += c.z * Tj;
+                  logT -= c.w;
+                  if (AUX) {
+                    const float4 c2 = s.itemx[it];
+                    const float t_min = c2.x, t_max = c2.y, alpha_t = c2.w;
+                    const int entry = (int)(__float_as_uint(c2.z) & 7u);
+                    const float od = c.w;
+                    const float ph = fabsf(od) < 0.02f
+                                         ? 1.0f + od * (-0.5f + od * (1.0f / 6.0f + od * (-1.0f / 24.0f)))
+                                         : clipf(__fdividef(1.0f - alpha_t, od), kMinVal, kMaxVal);
+                    const float w0 = ph - alpha_t, w1 = 1.0f - ph;
+                    const float alpha = 1.0f - alpha_t;
+                    float enx = 0.f, eny = 0.f, enz = 0.f;
+                    if (entry < 4) {
+                      const float4 n = s.nrm[k][entry];
+                      const float l = sqrtf(n.x * n.x + n.y * n.y + n.z * n.z);
+                      enx = -n.x / l; eny = -n.y / l; enz = -n.z / l;
+                    }
+                    const float ta = Tj * alpha;
+                    nd0 += ta * enx; nd1 += ta * eny; nd2 += ta * enz;
+                    nd3 += Tj * (w0 * t_max + w1 * t_min);
+                    const float wt = alpha * Tj;
+                    const float cmid = (t_min + t_max) * 0.5f;
+                    const float wc = wt * cmid;
+                    en0 += wt;
+                    en1 += wt > 1e-20f ? wt * logf(wt) : 0.0f;
+                    en2 += wt * cmid;
+                    en3 += wc > 1e-20f ? wc * logf(wc) : 0.0f;
                   }
-                  const float ta = Tj * alpha;
-                  nd0 += ta * enx; nd1 += ta * eny; nd2 += ta * enz;
-                  nd3 += Tj * (w0 * t_max + w1 * t_min);
-                  const float wt = alpha * Tj;
-                  const float cmid = (t_min + t_max) * 0.5f;
-                  const float wc = wt * cmid;
-                  en0 += wt;
-                  en1 += wt > 1e-20f ? wt * logf(wt) : 0.0f;
-                  en2 += wt * cmid;
-                  en3 += wc > 1e-20f ? wc * logf(wc) : 0.0f;
                 }
               }
             }
+            __syncthreads();
+            k0 = k1;
           }
           hi = next_hi;
           ++b;
           // all pixels saturated: the remaining tets would all be skipped
           if (__syncthreads_count(alive && logT >= -13.8f) == 0) {
-            if (hi > rs) { wait_buf(buf ^ 1); }  // drain the prefetch already in flight
+            if (hi > rs) wait_buf(buf ^ 1);  // drain the prefetch already in flight
             break;
           }
         }
@@ -444,15 +606,15 @@ __global__ void __launch_bounds__(((TS * TS + 31) / 32) * 32) tile_kernel(TileAr
             lsum = er * er + eg * eg + eb * eb;
           }
           logT = logf(fmaxf(1.0f - A, 1e-20f));
-          dlogT = -0.0f * (1.0f - A);
+          dlogT = -0.0f * (1.0f - A);  // the loss has no alpha term (loss_compute.wgsl:71)
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, o);
-        if (lane == 0) s.red[warp] = lsum;
+        if (lane == 0) s.lsum[warp] = lsum;
         __syncthreads();
         if (tid == 0) {
           double tot = 0.0;
-          for (int w = 0; w < NW; ++w) tot += (double)s.red[w];
+          for (int w = 0; w < NW; ++w) tot += (double)s.lsum[w];
           atomicAdd(&a.counters->loss[view], tot);
         }
       } else if (valid) {
@@ -463,10 +625,10 @@ __global__ void __launch_bounds__(((TS * TS + 31) / 32) * 32) tile_kernel(TileAr
         dlogT = -dl.w * (1.0f - img.w);
         dlr = dl.x; dlg = dl.y; dlb = dl.z;
       }
+      if (in_tile) s.pdl[pl] = make_float4(dlr, dlg, dlb, 0.0f);
       if (re > rs) {
-        int nb0 = (int)min((uint32_t)kBatch, re - rs);
         __syncthreads();
-        issue(0, rs, nb0, +1);
+        issue(0, rs, (int)min((uint32_t)kBatch, re - rs), +1);
         int b = 0;
         for (uint32_t lo = rs; lo < re;) {
           const int buf = b & 1;
@@ -479,171 +641,213 @@ __global__ void __launch_bounds__(((TS * TS + 31) / 32) * 32) tile_kernel(TileAr
           __syncthreads();
           spans(nb, false);  // adjoint: edge crossings only
           __syncthreads();
-          for (int k = 0; k < nb; ++k) {
-            float c19[19];
-#pragma unroll
-            for (int q = 0; q < 19; ++q) c19[q] = 0.0f;
-            bool has = false;
-            const short2 sp = s.span[k][prow];
-            if (valid && pcol >= sp.x && pcol <= sp.y) {
-              float t_min = -3.402823e38f, t_max = 3.402823e38f;
-              int min_face = 0, max_face = 0;
-              bool ok = true;
-#pragma unroll
-              for (int f = 0; f < 4; ++f) {
-                const float4 n = s.nrm[k][f];
-                const float den = dot3x(n.x, n.y, n.z, dx, dy, dz);
-                if (fabsf(den) < 1e-20f) {
-                  if (n.w > 0.0f) ok = false;
-                  continue;
-                }
-                const float t = fdv(n.w, den);
-                if (den > 0.0f) {
-                  if (t > t_min) { t_min = t; min_face = f; }
-                } else {
-                  if (t < t_max) { t_max = t; max_face = f; }
-                }
-              }
-              if (ok && t_min < t_max) {
-                const float4 cb = s.cb[k];
-                const float4 gg = s.gr[k];
-                const float dens = cb.w;
-                const float dcdt = dot3x(gg.x, gg.y, gg.z, dx, dy, dz);
-                const float csr_r = cb.x + dcdt * t_min, csg_r = cb.y + dcdt * t_min, csb_r = cb.z + dcdt * t_min;
-                const float cer_r = cb.x + dcdt * t_max, ceg_r = cb.y + dcdt * t_max, ceb_r = cb.z + dcdt * t_max;
-                const float csr = fmaxf(csr_r, 0.f), csg = fmaxf(csg_r, 0.f), csb = fmaxf(csb_r, 0.f);
-                const float cer = fmaxf(cer_r, 0.f), ceg = fmaxf(ceg_r, 0.f), ceb = fmaxf(ceb_r, 0.f);
-                const float dist = t_max - t_min;
-                const float od_raw = dens * dist;
-                const float od = clipf(od_raw, 1e-8f, 88.0f);
-                const float alpha_t = __expf(-od);
-                const float ph = fabsf(od) < 0.02f ? 1.0f + od * (-0.5f + od * (1.0f / 6.0f + od * (-1.0f / 24.0f)))
-                                                   : clipf(__fdividef(1.0f - alpha_t, od), kMinVal, kMaxVal);
-                const float w0 = ph - alpha_t, w1 = 1.0f - ph;
-                const float cpr = clipf(cer * w0 + csr * w1, kMinVal, kMaxVal);
-                const float cpg = clipf(ceg * w0 + csg * w1, kMinVal, kMaxVal);
-                const float cpb = clipf(ceb * w0 + csb * w1, kMinVal, kMaxVal);
-                const float prev_logT = fminf(logT + od, 0.0f);
+          prefixes(nb);
+          __syncthreads();
+          fill(nb);
+          __syncthreads();
+          for (int k0 = 0; k0 < nb;) {
+            const int k1 = sub_end(k0, nb);
+            const uint32_t base = s.toff[k0];
+            const uint32_t n_items = s.toff[k1] - base;
+            phase0(buf, k0, k1, false);
+            __syncthreads();
+            // phase 1: undo this pixel's items farthest first
+            if (valid) {
+              uint32_t m = s.pmask[pl] & ((k1 >= 32 ? 0xffffffffu : ((1u << k1) - 1u)) & ~((1u << k0) - 1u));
+              while (m) {
+                const int k = __ffs(m) - 1;
+                m &= m - 1u;
+                const uint32_t it = item_of(k, base);
+                const float4 c = s.item[it];
+                if (c.w < 0.0f) continue;  // ray miss: no state change, no gradient
+                const float prev_logT = fminf(logT + c.w, 0.0f);
                 const float t_prev = __expf(fmaxf(prev_logT, -88.0f));
-                Cr -= cpr * t_prev; Cg -= cpg * t_prev; Cb -= cpb * t_prev;
+                Cr -= c.x * t_prev; Cg -= c.y * t_prev; Cb -= c.z * t_prev;
                 logT = prev_logT;
                 if (t_prev >= 1e-6f) {
-                  has = true;
-                  const float dcpr = clipf(dlr * t_prev, kMinVal, kMaxVal);
-                  const float dcpg = clipf(dlg * t_prev, kMinVal, kMaxVal);
-                  const float dcpb = clipf(dlb * t_prev, kMinVal, kMaxVal);
                   const float d_od_state = -dlogT;
-                  dlogT = clipf(dlogT + (dlr * cpr + dlg * cpg + dlb * cpb) * t_prev, kMinVal, kMaxVal);
+                  dlogT = clipf(dlogT + (dlr * c.x + dlg * c.y + dlb * c.z) * t_prev, kMinVal, kMaxVal);
+                  s.item[it] = make_float4(t_prev, d_od_state, 1.0f, 0.0f);
+                } else {
+                  s.item[it].w = -1.0f;  // no gradient
+                }
+              }
+            }
+            __syncthreads();
+            // phase 2: per-item adjoint, item-parallel in 32-item warp chunks.
+            // Vertex gradients enter through moments: for a face (a, b, c) with
+            // unflipped normal n, hit h = cam + d t and s = dT / (n.d), the item
+            // adds s (a-h) x (c-a) to vertex b, s (a-h) x (a-b) to c and
+            // s ((a-h) x (b-c) + n) to a (backward_tiled_compute.wgsl:506-533).
+            // Since a - h = (a - cam) - t d, the sum over a tet's items needs only
+            // S = sum s and P = sum s t d per face; the vertex gradients are
+            // rebuilt from them once per tet at flush time.  Moments per item:
+            //  [0] density  [1..3] base colour  [4] sum(sb)  [5..7] d * d(dc/dt)
+            //  [8 + 4f] S_f  [9 + 4f .. 11 + 4f] P_f   (f = face 0..3)
+            float(*red)[kMom + 1] = s.red[warp];
+            const uint32_t n_valid = n_items;
+            for (uint32_t chunk = (uint32_t)warp * 32u; chunk < n_items; chunk += (uint32_t)NT) {
+              const uint32_t i = chunk + (uint32_t)lane;
+              float m[kMom];
+#pragma unroll
+              for (int q = 0; q < kMom; ++q) m[q] = 0.0f;
+              int k = -1;
+              if (i < n_valid) {
+                const float4 st = s.item[i];
+                const float4 ix = s.itemx[i];
+                const uint32_t pk = __float_as_uint(ix.z);
+                k = (int)((pk >> 5) & 31u);
+                if (st.w >= 0.0f && st.z > 0.5f) {
+                  const int p = (int)(pk >> 10);
+                  int fmin = (int)(pk & 7u);
+                  const int fmax = (int)((pk >> 3) & 3u);
+                  if (fmin == 4) fmin = 0;  // reference keeps min_face = 0 when no face enters
+                  const float t_min = ix.x, t_max = ix.y;
+                  const float t_prev = st.x, d_od_state = st.y;
+                  const float4 d = s.pdir[p];
+                  const float4 dlv = s.pdl[p];
+                  const float4 cb = s.cb[k];
+                  const float4 gg = s.gr[k];
+                  const float dcdt = dot3x(gg.x, gg.y, gg.z, d.x, d.y, d.z);
+                  Integral I;
+                  integrate(cb, dcdt, t_min, t_max, I, ix.w);
+                  const float dcpr = clipf(dlv.x * t_prev, kMinVal, kMaxVal);
+                  const float dcpg = clipf(dlv.y * t_prev, kMinVal, kMaxVal);
+                  const float dcpb = clipf(dlv.z * t_prev, kMinVal, kMaxVal);
                   float dph;
-                  if (fabsf(od) < 0.02f) dph = -0.5f + od * (1.0f / 3.0f + od * (-1.0f / 8.0f + od * (1.0f / 30.0f)));
-                  else dph = clipf(__fdividef(alpha_t * (od + 1.0f) - 1.0f, od * od), kMinVal, kMaxVal);
-                  const float dw0 = dph + alpha_t, dw1 = -dph;
-                  const float d_od_int = dcpr * (cer * dw0 + csr * dw1) + dcpg * (ceg * dw0 + csg * dw1) +
-                                         dcpb * (ceb * dw0 + csb * dw1);
+                  if (fabsf(I.od) < 0.02f)
+                    dph = -0.5f + I.od * (1.0f / 3.0f + I.od * (-1.0f / 8.0f + I.od * (1.0f / 30.0f)));
+                  else
+                    dph = clipf(__fdividef(I.alpha_t * (I.od + 1.0f) - 1.0f, I.od * I.od), kMinVal, kMaxVal);
+                  const float dw0 = dph + I.alpha_t, dw1 = -dph;
+                  const float d_od_int = dcpr * (I.cer * dw0 + I.csr * dw1) + dcpg * (I.ceg * dw0 + I.csg * dw1) +
+                                         dcpb * (I.ceb * dw0 + I.csb * dw1);
                   const float d_od = clipf(d_od_state + d_od_int, kMinVal, kMaxVal);
-                  const bool active = (od_raw >= 1e-8f) && (od_raw <= 88.0f);
+                  const bool active = (I.od_raw >= 1e-8f) && (I.od_raw <= 88.0f);
                   const float d_od_raw = active ? d_od : 0.0f;
-                  const float d_dens = clipf(d_od_raw * dist, kMinVal, kMaxVal);
-                  const float d_dist = clipf(d_od_raw * dens, kMinVal, kMaxVal);
+                  const float d_dist = clipf(d_od_raw * cb.w, kMinVal, kMaxVal);
                   float d_tmin = -d_dist, d_tmax = d_dist;
-                  const float dsr = csr_r > 0.f ? dcpr * w1 : 0.f, dsg = csg_r > 0.f ? dcpg * w1 : 0.f,
-                              dsb = csb_r > 0.f ? dcpb * w1 : 0.f;
-                  const float der = cer_r > 0.f ? dcpr * w0 : 0.f, deg = ceg_r > 0.f ? dcpg * w0 : 0.f,
-                              deb = ceb_r > 0.f ? dcpb * w0 : 0.f;
+                  const float dsr = I.csr_r > 0.f ? dcpr * I.w1 : 0.f, dsg = I.csg_r > 0.f ? dcpg * I.w1 : 0.f,
+                              dsb = I.csb_r > 0.f ? dcpb * I.w1 : 0.f;
+                  const float der = I.cer_r > 0.f ? dcpr * I.w0 : 0.f, deg = I.ceg_r > 0.f ? dcpg * I.w0 : 0.f,
+                              deb = I.ceb_r > 0.f ? dcpb * I.w0 : 0.f;
                   const float dbr = dsr + der, dbg = dsg + deg, dbb = dsb + deb;
                   const float ss = dsr + dsg + dsb, se = der + deg + deb;
                   const float d_dcdt = ss * t_min + se * t_max;
                   d_tmin += ss * dcdt;
                   d_tmax += se * dcdt;
-                  const float sb = dbr + dbg + dbb;
-                  const TetRec& r = s.rec[buf][k];
-                  const float vx[4] = {r.a.x, r.b.x, r.c.x, r.d.x};
-                  const float vy[4] = {r.a.y, r.b.y, r.c.y, r.d.y};
-                  const float vz[4] = {r.a.z, r.b.z, r.c.z, r.d.z};
-                  c19[0] = clipf(d_dens, kMinVal, kMaxVal);
-                  c19[1] = clipf(dbr, kMinVal, kMaxVal);
-                  c19[2] = clipf(dbg, kMinVal, kMaxVal);
-                  c19[3] = clipf(dbb, kMinVal, kMaxVal);
-                  c19[4] = clipf((camx - vx[0]) * sb + dx * d_dcdt, kMinVal, kMaxVal);
-                  c19[5] = clipf((camy - vy[0]) * sb + dy * d_dcdt, kMinVal, kMaxVal);
-                  c19[6] = clipf((camz - vz[0]) * sb + dz * d_dcdt, kMinVal, kMaxVal);
-                  float dv[12];
-#pragma unroll
-                  for (int q = 0; q < 12; ++q) dv[q] = 0.0f;
-                  const uint32_t flips = __float_as_uint(gg.w);
+                  m[0] = clipf(d_od_raw * I.dist, kMinVal, kMaxVal);
+                  m[1] = clipf(dbr, kMinVal, kMaxVal);
+                  m[2] = clipf(dbg, kMinVal, kMaxVal);
+                  m[3] = clipf(dbb, kMinVal, kMaxVal);
+                  m[4] = dbr + dbg + dbb;
+                  m[5] = d.x * d_dcdt;
+                  m[6] = d.y * d_dcdt;
+                  m[7] = d.z * d_dcdt;
 #pragma unroll
                   for (int side = 0; side < 2; ++side) {
-                    const int f = side == 0 ? min_face : max_face;
+                    const int f = side == 0 ? fmin : fmax;
                     const float dt = side == 0 ? d_tmin : d_tmax;
                     const float tt = side == 0 ? t_min : t_max;
-                    const int ia = kFaces[f][0], ib = kFaces[f][1], ic = kFaces[f][2];
                     const float4 nf = s.nrm[k][f];
-                    const float sg = ((flips >> f) & 1u) ? -1.0f : 1.0f;  // undo the inward flip
-                    const float nx = sg * nf.x, ny = sg * nf.y, nz = sg * nf.z;
-                    const float den = nx * dx + ny * dy + nz * dz;
+                    const float den = (s.flip[k][f] ? -1.0f : 1.0f) * (nf.x * d.x + nf.y * d.y + nf.z * d.z);
                     const float inv_den = fabsf(den) < kTiny ? clipf(1.0f / kTiny, kMinVal, kMaxVal)
-                                                             : clipf(1.0f / den, kMinVal, kMaxVal);
-                    const float hx = camx + dx * tt, hy = camy + dy * tt, hz = camz + dz * tt;
-                    const float ahx = vx[ia] - hx, ahy = vy[ia] - hy, ahz = vz[ia] - hz;
-                    // dt/dva = (cross(va-hit, vb-vc) + n) / den
-                    float ux = vx[ib] - vx[ic], uy = vy[ib] - vy[ic], uz = vz[ib] - vz[ic];
-                    float gax = (ahy * uz - ahz * uy + nx) * inv_den, gay = (ahz * ux - ahx * uz + ny) * inv_den,
-                          gaz = (ahx * uy - ahy * ux + nz) * inv_den;
-                    // dt/dvb = cross(va-hit, vc-va) / den
-                    ux = vx[ic] - vx[ia]; uy = vy[ic] - vy[ia]; uz = vz[ic] - vz[ia];
-                    float gbx = (ahy * uz - ahz * uy) * inv_den, gby = (ahz * ux - ahx * uz) * inv_den,
-                          gbz = (ahx * uy - ahy * ux) * inv_den;
-                    // dt/dvc = cross(va-hit, va-vb) / den
-                    ux = vx[ia] - vx[ib]; uy = vy[ia] - vy[ib]; uz = vz[ia] - vz[ib];
-                    float gcx = (ahy * uz - ahz * uy) * inv_den, gcy = (ahz * ux - ahx * uz) * inv_den,
-                          gcz = (ahx * uy - ahy * ux) * inv_den;
+                                                             : clipf(__fdividef(1.0f, den), kMinVal, kMaxVal);
+                    const float sv = dt * inv_den, st_ = sv * tt;
 #pragma unroll
                     for (int q = 0; q < 4; ++q) {
-                      if (q == ia) {
-                        dv[3 * q] += clipf(gax * dt, kMinVal, kMaxVal);
-                        dv[3 * q + 1] += clipf(gay * dt, kMinVal, kMaxVal);
-                        dv[3 * q + 2] += clipf(gaz * dt, kMinVal, kMaxVal);
-                      } else if (q == ib) {
-                        dv[3 * q] += clipf(gbx * dt, kMinVal, kMaxVal);
-                        dv[3 * q + 1] += clipf(gby * dt, kMinVal, kMaxVal);
-                        dv[3 * q + 2] += clipf(gbz * dt, kMinVal, kMaxVal);
-                      } else if (q == ic) {
-                        dv[3 * q] += clipf(gcx * dt, kMinVal, kMaxVal);
-                        dv[3 * q + 1] += clipf(gcy * dt, kMinVal, kMaxVal);
-                        dv[3 * q + 2] += clipf(gcz * dt, kMinVal, kMaxVal);
+                      if (q == f) {
+                        m[8 + 4 * q] += sv;
+                        m[9 + 4 * q] += st_ * d.x;
+                        m[10 + 4 * q] += st_ * d.y;
+                        m[11 + 4 * q] += st_ * d.z;
                       }
                     }
                   }
-                  dv[0] += -gg.x * sb;
-                  dv[1] += -gg.y * sb;
-                  dv[2] += -gg.z * sb;
-#pragma unroll
-                  for (int q = 0; q < 12; ++q) c19[7 + q] = clipf(dv[q], kMinVal, kMaxVal);
                 }
               }
-            }
-            const unsigned m = __ballot_sync(0xffffffffu, has);
-            if (m) {
-              float* acc = reinterpret_cast<float*>(&s.acc[k][0]);
-              if (__popc(m) <= 2) {
-                if (has) {
+              // transpose through shared memory; lane q < kMom then walks column q
+              // over the chunk's rows, flushing a partial sum at every tet boundary
 #pragma unroll
-                  for (int q = 0; q < 19; ++q) atomicAdd(&acc[q], c19[q]);
+              for (int q = 0; q < kMom; ++q) red[lane][q] = m[q];
+              const int kp = __shfl_up_sync(0xffffffffu, k, 1);
+              const unsigned heads = __ballot_sync(0xffffffffu, k >= 0 && (lane == 0 || kp != k));
+              const int n_rows = __popc(__ballot_sync(0xffffffffu, k >= 0));  // valid rows come first
+              red[lane][kMom] = __int_as_float(k);
+              __syncwarp();
+              if (lane < kMom && heads) {
+                float sum = 0.0f;
+                int cur = __float_as_int(red[0][kMom]);
+                for (int row = 0; row < n_rows; ++row) {
+                  if (row > 0 && ((heads >> row) & 1u)) {
+                    if (sum != 0.0f) atomicAdd(&s.mom[cur][lane], sum);
+                    sum = 0.0f;
+                    cur = __float_as_int(red[row][kMom]);
+                  }
+                  sum += red[row][lane];
                 }
-              } else {
-                const float r = warp_reduce_scatter<19>(c19, lane);
-                if (lane < 19) atomicAdd(&acc[lane], r);
+                if (sum != 0.0f) atomicAdd(&s.mom[cur][lane], sum);
               }
+              __syncwarp();
             }
+            __syncthreads();
+            k0 = k1;
           }
-          __syncthreads();
-          // flush this batch's per-tet sums (five 16-byte vector atomics per tet)
-          for (int q = tid; q < nb * 5; q += NT) {
-            const int k = q / 5, c = q - (q / 5) * 5;
-            const float4 v4 = s.acc[k][c];
-            if (v4.x != 0.f || v4.y != 0.f || v4.z != 0.f || v4.w != 0.f) {
-              atomicAdd(reinterpret_cast<float4*>(a.grad_slot + (size_t)s.tet[buf][k] * kGradSlot) + c, v4);
-              s.acc[k][c] = make_float4(0.f, 0.f, 0.f, 0.f);
+          // flush: rebuild each tet's 19 gradients from its moments and add them to
+          // the global slot (five 16-byte vector atomics per tet)
+          if (tid < nb) {
+            const int k = tid;
+            float* mm = s.mom[k];
+            bool any = false;
+#pragma unroll
+            for (int q = 0; q < kMom; ++q) any = any || (mm[q] != 0.0f);
+            if (any) {
+              const TetRec& r = s.rec[buf][k];
+              const float4 gg = s.gr[k];
+              float out[20];
+              out[0] = mm[0];
+              out[1] = mm[1]; out[2] = mm[2]; out[3] = mm[3];
+              const float sb = mm[4];
+              out[4] = clipf((camx - r.a.x) * sb + mm[5], kMinVal, kMaxVal);
+              out[5] = clipf((camy - r.a.y) * sb + mm[6], kMinVal, kMaxVal);
+              out[6] = clipf((camz - r.a.z) * sb + mm[7], kMinVal, kMaxVal);
+              float dv[12];
+              dv[0] = -gg.x * sb; dv[1] = -gg.y * sb; dv[2] = -gg.z * sb;
+#pragma unroll
+              for (int q = 3; q < 12; ++q) dv[q] = 0.0f;
+#pragma unroll
+              for (int f = 0; f < 4; ++f) {
+                const float S = mm[8 + 4 * f], Px = mm[9 + 4 * f], Py = mm[10 + 4 * f], Pz = mm[11 + 4 * f];
+                if (S == 0.0f && Px == 0.0f && Py == 0.0f && Pz == 0.0f) continue;
+                const int ia = kFaces[f][0], ib = kFaces[f][1], ic = kFaces[f][2];
+                const float4 va = rec_vertex(r, ia), vb = rec_vertex(r, ib), vc = rec_vertex(r, ic);
+                const float4 nf = s.nrm[k][f];
+                const float sg = s.flip[k][f] ? -1.0f : 1.0f;
+                // w = (a - cam) S - P
+                const float wx = (va.x - camx) * S - Px, wy = (va.y - camy) * S - Py, wz = (va.z - camz) * S - Pz;
+                float ux = vc.x - va.x, uy = vc.y - va.y, uz = vc.z - va.z;  // c - a
+                const float bx = wy * uz - wz * uy, by = wz * ux - wx * uz, bz = wx * uy - wy * ux;
+                ux = va.x - vb.x; uy = va.y - vb.y; uz = va.z - vb.z;  // a - b
+                const float cx = wy * uz - wz * uy, cy = wz * ux - wx * uz, cz = wx * uy - wy * ux;
+                const float ax = sg * nf.x * S - bx - cx, ay = sg * nf.y * S - by - cy, az = sg * nf.z * S - bz - cz;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                  if (q == ia) { dv[3 * q] += ax; dv[3 * q + 1] += ay; dv[3 * q + 2] += az; }
+                  if (q == ib) { dv[3 * q] += bx; dv[3 * q + 1] += by; dv[3 * q + 2] += bz; }
+                  if (q == ic) { dv[3 * q] += cx; dv[3 * q + 1] += cy; dv[3 * q + 2] += cz; }
+                }
+              }
+#pragma unroll
+              for (int q = 0; q < 12; ++q) out[7 + q] = clipf(dv[q], kMinVal, kMaxVal);
+              out[19] = 0.0f;
+              float4* dst = reinterpret_cast<float4*>(a.grad_slot + (size_t)s.tet[buf][k] * kGradSlot);
+#pragma unroll
+              for (int c = 0; c < 5; ++c) {
+                const float4 v4 = make_float4(out[4 * c], out[4 * c + 1], out[4 * c + 2], out[4 * c + 3]);
+                if (v4.x != 0.f || v4.y != 0.f || v4.z != 0.f || v4.w != 0.f) atomicAdd(dst + c, v4);
+              }
+#pragma unroll
+              for (int q = 0; q < kMom; ++q) mm[q] = 0.0f;
             }
           }
           __syncthreads();

@@ -164,3 +164,22 @@ def test_split_step_equals_train_step(c1_scene):
     for k in pa:
         assert rel_l2(pa[k], pb[k]) <= 1e-3, k
     assert a.step == b.step == 1
+
+
+def test_known_tet_matches_golden():
+    """The CUDA path reproduces the committed golden fixture (tests/golden)."""
+    import os
+
+    from conftest import ROOT
+
+    g = np.load(os.path.join(ROOT, "tests", "golden", "known_tet.npz"))
+    sc = known_tet_scene()
+    cam = _cams_known()
+    r = make_renderer(sc, cam)
+    img = r.forward_tiled(cam.cam_pos, cam.vp, cam.c2w_intrinsics)
+    np.testing.assert_array_equal(r.debug_tiles_touched(), g["tiles_touched"])
+    tiles, tets = r.debug_pairs()
+    np.testing.assert_array_equal(tiles, g["tiles"])
+    np.testing.assert_array_equal(tets, g["tets"])
+    np.testing.assert_array_equal(r.debug_ranges(), g["ranges"])
+    assert np.abs(img - g["image"]).max() <= IMG_TOL
