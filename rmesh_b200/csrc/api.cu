@@ -91,7 +91,7 @@ struct RmeshCtx {
 
   // per-run
   DevBuf views_d, counters_d, hp_d, sort_state, sort_status, scan_status;
-  DevBuf vis_key, vis_val, vis_tet, vis_cnt, vis_proj, vis_key_alt, vis_val_alt, tiles_touched;
+  DevBuf vis_key, vis_val, vis_tet, vis_cnt, vis_proj, vis_view, vis_key_alt, vis_val_alt, tiles_touched;
   DevBuf pair_key, pair_val, pair_key_alt, pair_val_alt, ranges;
   DevBuf rgba, aux, dl, gt, out_a, out_b, out_c, out_d;
   uint64_t cap_pairs = 0;
@@ -265,6 +265,7 @@ int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t
   CKR(ensure_buf(c, c->vis_tet, items * 4));
   CKR(ensure_buf(c, c->vis_cnt, items * 4));
   CKR(ensure_buf(c, c->vis_proj, items * 32));
+  CKR(ensure_buf(c, c->vis_view, items * sizeof(TetView)));
   CKR(ensure_buf(c, c->tiles_touched, items * 4));
   if (c->cap_pairs == 0) c->cap_pairs = std::max<uint64_t>(8 * items, 1u << 16);
   CKR(ensure_buf(c, c->pair_key, c->cap_pairs * 4));
@@ -350,8 +351,8 @@ int run_bin(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t tota
     pa.vis_tet = c->vis_tet.as<uint32_t>();
     pa.vis_cnt = c->vis_cnt.as<uint32_t>();
     pa.vis_proj = c->vis_proj.as<float4>();
-    pa.vis_view = nullptr;
-    pa.color4 = nullptr;
+    pa.vis_view = c->vis_view.as<TetView>();
+    pa.color4 = c->color4.as<float4>();
     pa.color_view_stride = 0;
     pa.tiles_touched = c->tiles_touched.as<uint32_t>();
     pa.status = status;
@@ -376,7 +377,6 @@ int run_bin(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t tota
     ea.views = views_dev;
     ea.tet_key_sorted = tk;
     ea.tet_val_sorted = tv;
-    ea.vis_tet = c->vis_tet.as<uint32_t>();
     ea.vis_cnt = c->vis_cnt.as<uint32_t>();
     ea.vis_proj = c->vis_proj.as<float4>();
     ea.n_vis_ptr = &cnt->n_vis;
@@ -448,6 +448,7 @@ TileArgs base_tile_args(RmeshCtx* c, const ViewParams* views_dev, int n_views, u
   ta.n_tiles = n_tiles;
   ta.ranges = c->ranges.as<uint2>();
   ta.pair_val = c->sorted_pair_val;
+  ta.vis_view = c->vis_view.as<TetView>();
   ta.rec = c->rec.as<TetRec>();
   ta.color4 = c->color4.as<float4>();
   ta.color_view_stride = 0;
@@ -848,7 +849,7 @@ int rmesh_get_info(RmeshCtx* c, RmeshInfo* info) {
                    &c->m_dens, &c->v_dens, &c->m_cgrad, &c->v_cgrad, &c->m_base, &c->v_base, &c->rec,
                    &c->color4, &c->grad_slot, &c->csr_off, &c->csr_ref, &c->views_d, &c->counters_d, &c->hp_d,
                    &c->sort_state, &c->sort_status, &c->scan_status, &c->vis_key, &c->vis_val, &c->vis_tet,
-                   &c->vis_cnt, &c->vis_proj, &c->vis_key_alt, &c->vis_val_alt, &c->tiles_touched, &c->pair_key,
+                   &c->vis_cnt, &c->vis_proj, &c->vis_view, &c->vis_key_alt, &c->vis_val_alt, &c->tiles_touched, &c->pair_key,
                    &c->pair_val, &c->pair_key_alt, &c->pair_val_alt, &c->ranges, &c->rgba, &c->aux, &c->dl,
                    &c->gt, &c->out_a, &c->out_b, &c->out_c, &c->out_d};
   for (DevBuf* b : all) info->device_bytes += b->bytes;
@@ -999,7 +1000,17 @@ int rmesh_debug_pairs(RmeshCtx* c, uint32_t* tiles, uint32_t* tets, uint64_t cap
   *n = c->last_n_pairs;
   const uint64_t k = std::min<uint64_t>(cap, c->last_n_pairs);
   if (k && tiles) CK(cudaMemcpyAsync(tiles, c->sorted_pair_key, k * 4, cudaMemcpyDefault, c->stream));
-  if (k && tets) CK(cudaMemcpyAsync(tets, c->sorted_pair_val, k * 4, cudaMemcpyDefault, c->stream));
+  if (k && tets) {
+    // the pair payload is the compact (view, tet) index: map it to tet ids in
+    // the pair buffer the sort left free
+    uint32_t* scratch = c->sorted_pair_val == c->pair_val.as<uint32_t>() ? c->pair_val_alt.as<uint32_t>()
+                                                                          : c->pair_val.as<uint32_t>();
+    const int blocks = (int)std::min<uint64_t>((k + 255) / 256, (uint64_t)c->num_sms * 8);
+    pair_tets_kernel<<<blocks, 256, 0, c->stream>>>(c->sorted_pair_key, c->sorted_pair_val, c->vis_tet.as<uint32_t>(),
+                                                     k, scratch);
+    CKL();
+    CK(cudaMemcpyAsync(tets, scratch, k * 4, cudaMemcpyDefault, c->stream));
+  }
   CK(cudaStreamSynchronize(c->stream));
   return RMESH_OK;
 }

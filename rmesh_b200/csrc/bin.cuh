@@ -24,12 +24,11 @@ struct EmitArgs {
   const ViewParams* views;
   const unsigned long long* tet_key_sorted;  // (view << 32) | ~depth, sorted
   const uint32_t* tet_val_sorted;            // compact index j
-  const uint32_t* vis_tet;
   const uint32_t* vis_cnt;
   const float4* vis_proj;
   const uint32_t* n_vis_ptr;
   uint32_t* pair_key;   // global tile id
-  uint32_t* pair_val;   // tet id
+  uint32_t* pair_val;   // compact index j of the (view, tet) entry (its per-view record)
   unsigned long long cap;
   unsigned long long* status;
   uint32_t* ticket;
@@ -80,7 +79,6 @@ __global__ void __launch_bounds__(256) emit_kernel(EmitArgs a) {
 
   const uint32_t view = (uint32_t)(a.tet_key_sorted[k] >> 32);
   const ViewParams& V = a.views[view];
-  const uint32_t tet = a.vis_tet[j];
   const float4 q0 = a.vis_proj[2 * j], q1 = a.vis_proj[2 * j + 1];
   const float px[4] = {q0.x, q0.z, q1.x, q1.z};
   const float py[4] = {q0.y, q0.w, q1.y, q1.w};
@@ -91,7 +89,7 @@ __global__ void __launch_bounds__(256) emit_kernel(EmitArgs a) {
       const unsigned long long w = off + local;
       if (w < a.cap) {
         a.pair_key[w] = V.tile_base + ty * (uint32_t)V.tiles_x + tx;
-        a.pair_val[w] = tet;
+        a.pair_val[w] = j;
       } else {
         overflow = true;
       }
@@ -134,6 +132,16 @@ __global__ void __launch_bounds__(256) ranges_kernel(const uint32_t* __restrict_
       if (!(last_of_view && counters->shortfall[v])) ranges[key].y = (uint32_t)(idx + 1);
     }
   }
+}
+
+// Debug view of the sorted pairs: the pair payload is the compact (view, tet)
+// index; map it back to the tet id (sentinel slots keep the reference's 0).
+__global__ void __launch_bounds__(256) pair_tets_kernel(const uint32_t* __restrict__ keys,
+                                                        const uint32_t* __restrict__ vals,
+                                                        const uint32_t* __restrict__ vis_tet, uint64_t n,
+                                                        uint32_t* __restrict__ out) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    out[i] = keys[i] == kSentinel ? 0u : vis_tet[vals[i]];
 }
 
 }  // namespace rm

@@ -9,11 +9,11 @@
 // queue), one thread owning each pixel's compositing state in registers, and
 // the tile's tets processed in batches of kBatch = 32:
 //
-//   stage    warp 0 stages the batch's 64-byte tet records and 16-byte colours
-//            into shared memory with TMA bulk copies (double buffered: batch
-//            b+1 is in flight while batch b is composited);
-//   setup    four threads per tet derive the per-tet quantities (tile-local
-//            vertex projections, inward face planes, colour base);
+//   stage    warp 0 stages the batch's 144-byte per-view tet records (face
+//            planes, colour base, projected vertices; written once per
+//            (view, tet) by the project kernel) into shared memory with TMA
+//            bulk copies (double buffered: batch b+1 is in flight while batch
+//            b is composited);
 //   spans    (tet, row) tasks derive each row's pixel span exactly as the
 //            reference scanline does; every covered (pixel, tet) pair is an
 //            "item", numbered tet-major through per-tet / per-row prefix sums,
@@ -26,9 +26,10 @@
 //            records the restored transmittance and d(logT) (adjoint);
 //   phase 2  adjoint only, item-parallel: the gradient of each item, then a
 //            warp-segmented reduction by tet (items are tet-major, so each
-//            warp's 32 items form contiguous per-tet segments) into a shared
-//            20-float slot per tet, flushed to global memory with five 16-byte
-//            vector atomics per tet and batch.
+//            warp's 32 items form contiguous per-tet segments) into 24 shared
+//            moments per tet, from which the tet's 19 gradients are rebuilt and
+//            flushed to global memory with five 16-byte vector atomics per tet
+//            and batch.
 // A tet covers ~5-20 of a tile's 144-256 pixels, so working on items keeps
 // all lanes busy where a thread-per-pixel sweep would idle most of them.
 // Batches whose item count exceeds the item buffer run in several sub-batches.
@@ -47,7 +48,8 @@
 namespace rm {
 
 constexpr int kBatch = 32;
-constexpr int kMom = 24;  // adjoint moments per tet (see phase 2)
+constexpr int kMom = 24;      // adjoint moments per tet (see phase 2)
+constexpr int kMomHalf = 12;  // moments transposed per reduction pass
 
 enum TileMode : int { kModeForward = 0, kModeBackward = 1, kModeTrain = 2 };
 
@@ -56,8 +58,9 @@ struct TileArgs {
   int n_views;
   uint32_t n_tiles;
   const uint2* ranges;
-  const uint32_t* pair_val;
-  const TetRec* rec;
+  const uint32_t* pair_val;    // index of the pair's per-view tet record
+  const TetView* vis_view;     // per-(view, visible tet) records
+  const TetRec* rec;           // tet records (vertex positions for the gradient flush)
   const float4* color4;
   uint32_t color_view_stride;  // 0: colours shared by all views; M: per-view colours
   float* rgba;                 // [pixels][4] (forward output; optional in train mode)
@@ -82,27 +85,18 @@ struct TileCfg {
 
 template <int TS, bool AUX>
 struct __align__(16) TileSmem {
-  TetRec rec[2][kBatch];
-  float4 col[2][kBatch];
-  float4 nrm[kBatch][4];  // inward face normal xyz, num = dot(n, va - cam)
-  float4 cb[kBatch];      // colour + dot(g, cam - v0), density
-  float4 gr[kBatch];      // colour gradient g
+  TetView view[2][kBatch];  // staged per-view tet records (double buffered)
   float mom[kBatch][kMom];  // adjoint moments per tet (phase 2)
-  float4 pdir[TS * TS];   // pixel ray direction
-  float4 pdl[TS * TS];    // pixel dL/dRGB (adjoint)
+  float4 pdir[TS * TS];     // pixel ray direction
+  float4 pdl[TS * TS];      // pixel dL/dRGB (adjoint)
   float4 item[TileCfg<TS, AUX>::CAP];   // (cp.rgb, od) -> adjoint: (t_prev, d_od_state, has, -)
   float4 itemx[TileCfg<TS, AUX>::CAP];  // (t_min, t_max, packed faces | tet | pixel, alpha_t)
-  float px[kBatch][4];
-  float py[kBatch][4];
-  float red[TileCfg<TS, AUX>::NW][32][kMom + 1];  // per-warp transpose (odd row stride)
+  float red[TileCfg<TS, AUX>::NW][32][kMomHalf + 1];  // per-warp transpose (odd row stride)
   uint32_t toff[kBatch + 1];   // tet-major item offsets
   uint32_t pmask[TS * TS];
-  uint32_t tet[2][kBatch];
-  uint32_t behind[kBatch];
   short2 span[kBatch][TS];
   uint16_t rowpref[kBatch][TS + 1];
   uint8_t ipix[kBatch * TS * TS];  // pixel of each item of the batch (tet-major)
-  uint8_t flip[kBatch][4];
   uint64_t bar[2];
   float lsum[16];
   uint32_t tile;
@@ -128,6 +122,9 @@ __device__ __forceinline__ void pixel_of_thread(int tid, int& row, int& col, boo
 
 __device__ __forceinline__ float4 rec_vertex(const TetRec& r, int i) {
   return i == 0 ? r.a : (i == 1 ? r.b : (i == 2 ? r.c : r.d));
+}
+__device__ __forceinline__ bool face_flipped(const TetView& tv, int f) {
+  return (__float_as_uint(tv.gm.w) >> f) & 1u;
 }
 
 // Ray vs the four inward face planes with the reference's rules
@@ -263,16 +260,12 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
       if (warp == 0) {
         if (lane == 0) {
           fence_proxy_async_smem();
-          mbar_arrive_expect_tx(&s.bar[buf], (uint32_t)nb * (uint32_t)(sizeof(TetRec) + sizeof(float4)));
+          mbar_arrive_expect_tx(&s.bar[buf], (uint32_t)nb * (uint32_t)sizeof(TetView));
         }
         __syncwarp();
         if (lane < nb) {
           const uint32_t pos = dir < 0 ? first - (uint32_t)lane : first + (uint32_t)lane;
-          const uint32_t t = a.pair_val[pos];
-          s.tet[buf][lane] = t;
-          bulk_copy_g2s(&s.rec[buf][lane], a.rec + t, (uint32_t)sizeof(TetRec), &s.bar[buf]);
-          bulk_copy_g2s(&s.col[buf][lane], a.color4 + (size_t)a.color_view_stride * view + t,
-                        (uint32_t)sizeof(float4), &s.bar[buf]);
+          bulk_copy_g2s(&s.view[buf][lane], a.vis_view + a.pair_val[pos], (uint32_t)sizeof(TetView), &s.bar[buf]);
         }
       }
     };
@@ -285,77 +278,35 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
         if (tid == 0) atomicOr(&a.counters->err, kErrSpinTimeout);
       }
     };
-    // per-tet setup, 4 threads per tet (thread q: vertex q and face q); mask clear
-    auto setup = [&](int buf, int nb) {
-      for (int i = tid; i < TS * TS; i += NT) s.pmask[i] = 0u;
-      for (int task = tid; task < 4 * nb; task += NT) {
-        const int k = task >> 2, q = task & 3;
-        const TetRec& r = s.rec[buf][k];
-        bool behind = false;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          const float4 v = rec_vertex(r, i);
-          const float w = fa(fa(fa(fm(V.vp[3], v.x), fm(V.vp[7], v.y)), fm(V.vp[11], v.z)), V.vp[15]);
-          behind = behind || (w <= 0.0f);
-        }
-        // tile-local projection for the in-tile coverage (rasterize_compute.wgsl:152-167).
-        // Fast arithmetic is safe here: spans include pixels up to 0.001 px
-        // outside the silhouette, where the exact ray test misses anyway, so a
-        // last-bit difference in a span end changes no pixel value.
-        const float4 vq = rec_vertex(r, q);
-        float ppx = 0.f, ppy = 0.f;
-        if (!behind) {
-          const float cx_ = V.vp[0] * vq.x + V.vp[4] * vq.y + V.vp[8] * vq.z + V.vp[12];
-          const float cy_ = V.vp[1] * vq.x + V.vp[5] * vq.y + V.vp[9] * vq.z + V.vp[13];
-          const float cw_ = V.vp[3] * vq.x + V.vp[7] * vq.y + V.vp[11] * vq.z + V.vp[15];
-          const float iw = __fdividef(1.0f, cw_);
-          ppx = (cx_ * iw + 1.0f) * 0.5f * V.Wf - tile_ox;
-          ppy = (1.0f - cy_ * iw) * 0.5f * V.Hf - tile_oy;
-        }
-        s.px[k][q] = ppx;
-        s.py[k][q] = ppy;
-        // face q (intersect.wgsl FACES): normal cross(vc - va, vb - va), flipped inward
-        const float4 va = rec_vertex(r, kFaces[q][0]), vb = rec_vertex(r, kFaces[q][1]);
-        const float4 vc = rec_vertex(r, kFaces[q][2]), vo = rec_vertex(r, kFaces[q][3]);
-        const float e1x = fs(vc.x, va.x), e1y = fs(vc.y, va.y), e1z = fs(vc.z, va.z);
-        const float e2x = fs(vb.x, va.x), e2y = fs(vb.y, va.y), e2z = fs(vb.z, va.z);
-        float nx = fs(fm(e1y, e2z), fm(e1z, e2y));
-        float ny = fs(fm(e1z, e2x), fm(e1x, e2z));
-        float nz = fs(fm(e1x, e2y), fm(e1y, e2x));
-        const bool flip = dot3x(nx, ny, nz, fs(vo.x, va.x), fs(vo.y, va.y), fs(vo.z, va.z)) < 0.0f;
-        if (flip) { nx = -nx; ny = -ny; nz = -nz; }
-        s.nrm[k][q] = make_float4(nx, ny, nz, dot3x(nx, ny, nz, fs(va.x, camx), fs(va.y, camy), fs(va.z, camz)));
-        s.flip[k][q] = flip ? 1 : 0;
-        if (q == 0) {
-          s.behind[k] = behind ? 1u : 0u;
-          const float4 col = s.col[buf][k];
-          const float gx = r.b.w, gy = r.c.w, gz = r.d.w;
-          const float boff = dot3x(gx, gy, gz, fs(camx, r.a.x), fs(camy, r.a.y), fs(camz, r.a.z));
-          s.cb[k] = make_float4(fa(col.x, boff), fa(col.y, boff), fa(col.z, boff), r.a.w);
-          s.gr[k] = make_float4(gx, gy, gz, 0.0f);
-        }
-      }
-    };
     // per-(tet,row) pixel spans -> span table.  vertex_rows selects the forward
     // rule (rasterize_compute.wgsl:170-275); without it this is the adjoint rule
     // (backward_tiled_compute.wgsl:241-299).
     // Rows/columns outside the image are dropped (their pixels are skipped by
     // the reference too, rasterize_compute.wgsl:332).
-    auto spans = [&](int nb, bool vertex_rows) {
+    // The tile-local vertex projections use fast arithmetic (the record's
+    // px/py, minus the tile origin): spans include pixels up to 0.001 px
+    // outside the silhouette, where the exact ray test misses anyway, so a
+    // last-bit difference in a span end changes no pixel value.
+    auto spans = [&](int buf, int nb, bool vertex_rows) {
+      for (int i = tid; i < TS * TS; i += NT) s.pmask[i] = 0u;
       for (int task = tid; task < nb * TS; task += NT) {
         const int k = task / TS, row = task - (task / TS) * TS;
         short2 sp = make_short2(0, -1);
-        if (!s.behind[k] && row < valid_rows) {
+        const TetView& tv = s.view[buf][k];
+        if (!((__float_as_uint(tv.gm.w) >> 4) & 1u) && row < valid_rows) {
+          const float4 gx4 = tv.px, gy4 = tv.py;
+          const float vpx[4] = {gx4.x - tile_ox, gx4.y - tile_ox, gx4.z - tile_ox, gx4.w - tile_ox};
+          const float vpy[4] = {gy4.x - tile_oy, gy4.y - tile_oy, gy4.z - tile_oy, gy4.w - tile_oy};
           float xl = 1e10f, xr = -1e10f;
           const float yc = fa((float)row, 0.5f);
           const int ei[6] = {0, 0, 0, 1, 1, 2};
           const int ej[6] = {1, 2, 3, 2, 3, 3};
 #pragma unroll
           for (int e = 0; e < 6; ++e) {
-            const float yi = s.py[k][ei[e]], yj = s.py[k][ej[e]];
+            const float yi = vpy[ei[e]], yj = vpy[ej[e]];
             if ((yi <= yc && yj > yc) || (yj <= yc && yi > yc)) {
               const float t = __fdividef(yc - yi, yj - yi);
-              const float x = s.px[k][ei[e]] + t * (s.px[k][ej[e]] - s.px[k][ei[e]]);
+              const float x = vpx[ei[e]] + t * (vpx[ej[e]] - vpx[ei[e]]);
               xl = fminf(xl, x);
               xr = fmaxf(xr, x);
             }
@@ -364,10 +315,10 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
             const float blo = fs(yc, 0.5f), bhi = fa(yc, 0.5f);
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-              const float vyq = s.py[k][q];
+              const float vyq = vpy[q];
               if (vyq >= blo && vyq < bhi) {
-                xl = fminf(xl, s.px[k][q]);
-                xr = fmaxf(xr, s.px[k][q]);
+                xl = fminf(xl, vpx[q]);
+                xr = fmaxf(xr, vpx[q]);
               }
             }
           }
@@ -450,32 +401,34 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
         float numo[4];
         const float* nump = nullptr;
         float bcr_o = 0.f, bcg_o = 0.f, bcb_o = 0.f;
+        const TetView& tv = s.view[buf][k];
         if (fwd && has_min_t) {
           // origin cam + d*min_t: num = dot(n, va - o), base offset dot(g, o - v0)
           const float oxp = fa(camx, fm(d.x, V.min_t)), oyp = fa(camy, fm(d.y, V.min_t)),
                       ozp = fa(camz, fm(d.z, V.min_t));
-          const TetRec& rr = s.rec[buf][k];
+          const uint32_t tet = tv.meta.x;
+          const TetRec rr = a.rec[tet];
 #pragma unroll
           for (int f = 0; f < 4; ++f) {
-            const float4 n = s.nrm[k][f];
+            const float4 n = tv.nrm[f];
             const float4 v = rec_vertex(rr, kFaces[f][0]);
             numo[f] = dot3x(n.x, n.y, n.z, fs(v.x, oxp), fs(v.y, oyp), fs(v.z, ozp));
           }
           nump = numo;
-          const float4 gg = s.gr[k];
+          const float4 gg = tv.gm;
           const float bo = dot3x(gg.x, gg.y, gg.z, fs(oxp, rr.a.x), fs(oyp, rr.a.y), fs(ozp, rr.a.z));
-          const float4 cc = s.col[buf][k];
+          const float4 cc = a.color4[(size_t)a.color_view_stride * view + tet];
           bcr_o = fa(cc.x, bo); bcg_o = fa(cc.y, bo); bcb_o = fa(cc.z, bo);
         }
         float t_min, t_max;
         int fmin, fmax;
         float4 out = make_float4(0.f, 0.f, 0.f, -1.0f);  // od < 0: the ray misses
         float4 out2 = make_float4(0.f, 0.f, 0.f, 0.f);
-        const bool hit = intersect4(s.nrm[k], nump, d.x, d.y, d.z, t_min, t_max, fmin, fmax);
+        const bool hit = intersect4(tv.nrm, nump, d.x, d.y, d.z, t_min, t_max, fmin, fmax);
         if (hit) {
-          float4 cb = s.cb[k];
+          float4 cb = tv.cb;
           if (fwd && has_min_t) cb = make_float4(bcr_o, bcg_o, bcb_o, cb.w);
-          const float4 gg = s.gr[k];
+          const float4 gg = tv.gm;
           const float dcdt = dot3x(gg.x, gg.y, gg.z, d.x, d.y, d.z);
           Integral I;
           integrate(cb, dcdt, t_min, t_max, I);
@@ -506,9 +459,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
           wait_buf(buf);
           if (failed) break;
           if (next_hi > rs) issue(buf ^ 1, next_hi - 1u, (int)min((uint32_t)kBatch, next_hi - rs), -1);
-          setup(buf, nb);
-          __syncthreads();
-          spans(nb, true);
+          spans(buf, nb, true);
           __syncthreads();
           prefixes(nb);
           __syncthreads();
@@ -545,7 +496,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
                     const float alpha = 1.0f - alpha_t;
                     float enx = 0.f, eny = 0.f, enz = 0.f;
                     if (entry < 4) {
-                      const float4 n = s.nrm[k][entry];
+                      const float4 n = s.view[buf][k].nrm[entry];
                       const float l = sqrtf(n.x * n.x + n.y * n.y + n.z * n.z);
                       enx = -n.x / l; eny = -n.y / l; enz = -n.z / l;
                     }
@@ -637,9 +588,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
           wait_buf(buf);
           if (failed) break;
           if (next_lo < re) issue(buf ^ 1, next_lo, (int)min((uint32_t)kBatch, re - next_lo), +1);
-          setup(buf, nb);
-          __syncthreads();
-          spans(nb, false);  // adjoint: edge crossings only
+          spans(buf, nb, false);  // adjoint: edge crossings only
           __syncthreads();
           prefixes(nb);
           __syncthreads();
@@ -684,7 +633,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
             // rebuilt from them once per tet at flush time.  Moments per item:
             //  [0] density  [1..3] base colour  [4] sum(sb)  [5..7] d * d(dc/dt)
             //  [8 + 4f] S_f  [9 + 4f .. 11 + 4f] P_f   (f = face 0..3)
-            float(*red)[kMom + 1] = s.red[warp];
+            float(*red)[kMomHalf + 1] = s.red[warp];
             const uint32_t n_valid = n_items;
             for (uint32_t chunk = (uint32_t)warp * 32u; chunk < n_items; chunk += (uint32_t)NT) {
               const uint32_t i = chunk + (uint32_t)lane;
@@ -706,8 +655,9 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
                   const float t_prev = st.x, d_od_state = st.y;
                   const float4 d = s.pdir[p];
                   const float4 dlv = s.pdl[p];
-                  const float4 cb = s.cb[k];
-                  const float4 gg = s.gr[k];
+                  const TetView& tv = s.view[buf][k];
+                  const float4 cb = tv.cb;
+                  const float4 gg = tv.gm;
                   const float dcdt = dot3x(gg.x, gg.y, gg.z, d.x, d.y, d.z);
                   Integral I;
                   integrate(cb, dcdt, t_min, t_max, I, ix.w);
@@ -749,8 +699,8 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
                     const int f = side == 0 ? fmin : fmax;
                     const float dt = side == 0 ? d_tmin : d_tmax;
                     const float tt = side == 0 ? t_min : t_max;
-                    const float4 nf = s.nrm[k][f];
-                    const float den = (s.flip[k][f] ? -1.0f : 1.0f) * (nf.x * d.x + nf.y * d.y + nf.z * d.z);
+                    const float4 nf = tv.nrm[f];
+                    const float den = (face_flipped(tv, f) ? -1.0f : 1.0f) * (nf.x * d.x + nf.y * d.y + nf.z * d.z);
                     const float inv_den = fabsf(den) < kTiny ? clipf(1.0f / kTiny, kMinVal, kMaxVal)
                                                              : clipf(__fdividef(1.0f, den), kMinVal, kMaxVal);
                     const float sv = dt * inv_den, st_ = sv * tt;
@@ -766,29 +716,37 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
                   }
                 }
               }
-              // transpose through shared memory; lane q < kMom then walks column q
-              // over the chunk's rows, flushing a partial sum at every tet boundary
-#pragma unroll
-              for (int q = 0; q < kMom; ++q) red[lane][q] = m[q];
+              // transpose through shared memory, half of the moments at a time;
+              // lane (h, q) with q < kMomHalf then walks column q over rows
+              // [16h, 16h + 16) of the chunk, adding a partial sum to the tet's
+              // moment at every tet boundary and at the end of its rows
               const int kp = __shfl_up_sync(0xffffffffu, k, 1);
               const unsigned heads = __ballot_sync(0xffffffffu, k >= 0 && (lane == 0 || kp != k));
               const int n_rows = __popc(__ballot_sync(0xffffffffu, k >= 0));  // valid rows come first
-              red[lane][kMom] = __int_as_float(k);
-              __syncwarp();
-              if (lane < kMom && heads) {
-                float sum = 0.0f;
-                int cur = __float_as_int(red[0][kMom]);
-                for (int row = 0; row < n_rows; ++row) {
-                  if (row > 0 && ((heads >> row) & 1u)) {
-                    if (sum != 0.0f) atomicAdd(&s.mom[cur][lane], sum);
-                    sum = 0.0f;
-                    cur = __float_as_int(red[row][kMom]);
+              const int wq = lane & 15, wr0 = (lane >> 4) * 16;
+              const int wr1 = min(wr0 + 16, n_rows);
+#pragma unroll
+              for (int hm = 0; hm < 2; ++hm) {
+#pragma unroll
+                for (int q = 0; q < kMomHalf; ++q) red[lane][q] = m[hm * kMomHalf + q];
+                red[lane][kMomHalf] = __int_as_float(k);
+                __syncwarp();
+                if (wq < kMomHalf && wr0 < wr1) {
+                  const int col = hm * kMomHalf + wq;
+                  float sum = 0.0f;
+                  int cur = __float_as_int(red[wr0][kMomHalf]);
+                  for (int row = wr0; row < wr1; ++row) {
+                    if (row > wr0 && ((heads >> row) & 1u)) {
+                      if (sum != 0.0f) atomicAdd(&s.mom[cur][col], sum);
+                      sum = 0.0f;
+                      cur = __float_as_int(red[row][kMomHalf]);
+                    }
+                    sum += red[row][wq];
                   }
-                  sum += red[row][lane];
+                  if (sum != 0.0f) atomicAdd(&s.mom[cur][col], sum);
                 }
-                if (sum != 0.0f) atomicAdd(&s.mom[cur][lane], sum);
+                __syncwarp();
               }
-              __syncwarp();
             }
             __syncthreads();
             k0 = k1;
@@ -802,8 +760,9 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
 #pragma unroll
             for (int q = 0; q < kMom; ++q) any = any || (mm[q] != 0.0f);
             if (any) {
-              const TetRec& r = s.rec[buf][k];
-              const float4 gg = s.gr[k];
+              const TetView& tv = s.view[buf][k];
+              const TetRec r = a.rec[tv.meta.x];
+              const float4 gg = tv.gm;
               float out[20];
               out[0] = mm[0];
               out[1] = mm[1]; out[2] = mm[2]; out[3] = mm[3];
@@ -821,8 +780,8 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
                 if (S == 0.0f && Px == 0.0f && Py == 0.0f && Pz == 0.0f) continue;
                 const int ia = kFaces[f][0], ib = kFaces[f][1], ic = kFaces[f][2];
                 const float4 va = rec_vertex(r, ia), vb = rec_vertex(r, ib), vc = rec_vertex(r, ic);
-                const float4 nf = s.nrm[k][f];
-                const float sg = s.flip[k][f] ? -1.0f : 1.0f;
+                const float4 nf = tv.nrm[f];
+                const float sg = face_flipped(tv, f) ? -1.0f : 1.0f;
                 // w = (a - cam) S - P
                 const float wx = (va.x - camx) * S - Px, wy = (va.y - camy) * S - Py, wz = (va.z - camz) * S - Pz;
                 float ux = vc.x - va.x, uy = vc.y - va.y, uz = vc.z - va.z;  // c - a
@@ -840,7 +799,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
 #pragma unroll
               for (int q = 0; q < 12; ++q) out[7 + q] = clipf(dv[q], kMinVal, kMaxVal);
               out[19] = 0.0f;
-              float4* dst = reinterpret_cast<float4*>(a.grad_slot + (size_t)s.tet[buf][k] * kGradSlot);
+              float4* dst = reinterpret_cast<float4*>(a.grad_slot + (size_t)tv.meta.x * kGradSlot);
 #pragma unroll
               for (int c = 0; c < 5; ++c) {
                 const float4 v4 = make_float4(out[4 * c], out[4 * c + 1], out[4 * c + 2], out[4 * c + 3]);
