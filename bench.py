@@ -44,6 +44,10 @@ N_VIEWS = 16
 LR = dict(lr_verts=1e-4, lr_dens=1e-2, lr_grads=1e-3)
 
 
+def res_text(res) -> str:
+    return ",".join(f"{w}^2" if w == h else f"{w}x{h}" for w, h in res)
+
+
 def peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -53,13 +57,13 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def build_workload(points: int, seed: int, rank: int):
+def build_workload(points: int, seed: int, rank: int, n_views: int = N_VIEWS, res=RES):
     from rmesh_b200.camera import orbit_cameras
     from rmesh_b200.scenes import gmm_cloud, make_scene
 
     rng = np.random.default_rng(seed)
     scene = make_scene(gmm_cloud(points, rng), rng, sh_degree=0)
-    cams = orbit_cameras(N_VIEWS, seed=seed + 1 + 1000 * rank, radius=(2.5, 4.0), resolutions=RES)
+    cams = orbit_cameras(n_views, seed=seed + 1 + 1000 * rank, radius=(2.5, 4.0), resolutions=res)
     trng = np.random.default_rng(seed + 2 + 1000 * rank)
     gts = [trng.uniform(0, 1, (c.height, c.width, 3)).astype(np.float32) for c in cams]
     return scene, cams, gts
@@ -137,7 +141,7 @@ def run_gpu(args):
     from rmesh_b200 import RMeshRenderer
     from rmesh_b200 import _lib
 
-    scene, cams, gts = build_workload(args.points, args.seed, rank)
+    scene, cams, gts = build_workload(args.points, args.seed, rank, args.views, args.res)
     r = RMeshRenderer(scene["vertices"], scene["indices"], scene["base_colors"], scene["densities"],
                       scene["color_grads"], scene["circumdata"], cams[0].width, cams[0].height,
                       tile_size=args.tile_size, device=local)
@@ -222,8 +226,8 @@ def run_gpu(args):
         "data": "synthetic (seeded GMM Delaunay mesh, seeded targets)",
         "config": {
             "workload": f"batched: {args.points}-point 8-component GMM Delaunay mesh ({r.n_tets} tets), "
-                        f"{N_VIEWS} views from {{256^2,512^2,800x600,1024^2}}, L2 loss, Adam",
-            "n_tets": r.n_tets, "n_vertices": r.n_vertices, "views_per_gpu": N_VIEWS,
+                        f"{args.views} views from {{{res_text(args.res)}}}, L2 loss, Adam",
+            "n_tets": r.n_tets, "n_vertices": r.n_vertices, "views_per_gpu": args.views,
             "pixels_per_step_per_gpu": n_pix, "tile_size": args.tile_size, "color_mode": "base_colors",
             "parallelism": f"dp{world} (views sharded, gradients summed)" if world > 1 else "single GPU",
             "l2": "inputs larger than L2 (mesh records + pair lists > 126 MB per step)",
@@ -232,7 +236,7 @@ def run_gpu(args):
         "plain": {"value": round(world * 1000.0 / ms_plain, 4), "unit": "train-steps/s", "ms_per_step": round(ms_plain, 4)},
         "batched_graph_vs_plain": round(ms_plain / ms_graph, 3),
         "e2e": {"value": round(world * 1000.0 / ms_e2e, 4), "unit": "train-steps/s",
-                "h2d_bytes_per_step": int(n_pix * 12 + N_VIEWS * 160 + 48),
+                "h2d_bytes_per_step": int(n_pix * 12 + args.views * 160 + 48),
                 "d2h_bytes_per_step": int(_lib.COUNTERS_BYTES)},
         "gpu_launches": int(total_launches),
         "stage_ms_per_step": {k: round(v / nsteps_prof, 4) for k, v in stage_ms.items()},
@@ -291,7 +295,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    scene, cams, gts = build_workload(args.points, args.seed, 0)
+    scene, cams, gts = build_workload(args.points, args.seed, 0, args.views, args.res)
     n_pix = sum(c.width * c.height for c in cams)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import Oracle
@@ -315,13 +319,14 @@ def run_reference(args):
     t_step = dt * n_pix / (cam.width * cam.height)
     v = round(1.0 / t_step, 6)
     sample = (f"one {cam.width}x{cam.height} view per step ({cam.width * cam.height} px), scaled by pixels to the "
-              f"{n_pix}-px 16-view step; C port of the reference kernels, OpenMP {threads} threads")
+              f"{n_pix}-px {args.views}-view step; C port of the reference kernels, OpenMP {threads} threads")
     print(json.dumps({
         "impl": "reference", "metric": "fwd+bwd train-steps/s (16 mixed-resolution views, batched graph-captured step)",
         "value": v, "unit": "train-steps/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t_step * 1e3, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded GMM Delaunay mesh, seeded targets)",
-        "config": {"workload": f"batched: {args.points}-point GMM Delaunay mesh, {N_VIEWS} views"},
+        "config": {"workload": f"batched: {args.points}-point 8-component GMM Delaunay mesh, {args.views} views "
+                               f"from {{{res_text(args.res)}}}, L2 loss, Adam"},
         "cpu_baseline": {"value": v, "unit": "train-steps/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "train-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference's own pipeline is wgpu (Vulkan/Metal) and cannot run here; this is its CPU port",
@@ -338,7 +343,12 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--tile-size", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--views", type=int, default=N_VIEWS, help="views per step (default: the 16-view workload)")
+    ap.add_argument("--res", default=None,
+                    help="comma-separated WxH choices for the views (default 256x256,512x512,800x600,1024x1024); "
+                         "smaller cases serve profiler captures")
     args = ap.parse_args()
+    args.res = RES if args.res is None else tuple(tuple(int(v) for v in x.split("x")) for x in args.res.split(","))
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         run_reference(args)
