@@ -46,6 +46,7 @@ extern "C" {
 #define RMESH_ERR_TIMEOUT 5      /* a bounded device spin gave up (kernel returned an error, no hang) */
 #define RMESH_ERR_STATE 6        /* call order violated (e.g. backward before forward_tiled) */
 #define RMESH_ERR_NO_DEVICE 7    /* no CUDA device / library built for another architecture */
+#define RMESH_ERR_TOO_LARGE 8    /* input above the fixed scratch of rmesh_count_tiles_static */
 
 typedef struct RmeshCtx RmeshCtx;
 
@@ -160,6 +161,35 @@ RMESH_API int rmesh_accumulate_views(RmeshCtx* ctx, const RmeshCamera* cams, int
                                      const RmeshTrainOpts* opts, float* loss_out);
 RMESH_API int rmesh_grad_slots(RmeshCtx* ctx, float** device_ptr, uint64_t* n_floats);
 RMESH_API int rmesh_apply_adam(RmeshCtx* ctx, const RmeshTrainOpts* opts);
+
+/* ---- allocation-free tile count ---------------------------------------------
+ * No counterpart in the reference.  For callers that must not allocate device
+ * memory (a per-frame visibility query in a viewer loop, where cudaMalloc and
+ * cudaFree would synchronise the device; a caller with a fixed memory budget
+ * that holds no context): the per-tet cull and conservative tile count of the
+ * project stage (project_compute.wgsl:88-262, the values rmesh_debug_tiles_touched
+ * reports after a single-view rmesh_forward_tiled) for one camera, plus the ids
+ * of the tile-touching tets, with no context and no allocation.
+ *  - All arrays are CUDA device (or managed) memory of the current device:
+ *    vertices [3 * n_vertices], indices [4 * n_tets], densities [n_tets];
+ *    outputs tiles_touched [n_tets] (by tet id), visible_tets [n_tets] (the
+ *    first counts[0] entries are the tile-touching tet ids, ascending) and
+ *    counts [2] (counts[1] receives device error bits: 2 = a bounded spin gave
+ *    up, 4 = a vertex index >= n_vertices).  cam->cam_pos and c2w_intrinsics
+ *    are not used.  tile_size 0 means 12.
+ *  - n_tets above RMESH_STATIC_MAX_TETS returns RMESH_ERR_TOO_LARGE.
+ *  - Asynchronous on `stream` (a cudaStream_t; NULL = the legacy default
+ *    stream): read the outputs after synchronising it.
+ *  - Scratch is one fixed 524,544-byte device array per device, shared by every
+ *    call; each call clears what must start at zero on its stream.  Calls in
+ *    flight at the same time on one device race on it: order them.  The first
+ *    call on each device (with that device current) looks up the array's
+ *    address and should come before any stream capture. */
+#define RMESH_STATIC_MAX_TETS (1u << 24)
+RMESH_API int rmesh_count_tiles_static(const float* vertices, uint64_t n_vertices, const uint32_t* indices,
+                                       const float* densities, uint64_t n_tets, const RmeshCamera* cam,
+                                       int32_t tile_size, uint32_t* tiles_touched, uint32_t* visible_tets,
+                                       uint32_t* counts, void* stream);
 
 /* ---- inspection (parity tests) --------------------------------------------- */
 /* tiles_touched of the last forward, indexed by tet id ([M], single view). */

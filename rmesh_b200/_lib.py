@@ -21,6 +21,8 @@ RMESH_ERR_PAIR_OVERFLOW = 4
 RMESH_ERR_TIMEOUT = 5
 RMESH_ERR_STATE = 6
 RMESH_ERR_NO_DEVICE = 7
+RMESH_ERR_TOO_LARGE = 8
+RMESH_STATIC_MAX_TETS = 1 << 24
 
 MODE_PLAIN, MODE_BATCHED, MODE_GRAPH = 0, 1, 2
 N_STAGES = 8
@@ -33,6 +35,7 @@ EXPORTED = (
     "rmesh_forward_tiled", "rmesh_backward", "rmesh_train_step", "rmesh_train_step_views",
     "rmesh_debug_tiles_touched", "rmesh_debug_pairs", "rmesh_debug_ranges", "rmesh_set_profiling",
     "rmesh_stage_times", "rmesh_accumulate_views", "rmesh_grad_slots", "rmesh_apply_adam",
+    "rmesh_count_tiles_static",
 )
 
 COUNTERS_BYTES = 792  # sizeof(rm::Counters), read back once per training run
@@ -110,6 +113,7 @@ def load() -> ctypes.CDLL:
         "rmesh_accumulate_views": ([vp, P(Camera), i32, vp, P(TrainOpts), vp], ctypes.c_int),
         "rmesh_grad_slots": ([vp, P(vp), P(u64)], ctypes.c_int),
         "rmesh_apply_adam": ([vp, P(TrainOpts)], ctypes.c_int),
+        "rmesh_count_tiles_static": ([vp, u64, vp, vp, u64, P(Camera), i32, vp, vp, vp, vp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -13,6 +13,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <cstdio>
 #include <cstring>
 #include <string>
@@ -1058,3 +1059,257 @@ int rmesh_stage_times(RmeshCtx* c, float* ms_out, int32_t* launches_out) {
 }
 
 }  // extern "C"
+
+// ============================================================================
+// Allocation-free tile count (rmesh_count_tiles_static)
+//
+// For callers that must not allocate device memory: a per-frame visibility
+// query in an interactive viewer, where cudaMalloc / cudaFree would
+// synchronise the device mid-frame, or a caller with a fixed device-memory
+// budget that owns no renderer context (a context allocates every buffer of
+// the path).  The entry point runs a variant of project_kernel (the same cull,
+// the same conservative tile count and the same chained-scan compaction of the
+// tile-touching tets) whose only scratch, the scan's block ticket and status
+// words, lives in the fixed file-scope array below.  It calls no cudaMalloc,
+// cudaFree or allocating library routine.
+//
+// Every call on a device shares that device's array.  The ticket and the first
+// ceil(n_tets / 256) status words must start at zero; each call clears them
+// with a memset on its own stream before its launch.  Two calls in flight at
+// the same time on one device (other streams, other threads) race on the array
+// and return wrong results: order them on one stream or with events.
+// ============================================================================
+namespace rm {
+
+constexpr uint32_t kStaticMaxTets = RMESH_STATIC_MAX_TETS;
+constexpr uint32_t kStaticScanBlocks = kStaticMaxTets / 256u;
+constexpr size_t kStaticTicketBytes = 256;  // the block ticket, on its own 256-byte line
+constexpr size_t kStaticScratchBytes = kStaticTicketBytes + 8 * (size_t)kStaticScanBlocks;  // 524,544 bytes
+constexpr uint32_t kErrBadIndex = 1u << 2;  // a vertex index >= n_vertices (the tet is skipped)
+static_assert(kStaticMaxTets % 256u == 0, "scan positions");
+
+static __device__ __align__(256) unsigned char g_count_scratch[kStaticScratchBytes];
+
+// Single-view variant of project_kernel: gathers the four vertices and the
+// density of each tet straight from the mesh arrays (no per-tet records), and
+// writes tiles_touched by tet id plus the ids of the tile-touching tets in
+// ascending order.  counts[0] receives their number, counts[1] error bits.
+__global__ void __launch_bounds__(256) count_tiles_static_kernel(const float* __restrict__ verts, uint64_t n_verts,
+                                                                 const uint32_t* __restrict__ idx,
+                                                                 const float* __restrict__ dens, uint32_t M,
+                                                                 ViewParams V, uint32_t* __restrict__ tiles_touched,
+                                                                 uint32_t* __restrict__ visible, uint32_t* counts,
+                                                                 unsigned char* scratch) {
+  uint32_t* ticket = reinterpret_cast<uint32_t*>(scratch);
+  unsigned long long* status = reinterpret_cast<unsigned long long*>(scratch + kStaticTicketBytes);
+  __shared__ uint32_t s_blk;
+  __shared__ uint32_t s_warp[8];
+  __shared__ unsigned long long s_prefix;
+  if (threadIdx.x == 0) s_blk = atomicAdd(ticket, 1u);
+  __syncthreads();
+  const uint32_t blk = s_blk;
+  const uint32_t tet = blk * 256u + threadIdx.x;
+
+  uint32_t count = 0;
+  bool flag = false, bad = false;
+  if (tet < M) {
+    uint32_t q[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      q[k] = idx[4 * (size_t)tet + k];
+      bad = bad || (uint64_t)q[k] >= n_verts;
+    }
+    bool visible = !bad;
+    if (!bad) {
+      float vx[4], vy[4], vz[4], p[4][4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        vx[k] = verts[3 * (size_t)q[k]];
+        vy[k] = verts[3 * (size_t)q[k] + 1];
+        vz[k] = verts[3 * (size_t)q[k] + 2];
+        float c[4];
+        clip_exact(V.vp, vx[k], vy[k], vz[k], c);
+        const float inv_w = fdv(1.0f, fa(c[3], 1e-6f));
+        p[k][0] = fm(c[0], inv_w);
+        p[k][1] = fm(c[1], inv_w);
+        p[k][2] = fm(c[2], inv_w);
+        p[k][3] = c[3];
+      }
+      const bool any_behind = (p[0][3] <= 0.0f) || (p[1][3] <= 0.0f) || (p[2][3] <= 0.0f) || (p[3][3] <= 0.0f);
+      if (!any_behind) {  // NDC box and extent culls (project_compute.wgsl:124-144)
+        const float min_x = fminf(fminf(p[0][0], p[1][0]), fminf(p[2][0], p[3][0]));
+        const float max_x = fmaxf(fmaxf(p[0][0], p[1][0]), fmaxf(p[2][0], p[3][0]));
+        const float min_y = fminf(fminf(p[0][1], p[1][1]), fminf(p[2][1], p[3][1]));
+        const float max_y = fmaxf(fmaxf(p[0][1], p[1][1]), fmaxf(p[2][1], p[3][1]));
+        const float min_z = fminf(fminf(p[0][2], p[1][2]), fminf(p[2][2], p[3][2]));
+        if (max_x < -1.0f || min_x > 1.0f || max_y < -1.0f || min_y > 1.0f || min_z > 1.0f) visible = false;
+        if (fm(fm(fs(max_x, min_x), V.Wf), fm(fs(max_y, min_y), V.Hf)) < 1.0f) visible = false;
+      }
+      if (visible) {  // optical-depth cull (project_compute.wgsl:146-162)
+        const int ei[6] = {1, 2, 3, 2, 3, 3};
+        const int ej[6] = {0, 0, 0, 1, 1, 2};
+        float e2[6];
+#pragma unroll
+        for (int e = 0; e < 6; ++e) {
+          const float dx = fs(vx[ei[e]], vx[ej[e]]), dy = fs(vy[ei[e]], vy[ej[e]]), dz = fs(vz[ei[e]], vz[ej[e]]);
+          e2[e] = dot3x(dx, dy, dz, dx, dy, dz);
+        }
+        const float m = fmaxf(fmaxf(e2[0], fmaxf(e2[1], e2[2])), fmaxf(e2[3], fmaxf(e2[4], e2[5])));
+        if (fm(dens[tet], __fsqrt_rn(m)) < 0.01f) visible = false;
+      }
+      if (visible && !any_behind) {
+        float px[4], py[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          px[k] = fm(fm(fa(p[k][0], 1.0f), 0.5f), V.Wf);
+          py[k] = fm(fm(fs(1.0f, p[k][1]), 0.5f), V.Hf);
+        }
+        scanline_tiles(px, py, V.Wf, V.Hf, (uint32_t)V.TS,
+                       [&](uint32_t, uint32_t tx0, uint32_t tx1) { count += tx1 - tx0 + 1u; });
+      }
+    }
+    if (!visible) count = 0u;
+    tiles_touched[tet] = count;
+    flag = count > 0u;
+  }
+  if (bad) atomicOr(&counts[1], kErrBadIndex);
+  // block scan of the flags, then the chained scan across blocks
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const unsigned ballot = __ballot_sync(0xffffffffu, flag);
+  if (lane == 0) s_warp[warp] = __popc(ballot);
+  __syncthreads();
+  uint32_t warp_off = 0, block_total = 0;
+#pragma unroll
+  for (int w = 0; w < 8; ++w) {
+    const uint32_t c = s_warp[w];
+    if (w < warp) warp_off += c;
+    block_total += c;
+  }
+  if (warp == 0) {
+    const unsigned long long pre = chained_lookback(status, blk, block_total, &counts[1]);
+    if (lane == 0) s_prefix = pre;
+  }
+  __syncthreads();
+  const unsigned long long base = s_prefix;
+  if (flag) visible[base + warp_off + __popc(ballot & ((1u << lane) - 1u))] = tet;
+  if (threadIdx.x == 0 && (uint64_t)(blk + 1u) * 256u >= M) counts[0] = (uint32_t)(base + block_total);
+}
+
+namespace {
+
+// Device address of g_count_scratch per device ordinal, looked up on the first
+// call made with that device current.
+constexpr int kStaticMaxDevices = 64;
+std::mutex g_scratch_mu;
+unsigned char* g_scratch_ptr[kStaticMaxDevices] = {};
+
+typedef int (*MemRangeFn)(unsigned long long* base, size_t* size, unsigned long long ptr);
+
+// [p, p + bytes) must lie in one device (or managed) allocation of the current
+// device; the kernel would otherwise read or write outside the caller's arrays.
+bool device_range_ok(const void* p, size_t bytes, int dev) {
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  if (at.type == cudaMemoryTypeDevice) {
+    if (at.device != dev) return false;
+  } else if (at.type != cudaMemoryTypeManaged) {
+    return false;
+  }
+  static MemRangeFn range_fn = nullptr;
+  static bool looked_up = false;
+  if (!looked_up) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuMemGetAddressRange", &fn, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      range_fn = reinterpret_cast<MemRangeFn>(fn);
+    looked_up = true;
+  }
+  if (range_fn) {
+    unsigned long long base = 0;
+    size_t size = 0;
+    if (range_fn(&base, &size, (unsigned long long)(uintptr_t)p) != 0) return false;
+    if ((uintptr_t)p + bytes > base + size) return false;
+  }
+  return true;
+}
+
+}  // namespace
+}  // namespace rm
+
+extern "C" int rmesh_count_tiles_static(const float* vertices, uint64_t n_vertices, const uint32_t* indices,
+                                        const float* densities, uint64_t n_tets, const RmeshCamera* cam,
+                                        int32_t tile_size, uint32_t* tiles_touched, uint32_t* visible_tets,
+                                        uint32_t* counts, void* stream) {
+  using namespace rm;
+  if (n_tets > kStaticMaxTets) return RMESH_ERR_TOO_LARGE;
+  if (!cam || !counts) return RMESH_ERR_INVALID_ARG;
+  if (n_tets > 0 && (!vertices || !indices || !densities || !tiles_touched || !visible_tets || n_vertices == 0))
+    return RMESH_ERR_INVALID_ARG;
+  if (n_vertices > (1ull << 32)) return RMESH_ERR_INVALID_ARG;
+  const int ts = tile_size == 0 ? 12 : tile_size;
+  if (ts < 1 || ts > 256) return RMESH_ERR_INVALID_ARG;
+  if (cam->width <= 0 || cam->height <= 0 || cam->width > 65536 || cam->height > 65536) return RMESH_ERR_INVALID_ARG;
+
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return RMESH_ERR_NO_DEVICE;
+  }
+  if (dev < 0 || dev >= kStaticMaxDevices) return RMESH_ERR_INVALID_ARG;
+  unsigned char* scratch = nullptr;
+  {
+    // first call on this device: look up the scratch array's device address
+    // (this may load the module on the device, so make it before any capture)
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    if (!g_scratch_ptr[dev]) {
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_count_scratch) != cudaSuccess || !p) {
+        cudaGetLastError();
+        return RMESH_ERR_CUDA;
+      }
+      g_scratch_ptr[dev] = static_cast<unsigned char*>(p);
+    }
+    scratch = g_scratch_ptr[dev];
+  }
+
+  const uint64_t M = n_tets;
+  if (!device_range_ok(counts, 8, dev)) return RMESH_ERR_INVALID_ARG;
+  if (M > 0 && (!device_range_ok(vertices, 12 * n_vertices, dev) || !device_range_ok(indices, 16 * M, dev) ||
+                !device_range_ok(densities, 4 * M, dev) || !device_range_ok(tiles_touched, 4 * M, dev) ||
+                !device_range_ok(visible_tets, 4 * M, dev)))
+    return RMESH_ERR_INVALID_ARG;
+
+  ViewParams V;
+  memset(&V, 0, sizeof(V));
+  memcpy(V.vp, cam->vp, sizeof(V.vp));
+  V.cam[0] = cam->cam_pos[0];
+  V.cam[1] = cam->cam_pos[1];
+  V.cam[2] = cam->cam_pos[2];
+  V.W = cam->width;
+  V.H = cam->height;
+  V.Wf = (float)cam->width;
+  V.Hf = (float)cam->height;
+  V.TS = ts;
+  V.tiles_x = (cam->width + ts - 1) / ts;
+  V.tiles_y = (cam->height + ts - 1) / ts;
+
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(counts, 0, 8, st) != cudaSuccess) {
+    cudaGetLastError();
+    return RMESH_ERR_CUDA;
+  }
+  if (M == 0) return RMESH_OK;
+  const uint32_t nblk = (uint32_t)((M + 255) / 256);
+  if (cudaMemsetAsync(scratch, 0, kStaticTicketBytes + 8 * (size_t)nblk, st) != cudaSuccess) {
+    cudaGetLastError();
+    return RMESH_ERR_CUDA;
+  }
+  count_tiles_static_kernel<<<nblk, 256, 0, st>>>(vertices, n_vertices, indices, densities, (uint32_t)M, V,
+                                                   tiles_touched, visible_tets, counts, scratch);
+  if (cudaGetLastError() != cudaSuccess) return RMESH_ERR_CUDA;
+  return RMESH_OK;
+}
