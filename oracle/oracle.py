@@ -70,6 +70,7 @@ class Oracle:
         self._loss.restype = ctypes.c_double
         self._backward = getattr(L, "orc_backward" + s)
         self._adam = getattr(L, "orc_adam" + s)
+        self._sh_backward = getattr(L, "orc_sh_backward" + s)
         rt = ctypes.c_float if dtype == "f32" else ctypes.c_double
         self._rt = rt
         self._raster.argtypes = [self.rp, _u32p, self.rp, self.rp, self.rp, _u32p, _u32p, self.rp, self.rp,
@@ -99,18 +100,30 @@ class Oracle:
         tile_bits = 1 if num_tiles <= 1 else int(num_tiles - 1).bit_length()
         return (32 + tile_bits + 7) & ~7
 
+    def sh_values(self, sh, f16=True):
+        """Coefficient values the SH colour reads: the reference stores them as
+        f16 with round-to-nearest-even (crates/rmesh-viewer/src/gpu_state.rs:60-88);
+        f16=False keeps them unrounded (finite-difference checks in float64)."""
+        if sh is None:
+            return None
+        a = np.asarray(sh, dtype=np.float32)
+        if f16:
+            a = a.astype(np.float16).astype(np.float32)
+        return self._r(a)
+
     # ---- stages -----------------------------------------------------------
-    def project(self, scene, cam, tile_size=12, sh_packed=None, sh_degree=0):
+    def project(self, scene, cam, tile_size=12, sh=None, sh_degree=0):
+        """sh: coefficient values [M*3*nc] as read by the shader (see sh_values)."""
         v, idx = self._r(scene["vertices"]), self._u(scene["indices"])
         m = idx.size // 4
         vp, c2w, intr, cp, W, H = self._cam(cam)
         visible = np.zeros(m, dtype=np.uint8)
         tt = np.zeros(m, dtype=np.uint32)
         colors = np.zeros(3 * m, dtype=self.np)
-        shp = None if sh_packed is None else self._u(sh_packed)
+        shp = None if sh is None else self._r(sh)
         self._project(ctypes.c_int64(m), _ptr(v, self.rp), _ptr(idx, _u32p), _ptr(self._r(scene["densities"]), self.rp),
                       _ptr(self._r(scene["color_grads"]), self.rp), _ptr(self._r(scene["circumdata"]), self.rp),
-                      _ptr(self._r(scene["base_colors"]), self.rp), _ptr(shp, _u32p), ctypes.c_int(sh_degree),
+                      _ptr(self._r(scene["base_colors"]), self.rp), _ptr(shp, self.rp), ctypes.c_int(sh_degree),
                       _ptr(vp, self.rp), _ptr(cp, self.rp), ctypes.c_int(W), ctypes.c_int(H), ctypes.c_int(tile_size),
                       _ptr(visible, _u8p), _ptr(tt, _u32p), _ptr(colors, self.rp))
         return visible, tt, colors
@@ -194,13 +207,14 @@ class Oracle:
 
     # ---- host sequencing --------------------------------------------------
     def forward_tiled(self, scene, cam, tile_size=12, min_t=0.0, aux=False, stats=False,
-                      sh_packed=None, sh_degree=0):
-        """lib.rs:1041-1204.  Returns the image plus every intermediate buffer."""
+                      sh=None, sh_degree=0):
+        """lib.rs:1041-1204.  Returns the image plus every intermediate buffer.
+        sh: coefficient values (see sh_values) selecting the SH colour branch."""
         W, H = int(cam.width), int(cam.height)
         tiles_x = (W + tile_size - 1) // tile_size
         tiles_y = (H + tile_size - 1) // tile_size
         num_tiles = tiles_x * tiles_y
-        visible, tt, colors = self.project(scene, cam, tile_size, sh_packed, sh_degree)
+        visible, tt, colors = self.project(scene, cam, tile_size, sh, sh_degree)
         lo, hi, vals, emitted = self.emit(scene, cam, visible, tt, tile_size)
         slo, shi, svals = self.sort_pairs(lo, hi, vals, num_tiles)
         ranges = self.tile_ranges(shi, num_tiles)
@@ -210,10 +224,31 @@ class Oracle:
                    unsorted=(lo, hi, vals))
         return out
 
-    def backward(self, scene, cam, dl_d_image, fwd, tile_size=12, threads=1):
-        """lib.rs:1894-2031 (the sort it redoes equals the forward's)."""
-        return self.backward_raw(scene, cam, fwd["colors"], fwd["vals"], fwd["ranges"],
-                                 np.asarray(dl_d_image).reshape(-1), fwd["image"].reshape(-1), tile_size, threads)
+    def backward(self, scene, cam, dl_d_image, fwd, tile_size=12, threads=1, sh=None, sh_degree=0):
+        """lib.rs:1894-2031 (the sort it redoes equals the forward's).  With sh
+        (the coefficient values of the forward), the colour gradient continues
+        through the SH colour: d_sh is added, d_vertices and d_color_grads gain
+        the colour's dependence on them, and d_base_colors is zero."""
+        g = self.backward_raw(scene, cam, fwd["colors"], fwd["vals"], fwd["ranges"],
+                              np.asarray(dl_d_image).reshape(-1), fwd["image"].reshape(-1), tile_size, threads)
+        if sh is not None:
+            g["d_sh"] = self.sh_backward(scene, cam, sh, sh_degree, fwd["visible"], g["d_base_colors"],
+                                         g["d_vertices"], g["d_color_grads"])
+            g["d_base_colors"] = np.zeros_like(g["d_base_colors"])
+        return g
+
+    def sh_backward(self, scene, cam, sh, sh_degree, visible, d_colors, d_vertices, d_color_grads):
+        """Adjoint of the SH colour; adds into d_vertices / d_color_grads in place."""
+        m = scene["indices"].size // 4
+        nc = (sh_degree + 1) ** 2
+        d_sh = np.zeros(3 * nc * m, dtype=self.np)
+        cp = self._r(cam.cam_pos)
+        self._sh_backward(ctypes.c_int64(m), _ptr(self._r(scene["vertices"]), self.rp),
+                          _ptr(self._u(scene["indices"]), _u32p), _ptr(self._r(scene["color_grads"]), self.rp),
+                          _ptr(self._r(sh), self.rp), ctypes.c_int(sh_degree), _ptr(cp, self.rp),
+                          _ptr(np.ascontiguousarray(visible, dtype=np.uint8), _u8p), _ptr(self._r(d_colors), self.rp),
+                          _ptr(d_sh, self.rp), _ptr(d_vertices, self.rp), _ptr(d_color_grads, self.rp))
+        return d_sh
 
     def loss_value(self, scene, cam, gt, loss_type=1, tile_size=12):
         fwd = self.forward_tiled(scene, cam, tile_size)
@@ -222,25 +257,39 @@ class Oracle:
 
 
 class OracleTrainer:
-    """lib.rs:2405-2636 on the CPU: one view per step, Adam on three groups."""
+    """lib.rs:2405-2636 on the CPU: one view per step, Adam on three groups
+    (four with SH colours: use_sh adds the coefficients, learning rate lr_sh)."""
 
-    def __init__(self, scene, dtype="f32", tile_size=12):
+    def __init__(self, scene, dtype="f32", tile_size=12, use_sh=False):
         self.o = Oracle(dtype)
         self.scene = {k: (np.array(v, dtype=self.o.np) if k in ("vertices", "densities", "color_grads",
                                                                 "base_colors", "circumdata") else v)
                       for k, v in scene.items()}
+        self.use_sh = use_sh
+        groups = ["vertices", "densities", "color_grads"]
+        if use_sh:
+            self.sh = np.array(scene["sh_coeffs"], dtype=np.float32)  # fp32 master values
+            self.sh_degree = int(scene["sh_degree"])
+            self.m_sh = np.zeros_like(self.sh, dtype=self.o.np)
+            self.v_sh = np.zeros_like(self.sh, dtype=self.o.np)
         self.tile_size = tile_size
         self.step = 0
         z = lambda k: np.zeros_like(self.scene[k])
-        self.m = {k: z(k) for k in ("vertices", "densities", "color_grads")}
-        self.v = {k: z(k) for k in ("vertices", "densities", "color_grads")}
+        self.m = {k: z(k) for k in groups}
+        self.v = {k: z(k) for k in groups}
 
-    def train_step(self, cam, gt, lr_verts, lr_dens, lr_grads, loss_type=1):
-        fwd = self.o.forward_tiled(self.scene, cam, self.tile_size)
+    def train_step(self, cam, gt, lr_verts, lr_dens, lr_grads, loss_type=1, lr_sh=0.0):
+        shv = self.o.sh_values(self.sh) if self.use_sh else None
+        deg = self.sh_degree if self.use_sh else 0
+        fwd = self.o.forward_tiled(self.scene, cam, self.tile_size, sh=shv, sh_degree=deg)
         loss, dl = self.o.loss(fwd["image"], gt, loss_type)
-        g = self.o.backward(self.scene, cam, dl, fwd, self.tile_size)
+        g = self.o.backward(self.scene, cam, dl, fwd, self.tile_size, sh=shv, sh_degree=deg)
         self.step += 1
         for key, gk, lr in (("vertices", "d_vertices", lr_verts), ("densities", "d_densities", lr_dens),
                             ("color_grads", "d_color_grads", lr_grads)):
             self.o.adam(self.scene[key], g[gk], self.m[key], self.v[key], self.step, lr)
+        if self.use_sh:
+            p = self.sh.astype(self.o.np)
+            self.o.adam(p, g["d_sh"], self.m_sh, self.v_sh, self.step, lr_sh)
+            self.sh = p.astype(np.float32)
         return loss, fwd, g

@@ -157,35 +157,82 @@ static const R C3_0 = (R)-0.5900435899266435, C3_1 = (R)2.890611442640554, C3_2 
                C3_3 = (R)0.3731763325901154, C3_4 = (R)-0.4570457994644658, C3_5 = (R)1.445305721320277,
                C3_6 = (R)-0.5900435899266435;
 
-static inline float half_to_float(uint16_t h) {
-    uint32_t s = (uint32_t)(h >> 15) << 31, e = (h >> 10) & 0x1F, m = h & 0x3FF, bits;
-    if (e == 0) {
-        if (m == 0) bits = s;
-        else { /* subnormal */
-            e = 127 - 15 + 1;
-            while (!(m & 0x400)) { m <<= 1; e--; }
-            m &= 0x3FF;
-            bits = s | (e << 23) | (m << 13);
-        }
-    } else if (e == 31) bits = s | 0x7F800000u | (m << 13);
-    else bits = s | ((e - 15 + 127) << 23) | (m << 13);
-    float f;
-    memcpy(&f, &bits, 4);
-    return f;
+/* SH basis value i at unit direction (x, y, z), as the reference evaluates it
+ * term by term (project_compute.wgsl:282-305): the coefficient multiplies the
+ * product of the constant and the direction monomial. */
+static inline R sh_basis(uint32_t i, R x, R y, R z) {
+    R xx = x * x, yy = y * y, zz = z * z;
+    switch (i) {
+        case 0: return C0;
+        case 1: return -(C1 * y);
+        case 2: return C1 * z;
+        case 3: return -(C1 * x);
+        case 4: return C2_0 * (x * y);
+        case 5: return C2_1 * (y * z);
+        case 6: return C2_2 * ((R)2 * zz - xx - yy);
+        case 7: return C2_3 * (x * z);
+        case 8: return C2_4 * (xx - yy);
+        case 9: return C3_0 * y * ((R)3 * xx - yy);
+        case 10: return C3_1 * x * y * z;
+        case 11: return C3_2 * y * ((R)4 * zz - xx - yy);
+        case 12: return C3_3 * z * ((R)2 * zz - (R)3 * xx - (R)3 * yy);
+        case 13: return C3_4 * x * ((R)4 * zz - xx - yy);
+        case 14: return C3_5 * z * (xx - yy);
+        default: return C3_6 * x * (xx - (R)3 * yy);
+    }
 }
-static inline R read_sh_f16(const uint32_t* sh, uint32_t base, uint32_t i) {
-    uint32_t w = sh[base + i / 2];
-    uint16_t h = (i & 1u) ? (uint16_t)(w >> 16) : (uint16_t)(w & 0xFFFF);
-    return (R)half_to_float(h);
+
+/* d basis_i / d(x, y, z), direction components treated as independent. */
+static inline V3 sh_basis_grad(uint32_t i, R x, R y, R z) {
+    R xx = x * x, yy = y * y, zz = z * z;
+    switch (i) {
+        case 0: return v3(0, 0, 0);
+        case 1: return v3(0, -C1, 0);
+        case 2: return v3(0, 0, C1);
+        case 3: return v3(-C1, 0, 0);
+        case 4: return v3(C2_0 * y, C2_0 * x, 0);
+        case 5: return v3(0, C2_1 * z, C2_1 * y);
+        case 6: return v3(-(R)2 * C2_2 * x, -(R)2 * C2_2 * y, (R)4 * C2_2 * z);
+        case 7: return v3(C2_3 * z, 0, C2_3 * x);
+        case 8: return v3((R)2 * C2_4 * x, -(R)2 * C2_4 * y, 0);
+        case 9: return v3((R)6 * C3_0 * x * y, C3_0 * ((R)3 * xx - (R)3 * yy), 0);
+        case 10: return v3(C3_1 * y * z, C3_1 * x * z, C3_1 * x * y);
+        case 11: return v3(-(R)2 * C3_2 * x * y, C3_2 * ((R)4 * zz - xx - (R)3 * yy), (R)8 * C3_2 * y * z);
+        case 12: return v3(-(R)6 * C3_3 * x * z, -(R)6 * C3_3 * y * z, C3_3 * ((R)6 * zz - (R)3 * xx - (R)3 * yy));
+        case 13: return v3(C3_4 * ((R)4 * zz - (R)3 * xx - yy), -(R)2 * C3_4 * x * y, (R)8 * C3_4 * x * z);
+        case 14: return v3((R)2 * C3_5 * x * z, -(R)2 * C3_5 * y * z, C3_5 * (xx - yy));
+        default: return v3(C3_6 * ((R)3 * xx - (R)3 * yy), -(R)6 * C3_6 * x * y, 0);
+    }
+}
+
+/* d softplus(x) / dx (crates/rmesh-util/src/wgsl/math.wgsl:27-33). */
+static inline R dsoftplus(R x) {
+    if (x * (R)10 > (R)20) return (R)1;
+    R e = REXP((R)10 * x);
+    return safe_div(e, (R)1 + e);
+}
+
+/* Unit direction from the camera to the tet centroid and the centroid itself
+ * (project_compute.wgsl:268-273). */
+static inline R sh_dir(const V3 v[4], const R* cam3, V3* centroid, V3* dir) {
+    *centroid = vscale(vadd(vadd(vadd(v[0], v[1]), v[2]), v[3]), (R)0.25);
+    V3 raw = vsub(*centroid, v3(cam3[0], cam3[1], cam3[2]));
+    R len = RSQRT(vdot(raw, raw));
+    *dir = v3(0, 0, 0);
+    if (len > (R)0) *dir = v3(raw.x / len, raw.y / len, raw.z / len);
+    return len;
 }
 
 /* ======================================================================== */
 /* orc_project -- project_compute.wgsl:88-325 (per tet id).                 */
 /* Outputs, indexed by tet id: visible (0/1), tiles_touched, colors[3M].    */
-/* sh_packed == NULL selects the base_colors copy branch (:319-324).        */
+/* sh == NULL selects the base_colors copy branch (:319-324).  sh holds the  */
+/* coefficient values [M][3][nc] the shader reads: the reference stores    */
+/* them as f16 (crates/rmesh-viewer/src/gpu_state.rs:60-88), so callers    */
+/* pass f16-rounded values for parity and unrounded ones for f64 checks.  */
 /* ======================================================================== */
 static void project_one(uint32_t t, const R* verts, const uint32_t* idx, const R* dens, const R* cgrad,
-                        const R* circ, const R* base, const uint32_t* sh, int sh_degree, const R* vp,
+                        const R* circ, const R* base, const R* sh, int sh_degree, const R* vp,
                         const R* cam3, R W, R H, uint32_t ts, uint8_t* visible, uint32_t* tiles_touched,
                         R* colors) {
     (void)circ;
@@ -279,43 +326,38 @@ static void project_one(uint32_t t, const R* verts, const uint32_t* idx, const R
 
     /* colors (project_compute.wgsl:264-324) */
     if (sh != NULL) {
-        V3 centroid = vscale(vadd(vadd(vadd(v[0], v[1]), v[2]), v[3]), (R)0.25);
-        V3 cam = v3(cam3[0], cam3[1], cam3[2]);
-        V3 raw = vsub(centroid, cam);
-        R len = RSQRT(vdot(raw, raw));
-        V3 dir = v3(0, 0, 0);
-        if (len > (R)0) dir = v3(raw.x / len, raw.y / len, raw.z / len);
+        V3 centroid, dir;
+        sh_dir(v, cam3, &centroid, &dir);
         R x = dir.x, y = dir.y, z = dir.z;
         uint32_t deg = (uint32_t)sh_degree;
         uint32_t nc = (deg + 1u) * (deg + 1u);
-        uint32_t stride = nc * 3u;
-        uint32_t sh_base = t * ((stride + 1u) / 2u);
+        const R* co = sh + (size_t)t * 3u * nc;
         R rgb[3];
         for (uint32_t c = 0; c < 3; ++c) {
-            uint32_t o = c * nc;
-            R val = C0 * read_sh_f16(sh, sh_base, o);
+            const R* q = co + c * nc;
+            R val = C0 * q[0];
             if (deg >= 1u) {
-                val -= C1 * y * read_sh_f16(sh, sh_base, o + 1u);
-                val += C1 * z * read_sh_f16(sh, sh_base, o + 2u);
-                val -= C1 * x * read_sh_f16(sh, sh_base, o + 3u);
+                val -= C1 * y * q[1];
+                val += C1 * z * q[2];
+                val -= C1 * x * q[3];
             }
             if (deg >= 2u) {
                 R xx = x * x, yy = y * y, zz = z * z, xy = x * y, yz = y * z, xz = x * z;
-                val += C2_0 * xy * read_sh_f16(sh, sh_base, o + 4u);
-                val += C2_1 * yz * read_sh_f16(sh, sh_base, o + 5u);
-                val += C2_2 * ((R)2 * zz - xx - yy) * read_sh_f16(sh, sh_base, o + 6u);
-                val += C2_3 * xz * read_sh_f16(sh, sh_base, o + 7u);
-                val += C2_4 * (xx - yy) * read_sh_f16(sh, sh_base, o + 8u);
+                val += C2_0 * xy * q[4];
+                val += C2_1 * yz * q[5];
+                val += C2_2 * ((R)2 * zz - xx - yy) * q[6];
+                val += C2_3 * xz * q[7];
+                val += C2_4 * (xx - yy) * q[8];
             }
             if (deg >= 3u) {
                 R xx = x * x, yy = y * y, zz = z * z;
-                val += C3_0 * y * ((R)3 * xx - yy) * read_sh_f16(sh, sh_base, o + 9u);
-                val += C3_1 * x * y * z * read_sh_f16(sh, sh_base, o + 10u);
-                val += C3_2 * y * ((R)4 * zz - xx - yy) * read_sh_f16(sh, sh_base, o + 11u);
-                val += C3_3 * z * ((R)2 * zz - (R)3 * xx - (R)3 * yy) * read_sh_f16(sh, sh_base, o + 12u);
-                val += C3_4 * x * ((R)4 * zz - xx - yy) * read_sh_f16(sh, sh_base, o + 13u);
-                val += C3_5 * z * (xx - yy) * read_sh_f16(sh, sh_base, o + 14u);
-                val += C3_6 * x * (xx - (R)3 * yy) * read_sh_f16(sh, sh_base, o + 15u);
+                val += C3_0 * y * ((R)3 * xx - yy) * q[9];
+                val += C3_1 * x * y * z * q[10];
+                val += C3_2 * y * ((R)4 * zz - xx - yy) * q[11];
+                val += C3_3 * z * ((R)2 * zz - (R)3 * xx - (R)3 * yy) * q[12];
+                val += C3_4 * x * ((R)4 * zz - xx - yy) * q[13];
+                val += C3_5 * z * (xx - yy) * q[14];
+                val += C3_6 * x * (xx - (R)3 * yy) * q[15];
             }
             rgb[c] = val + (R)0.5;
         }
@@ -328,13 +370,13 @@ static void project_one(uint32_t t, const R* verts, const uint32_t* idx, const R
 }
 
 EXPORT int SFX(orc_project)(int64_t M, const R* verts, const uint32_t* idx, const R* dens, const R* cgrad,
-                            const R* circ, const R* base, const uint32_t* sh_packed, int sh_degree,
+                            const R* circ, const R* base, const R* sh, int sh_degree,
                             const R* vp, const R* cam, int W, int H, int tile_size, uint8_t* visible,
                             uint32_t* tiles_touched, R* colors) {
     R Wf = (R)W, Hf = (R)H;
 #pragma omp parallel for schedule(static)
     for (int64_t t = 0; t < M; ++t)
-        project_one((uint32_t)t, verts, idx, dens, cgrad, circ, base, sh_packed, sh_degree, vp, cam, Wf, Hf,
+        project_one((uint32_t)t, verts, idx, dens, cgrad, circ, base, sh, sh_degree, vp, cam, Wf, Hf,
                     (uint32_t)tile_size, visible, tiles_touched, colors);
     return 0;
 }
@@ -909,6 +951,66 @@ EXPORT void SFX(orc_backward)(const R* verts, const uint32_t* idx, const R* colo
         for (int64_t tile = 0; tile < ntiles; ++tile)
             backward_tile(&cm, tile, verts, idx, colors, dens, cgrad, vals, ranges, dl, rendered, d_verts, d_dens,
                           d_cgrad, d_base, 1);
+    }
+}
+
+/* ======================================================================== */
+/* orc_sh_backward -- adjoint of the SH colour (project_compute.wgsl:264-318) */
+/* which the reference does not have.  For each tet with visible[t], chains  */
+/* d_colors (the adjoint's colour gradient) through softplus, the SH basis,   */
+/* the colour-gradient offset dot(g, v0 - centroid) and the view direction   */
+/* normalize(centroid - cam): writes d_sh [M][3][nc] and ADDS to d_verts     */
+/* [3N] and d_cgrad [3M].  Serial (deterministic vertex sums).               */
+/* ======================================================================== */
+EXPORT void SFX(orc_sh_backward)(int64_t M, const R* verts, const uint32_t* idx, const R* cgrad, const R* sh,
+                                 int sh_degree, const R* cam3, const uint8_t* visible, const R* d_colors,
+                                 R* d_sh, R* d_verts, R* d_cgrad) {
+    uint32_t nc = (uint32_t)((sh_degree + 1) * (sh_degree + 1));
+    memset(d_sh, 0, sizeof(R) * (size_t)M * 3u * nc);
+    for (int64_t t = 0; t < M; ++t) {
+        if (!visible[t]) continue;
+        R dc[3] = {d_colors[3 * t], d_colors[3 * t + 1], d_colors[3 * t + 2]};
+        if (dc[0] == (R)0 && dc[1] == (R)0 && dc[2] == (R)0) continue;
+        V3 v[4];
+        for (int k = 0; k < 4; ++k) v[k] = load_v3(verts, idx[4 * t + k]);
+        V3 centroid, dir;
+        R len = sh_dir(v, cam3, &centroid, &dir);
+        const R* co = sh + (size_t)t * 3u * nc;
+        R* dco = d_sh + (size_t)t * 3u * nc;
+        V3 g = load_v3(cgrad, t);
+        V3 v0c = vsub(v[0], centroid);
+        R off = vdot(g, v0c);
+        R sum_drgb = 0;
+        V3 d_dir = v3(0, 0, 0);
+        for (uint32_t c = 0; c < 3; ++c) {
+            R val = 0;
+            for (uint32_t i = 0; i < nc; ++i) val += sh_basis(i, dir.x, dir.y, dir.z) * co[c * nc + i];
+            R drgb = dc[c] * dsoftplus(val + (R)0.5 + off);
+            sum_drgb += drgb;
+            for (uint32_t i = 0; i < nc; ++i) {
+                dco[c * nc + i] = drgb * sh_basis(i, dir.x, dir.y, dir.z);
+                d_dir = vadd(d_dir, vscale(sh_basis_grad(i, dir.x, dir.y, dir.z), drgb * co[c * nc + i]));
+            }
+        }
+        /* offset = dot(g, v0 - centroid) */
+        d_cgrad[3 * t] += sum_drgb * v0c.x;
+        d_cgrad[3 * t + 1] += sum_drgb * v0c.y;
+        d_cgrad[3 * t + 2] += sum_drgb * v0c.z;
+        V3 d_centroid = vscale(g, -sum_drgb);
+        V3 d_v0 = vscale(g, sum_drgb);
+        /* dir = raw / |raw|, raw = centroid - cam */
+        if (len > (R)0) {
+            R dd = vdot(dir, d_dir);
+            d_centroid = vadd(d_centroid, vscale(vsub(d_dir, vscale(dir, dd)), (R)1 / len));
+        }
+        for (int k = 0; k < 4; ++k) {
+            uint32_t vi = idx[4 * t + k];
+            V3 dv = vscale(d_centroid, (R)0.25);
+            if (k == 0) dv = vadd(dv, d_v0);
+            d_verts[3 * vi] += dv.x;
+            d_verts[3 * vi + 1] += dv.y;
+            d_verts[3 * vi + 2] += dv.z;
+        }
     }
 }
 

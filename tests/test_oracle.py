@@ -364,3 +364,82 @@ def test_single_tet_loss_decreases():
     assert losses[0] > 0
     assert losses[9] < losses[0]
     assert losses[-1] < 0.01 * losses[0], (losses[0], losses[-1])
+
+
+def _sh_scene(seed=3, points=60, degree=3):
+    from rmesh_b200.scenes import make_scene, uniform_cloud
+
+    rng = np.random.default_rng(seed)
+    sc = make_scene(uniform_cloud(points, rng, -0.6, 0.6), rng, sh_degree=degree)
+    return sc
+
+
+def test_sh_degree0_colour_is_softplus_of_dc(oracle32):
+    """project_compute.wgsl:264-318 at degree 0: colour = softplus(C0*sh0 + 0.5 +
+    dot(g, v0 - centroid)) per channel, with the f16-rounded coefficient."""
+    from rmesh_b200.scenes import SH_C0
+
+    sc = _sh_scene(degree=0)
+    cam = _cam((1.8, -1.2, 0.9), (0, 0, 0), 60.0)
+    shv = oracle32.sh_values(sc["sh_coeffs"])
+    vis, _, col = oracle32.project(sc, cam, 12, sh=shv, sh_degree=0)
+    v = sc["vertices"].reshape(-1, 3).astype(np.float64)
+    t = sc["indices"].reshape(-1, 4)
+    cen = v[t].mean(axis=1)
+    off = np.einsum("ij,ij->i", sc["color_grads"].reshape(-1, 3), v[t[:, 0]] - cen)
+    rgb = SH_C0 * shv.reshape(-1, 3).astype(np.float64) + 0.5 + off[:, None]
+    want = np.where(rgb * 10 > 20, rgb, 0.1 * np.log1p(np.exp(10 * rgb)))
+    m = vis.astype(bool)
+    assert m.sum() > 20
+    np.testing.assert_allclose(col.reshape(-1, 3)[m], want[m], rtol=2e-5, atol=2e-6)
+
+
+def test_sh_fd_gradients(oracle64):
+    """Adjoint of the SH colour (no reference counterpart): central finite
+    differences in float64, step 1e-4, on sampled coefficients, colour gradients,
+    densities and vertices of a degree-3 scene (the gradient check of the
+    10k-point degree-3 configuration, at a size the oracle finishes quickly)."""
+    sc = {k: (np.asarray(v, np.float64) if isinstance(v, np.ndarray) and v.dtype.kind == "f" else v)
+          for k, v in _sh_scene().items()}
+    deg = sc["sh_degree"]
+    cam = _cam((1.9, -1.1, 0.8), (0, 0, 0), 60.0)
+    gt = np.random.default_rng(8).uniform(0, 1, (H, W, 3))
+    sh = oracle64.sh_values(sc["sh_coeffs"], f16=False)
+
+    def loss_of(scene, shv):
+        f = oracle64.forward_tiled(scene, cam, sh=shv, sh_degree=deg)
+        return oracle64.loss(f["image"], gt, 1)[0]
+
+    f = oracle64.forward_tiled(sc, cam, sh=sh, sh_degree=deg)
+    _, dl = oracle64.loss(f["image"], gt, 1)
+    g = oracle64.backward(sc, cam, dl, f, sh=sh, sh_degree=deg)
+    assert np.abs(g["d_base_colors"]).max() == 0.0
+    rng = np.random.default_rng(11)
+    eps = 1e-4
+    fails, checked = [], 0
+    for key, gkey, n in (("sh", "d_sh", 60), ("color_grads", "d_color_grads", 30), ("densities", "d_densities", 20),
+                         ("vertices", "d_vertices", 30)):
+        arr = sh if key == "sh" else sc[key]
+        # sample among parameters with a non-negligible gradient so the check has teeth
+        cand = np.nonzero(np.abs(g[gkey]) > 1e-6)[0]
+        assert cand.size >= 5, key
+        for i in rng.choice(cand, size=min(n, cand.size), replace=False):
+            vals = []
+            for sgn in (+1, -1):
+                a2 = arr.copy()
+                a2[i] += sgn * eps
+                if key == "sh":
+                    vals.append(loss_of(sc, a2))
+                else:
+                    sp = dict(sc)
+                    sp[key] = a2
+                    vals.append(loss_of(sp, sh))
+            num = (vals[0] - vals[1]) / (2 * eps)
+            ana = g[gkey][i]
+            err = abs(ana - num)
+            tol = 1e-3 if key in ("sh", "color_grads") else 0.10  # vertices/densities: pixel coverage steps
+            if err > tol * max(abs(ana), abs(num)) and err > 1e-7:
+                fails.append((key, int(i), float(ana), float(num)))
+            checked += 1
+    assert checked >= 100
+    assert len(fails) <= 2, fails  # a vertex step may cross a pixel-coverage edge
