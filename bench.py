@@ -5,9 +5,10 @@ set -- a Delaunay mesh of 100,000 points from an 8-component Gaussian mixture
 (~650k tets), 16 cameras on a sphere of radius U[2.5, 4] with resolutions drawn
 from {256^2, 512^2, 800x600, 1024^2}; one step renders all 16 views, computes
 the L2 loss against seeded targets, back-propagates and applies one Adam update
-(forward + backward + Adam).  Synthetic, seeded data; colours are the
-reference's base-colour training path (spherical harmonics are not evaluated by
-the reference's train_step).
+(forward + backward + Adam).  Synthetic, seeded data.  Colours are degree-3
+spherical harmonics (the benchmark's sh_degree 3), evaluated per view with the
+reference shader's formula and trained with lr_sh 2.5e-3; ``--sh-degree -1``
+selects the reference binding's base-colour training path instead.
 
 Line printed by rank 0 (one JSON object):
   value          train-steps/s of the batched, graph-captured path, inputs in HBM
@@ -42,6 +43,7 @@ sys.path.insert(0, ROOT)
 RES = ((256, 256), (512, 512), (800, 600), (1024, 1024))
 N_VIEWS = 16
 LR = dict(lr_verts=1e-4, lr_dens=1e-2, lr_grads=1e-3)
+LR_SH = 2.5e-3
 
 
 def res_text(res) -> str:
@@ -57,12 +59,12 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def build_workload(points: int, seed: int, rank: int, n_views: int = N_VIEWS, res=RES):
+def build_workload(points: int, seed: int, rank: int, n_views: int = N_VIEWS, res=RES, sh_degree: int = 3):
     from rmesh_b200.camera import orbit_cameras
     from rmesh_b200.scenes import gmm_cloud, make_scene
 
     rng = np.random.default_rng(seed)
-    scene = make_scene(gmm_cloud(points, rng), rng, sh_degree=0)
+    scene = make_scene(gmm_cloud(points, rng), rng, sh_degree=max(sh_degree, 0))
     cams = orbit_cameras(n_views, seed=seed + 1 + 1000 * rank, radius=(2.5, 4.0), resolutions=res)
     trng = np.random.default_rng(seed + 2 + 1000 * rank)
     gts = [trng.uniform(0, 1, (c.height, c.width, 3)).astype(np.float32) for c in cams]
@@ -141,10 +143,12 @@ def run_gpu(args):
     from rmesh_b200 import RMeshRenderer
     from rmesh_b200 import _lib
 
-    scene, cams, gts = build_workload(args.points, args.seed, rank, args.views, args.res)
+    scene, cams, gts = build_workload(args.points, args.seed, rank, args.views, args.res, args.sh_degree)
+    sh_kw = dict(sh_coeffs=scene["sh_coeffs"], sh_degree=args.sh_degree) if args.sh_degree >= 0 else {}
+    lr_sh = LR_SH if args.sh_degree >= 0 else 0.0
     r = RMeshRenderer(scene["vertices"], scene["indices"], scene["base_colors"], scene["densities"],
                       scene["color_grads"], scene["circumdata"], cams[0].width, cams[0].height,
-                      tile_size=args.tile_size, device=local)
+                      tile_size=args.tile_size, device=local, **sh_kw)
     stream = torch.cuda.Stream(device=local)
     r.set_stream(stream.cuda_stream)
     n_pix = sum(c.width * c.height for c in cams)
@@ -156,12 +160,12 @@ def run_gpu(args):
 
     def step(mode, gt):
         if dist is None:
-            return r.train_step_views(cams, gt, loss_type=1, mode=mode, **LR)
+            return r.train_step_views(cams, gt, loss_type=1, mode=mode, lr_sh=lr_sh, **LR)
         # data parallel: this rank's views -> sum of all ranks' gradients -> Adam
         losses = r.accumulate_views(cams, gt, loss_type=1, mode=mode)
         with torch.cuda.stream(stream):
             dist.all_reduce(slots)
-        r.apply_adam(**LR)
+        r.apply_adam(lr_sh=lr_sh, **LR)
         return losses
 
     def timed(mode, gt, steps):
@@ -224,14 +228,7 @@ def run_gpu(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded GMM Delaunay mesh, seeded targets)",
-        "config": {
-            "workload": f"batched: {args.points}-point 8-component GMM Delaunay mesh ({r.n_tets} tets), "
-                        f"{args.views} views from {{{res_text(args.res)}}}, L2 loss, Adam",
-            "n_tets": r.n_tets, "n_vertices": r.n_vertices, "views_per_gpu": args.views,
-            "pixels_per_step_per_gpu": n_pix, "tile_size": args.tile_size, "color_mode": "base_colors",
-            "parallelism": f"dp{world} (views sharded, gradients summed)" if world > 1 else "single GPU",
-            "l2": "inputs larger than L2 (mesh records + pair lists > 126 MB per step)",
-        },
+        "config": workload_config(args, r.n_tets, r.n_vertices, n_pix, world),
         "mpix_per_s": round(world * n_pix / (ms_graph * 1e-3) / 1e6, 2),
         "plain": {"value": round(world * 1000.0 / ms_plain, 4), "unit": "train-steps/s", "ms_per_step": round(ms_plain, 4)},
         "batched_graph_vs_plain": round(ms_plain / ms_graph, 3),
@@ -258,6 +255,26 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
+def workload_config(args, n_tets, n_vertices, n_pix, world):
+    """The config object of the JSON line (both arms)."""
+    return {
+        "workload": f"batched: {args.points}-point 8-component GMM Delaunay mesh ({n_tets} tets), "
+                    f"{args.views} views from {{{res_text(args.res)}}}, L2 loss, Adam",
+        "n_tets": n_tets, "n_vertices": n_vertices, "views_per_gpu": args.views,
+        "pixels_per_step_per_gpu": n_pix, "tile_size": args.tile_size,
+        "color_mode": f"sh_degree {args.sh_degree}" if args.sh_degree >= 0 else "base_colors",
+        "parallelism": f"dp{world} (views sharded, gradients summed)" if world > 1 else "single GPU",
+        "l2": "inputs larger than L2 (mesh records + pair lists > 126 MB per step)",
+    }
+
+
+def _oracle_sh(o, scene, args):
+    """The oracle's SH inputs for the workload's colour mode."""
+    if args.sh_degree < 0:
+        return None, 0
+    return o.sh_values(scene["sh_coeffs"]), args.sh_degree
+
+
 def cpu_baseline(scene, cams, gts, args, budget_s=20.0):
     """The oracle's train step (project, emit, sort, ranges, rasterize, loss,
     adjoint, Adam) on all host cores for views of the step until ~budget_s,
@@ -267,15 +284,16 @@ def cpu_baseline(scene, cams, gts, args, budget_s=20.0):
 
     o = Oracle("f32")
     threads = o.max_threads
+    shv, deg = _oracle_sh(o, scene, args)
     # cheapest views first so the sample covers several views within the budget
     order = sorted(range(len(cams)), key=lambda i: cams[i].width * cams[i].height)
     t0 = time.perf_counter()
     px_done, views_done = 0, 0
     for i in order:
         cam, gt = cams[i], gts[i]
-        fwd = o.forward_tiled(scene, cam, args.tile_size)
+        fwd = o.forward_tiled(scene, cam, args.tile_size, sh=shv, sh_degree=deg)
         _, dl = o.loss(fwd["image"], gt, 1)
-        o.backward(scene, cam, dl, fwd, args.tile_size, threads=threads)
+        o.backward(scene, cam, dl, fwd, args.tile_size, threads=threads, sh=shv, sh_degree=deg)
         px_done += cam.width * cam.height
         views_done += 1
         if time.perf_counter() - t0 > budget_s:
@@ -295,7 +313,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    scene, cams, gts = build_workload(args.points, args.seed, 0, args.views, args.res)
+    scene, cams, gts = build_workload(args.points, args.seed, 0, args.views, args.res, args.sh_degree)
     n_pix = sum(c.width * c.height for c in cams)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import Oracle
@@ -305,10 +323,12 @@ def run_reference(args):
     cam = min(cams, key=lambda c: c.width * c.height)
     gt = gts[cams.index(cam)]
 
+    shv, deg = _oracle_sh(o, scene, args)
+
     def one():
-        fwd = o.forward_tiled(scene, cam, args.tile_size)
+        fwd = o.forward_tiled(scene, cam, args.tile_size, sh=shv, sh_degree=deg)
         _, dl = o.loss(fwd["image"], gt, 1)
-        o.backward(scene, cam, dl, fwd, args.tile_size, threads=threads)
+        o.backward(scene, cam, dl, fwd, args.tile_size, threads=threads, sh=shv, sh_degree=deg)
 
     for _ in range(args.warmup):
         one()
@@ -325,8 +345,8 @@ def run_reference(args):
         "value": v, "unit": "train-steps/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t_step * 1e3, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded GMM Delaunay mesh, seeded targets)",
-        "config": {"workload": f"batched: {args.points}-point 8-component GMM Delaunay mesh, {args.views} views "
-                               f"from {{{res_text(args.res)}}}, L2 loss, Adam"},
+        "config": workload_config(args, scene["indices"].size // 4, scene["vertices"].size // 3, n_pix,
+                                  int(os.environ.get("WORLD_SIZE", "1"))),
         "cpu_baseline": {"value": v, "unit": "train-steps/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "train-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference's own pipeline is wgpu (Vulkan/Metal) and cannot run here; this is its CPU port",
@@ -344,6 +364,8 @@ def main():
     ap.add_argument("--tile-size", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--views", type=int, default=N_VIEWS, help="views per step (default: the 16-view workload)")
+    ap.add_argument("--sh-degree", type=int, default=3, choices=[-1, 0, 1, 2, 3],
+                    help="SH degree of the colours (-1: base colours)")
     ap.add_argument("--res", default=None,
                     help="comma-separated WxH choices for the views (default 256x256,512x512,800x600,1024x1024); "
                          "smaller cases serve profiler captures")

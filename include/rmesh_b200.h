@@ -29,7 +29,7 @@
 extern "C" {
 #endif
 
-#define RMESH_ABI_VERSION 1
+#define RMESH_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define RMESH_API __attribute__((visibility("default")))
@@ -65,7 +65,14 @@ typedef struct {
   int32_t aux_dim;           /* reference aux_dim (only 0 is supported) */
   int32_t tile_size;         /* 0 -> 12, the reference's hard-coded value (lib.rs:442) */
   int32_t device;            /* CUDA device ordinal, -1 = current */
-  int32_t reserved[3];
+  int32_t sh_degree;         /* 0..3, used when sh_coeffs is set */
+  const float* sh_coeffs;    /* NULL: colours are base_colors (the reference's training
+                              * path, lib.rs:393-439); else [M][3][(sh_degree+1)^2]
+                              * coefficients (coefficient c*nc + i of channel c), colour =
+                              * softplus(SH(dir) + 0.5 + dot(g, v0 - centroid)) per view
+                              * (project_compute.wgsl:264-318), read as f16 like the
+                              * reference's packed buffer (rmesh-viewer/src/gpu_state.rs:60-88) */
+  int32_t reserved[2];
 } RmeshSceneDesc;
 
 /* One view: the three arrays of the reference camera methods (lib.rs:1040-1048)
@@ -87,7 +94,8 @@ typedef struct {
   float lr_base;      /* 0 keeps base colours fixed, as the reference train_step does */
   int32_t loss_type;  /* 0 = L1, 1 = L2 */
   int32_t mode;       /* RMESH_MODE_* */
-  int32_t reserved[2];
+  float lr_sh;        /* SH coefficients' learning rate (SH contexts; no reference counterpart) */
+  int32_t reserved;
 } RmeshTrainOpts;
 
 #define RMESH_MODE_PLAIN 0    /* one launch sequence per view, one tile per CTA */
@@ -127,6 +135,16 @@ RMESH_API int rmesh_get_params(RmeshCtx* ctx, float* vertices, float* base_color
 /* getters step/width/height, lib.rs:2688-2705 */
 RMESH_API int rmesh_get_info(RmeshCtx* ctx, RmeshInfo* info);
 
+/* SH coefficients of a context created with sh_coeffs (no reference
+ * counterpart: the reference's binding trains base colours only).  get/update
+ * copy [M][3][nc] floats; get_sh_grad returns the coefficient gradient of the
+ * last rmesh_backward / training call; set_lr_sh sets the learning rate that
+ * rmesh_train_step applies to them (default 0). */
+RMESH_API int rmesh_update_sh(RmeshCtx* ctx, const float* sh_coeffs);
+RMESH_API int rmesh_get_sh(RmeshCtx* ctx, float* sh_coeffs);
+RMESH_API int rmesh_get_sh_grad(RmeshCtx* ctx, float* d_sh_coeffs);
+RMESH_API int rmesh_set_lr_sh(RmeshCtx* ctx, float lr_sh);
+
 /* ---- the path ------------------------------------------------------------- */
 /* forward_tiled, lib.rs:1041-1204: project -> bin -> sort -> ranges -> composite.
  * rgba_out [H][W][4]; aux_out [H][W][8] or NULL (render_aux). */
@@ -155,7 +173,8 @@ RMESH_API int rmesh_train_step_views(RmeshCtx* ctx, const RmeshCamera* cams, int
 /* Data-parallel split of rmesh_train_step_views (no reference counterpart):
  * accumulate the gradient of this rank's views into the context's per-tet
  * gradient slots (zeroed first, no Adam); expose those slots (device memory,
- * n_floats = 20 * M) so the caller can sum them across ranks, e.g. with an
+ * n_floats = 20 * M, plus 3 * nc * M SH coefficient gradients after them in
+ * an SH context) so the caller can sum them across ranks, e.g. with an
  * NCCL all-reduce; then apply one Adam update from the slots. */
 RMESH_API int rmesh_accumulate_views(RmeshCtx* ctx, const RmeshCamera* cams, int32_t n_views, const float* gt_rgb,
                                      const RmeshTrainOpts* opts, float* loss_out);
@@ -203,11 +222,12 @@ RMESH_API int rmesh_debug_ranges(RmeshCtx* ctx, uint32_t* ranges, uint64_t n_til
 /* ---- profiling -------------------------------------------------------------- */
 /* When enabled, CUDA events bracket each stage on the context stream; the
  * accumulated milliseconds are returned by rmesh_stage_times in the order
- * records, project, tet_sort, emit, pair_sort, ranges, composite, adam.
+ * records, project, tet_sort, emit, pair_sort, ranges, composite, adam,
+ * sh_adjoint (the SH colour adjoint; zero without SH colours).
  * ms_out has RMESH_N_STAGES entries; launches_out has RMESH_N_STAGES + 1
  * (per-stage span counts, then the number of kernels launched).  Both are
  * reset by the call. */
-#define RMESH_N_STAGES 8
+#define RMESH_N_STAGES 9
 RMESH_API int rmesh_set_profiling(RmeshCtx* ctx, int32_t on);
 RMESH_API int rmesh_stage_times(RmeshCtx* ctx, float* ms_out, int32_t* launches_out);
 

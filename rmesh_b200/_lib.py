@@ -25,8 +25,8 @@ RMESH_ERR_TOO_LARGE = 8
 RMESH_STATIC_MAX_TETS = 1 << 24
 
 MODE_PLAIN, MODE_BATCHED, MODE_GRAPH = 0, 1, 2
-N_STAGES = 8
-STAGE_NAMES = ("records", "project", "tet_sort", "emit", "pair_sort", "ranges", "composite", "adam")
+N_STAGES = 9
+STAGE_NAMES = ("records", "project", "tet_sort", "emit", "pair_sort", "ranges", "composite", "adam", "sh_adjoint")
 
 # every symbol declared in include/rmesh_b200.h
 EXPORTED = (
@@ -35,7 +35,7 @@ EXPORTED = (
     "rmesh_forward_tiled", "rmesh_backward", "rmesh_train_step", "rmesh_train_step_views",
     "rmesh_debug_tiles_touched", "rmesh_debug_pairs", "rmesh_debug_ranges", "rmesh_set_profiling",
     "rmesh_stage_times", "rmesh_accumulate_views", "rmesh_grad_slots", "rmesh_apply_adam",
-    "rmesh_count_tiles_static",
+    "rmesh_count_tiles_static", "rmesh_update_sh", "rmesh_get_sh", "rmesh_get_sh_grad", "rmesh_set_lr_sh",
 )
 
 COUNTERS_BYTES = 792  # sizeof(rm::Counters), read back once per training run
@@ -47,7 +47,8 @@ class SceneDesc(ctypes.Structure):
         ("vertices", ctypes.c_void_p), ("indices", ctypes.c_void_p), ("base_colors", ctypes.c_void_p),
         ("densities", ctypes.c_void_p), ("color_grads", ctypes.c_void_p), ("circumdata", ctypes.c_void_p),
         ("width", ctypes.c_int32), ("height", ctypes.c_int32), ("aux_dim", ctypes.c_int32),
-        ("tile_size", ctypes.c_int32), ("device", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3),
+        ("tile_size", ctypes.c_int32), ("device", ctypes.c_int32), ("sh_degree", ctypes.c_int32),
+        ("sh_coeffs", ctypes.c_void_p), ("reserved", ctypes.c_int32 * 2),
     ]
 
 
@@ -62,7 +63,7 @@ class TrainOpts(ctypes.Structure):
     _fields_ = [
         ("lr_verts", ctypes.c_float), ("lr_dens", ctypes.c_float), ("lr_grads", ctypes.c_float),
         ("lr_base", ctypes.c_float), ("loss_type", ctypes.c_int32), ("mode", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 2),
+        ("lr_sh", ctypes.c_float), ("reserved", ctypes.c_int32),
     ]
 
 
@@ -114,6 +115,10 @@ def load() -> ctypes.CDLL:
         "rmesh_grad_slots": ([vp, P(vp), P(u64)], ctypes.c_int),
         "rmesh_apply_adam": ([vp, P(TrainOpts)], ctypes.c_int),
         "rmesh_count_tiles_static": ([vp, u64, vp, vp, u64, P(Camera), i32, vp, vp, vp, vp], ctypes.c_int),
+        "rmesh_update_sh": ([vp, vp], ctypes.c_int),
+        "rmesh_get_sh": ([vp, vp], ctypes.c_int),
+        "rmesh_get_sh_grad": ([vp, vp], ctypes.c_int),
+        "rmesh_set_lr_sh": ([vp, f32], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

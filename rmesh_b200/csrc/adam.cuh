@@ -8,9 +8,10 @@
 // Adam restates crates/rmesh-train/src/wgsl/adam_compute.wgsl:121-149 per
 // element (NaN -> 0, clip to +-1e20, bias correction exp(step*ln(beta)),
 // safe_div / safe_sqrt), for every group in ONE launch: vertices (lr_verts),
-// densities (lr_dens), colour gradients (lr_grads), and base colours when
+// densities (lr_dens), colour gradients (lr_grads), base colours when
 // lr_base > 0 (the reference's train_step leaves base colours untouched,
-// crates/rmesh-python/src/lib.rs:393-439, 2590-2626).  The step is skipped
+// crates/rmesh-python/src/lib.rs:393-439, 2590-2626), and SH coefficients
+// (lr_sh) when the mesh is coloured by spherical harmonics.  The step is skipped
 // entirely when the run raised an error (e.g. pair overflow), so the host can
 // grow its buffers and redo the step.
 #pragma once
@@ -51,6 +52,9 @@ struct AdamArgs {
   float* m_cgrad; float* v_cgrad;
   float* m_base; float* v_base;
   const float* grad_slot;
+  float* sh; float* m_sh; float* v_sh;  // SH coefficients (nullptr: base colours)
+  const float* d_sh;
+  long long n_sh;
   const uint32_t* csr_off;
   const uint32_t* csr_ref;
   const AdamParams* hp;
@@ -65,10 +69,13 @@ __global__ void __launch_bounds__(256) adam_kernel(AdamArgs a) {
   const float step_f = (float)hp.step;
   const float b1p = expf(step_f * logf(hp.beta1));
   const float b2p = expf(step_f * logf(hp.beta2));
-  const long long total = (long long)a.N + a.M;
+  const long long total = (long long)a.N + a.M + (a.sh && hp.lr_sh > 0.0f ? a.n_sh : 0);
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
-    if (i < a.N) {
+    if (i >= (long long)a.N + a.M) {
+      const size_t e = (size_t)(i - a.N - a.M);
+      adam_elem(a.sh[e], a.m_sh[e], a.v_sh[e], a.d_sh[e], hp.lr_sh, hp.beta1, hp.beta2, hp.eps, b1p, b2p);
+    } else if (i < a.N) {
       const uint32_t vtx = (uint32_t)i;
 #pragma unroll
       for (int c = 0; c < 3; ++c) {

@@ -24,6 +24,7 @@
 #include "bin.cuh"
 #include "common.cuh"
 #include "project.cuh"
+#include "sh.cuh"
 #include "sort.cuh"
 #include "tile.cuh"
 
@@ -65,7 +66,7 @@ struct DevBuf {
   }
 };
 
-enum Stage { kStRecords = 0, kStProject, kStTetSort, kStEmit, kStPairSort, kStRanges, kStComposite, kStAdam };
+enum Stage { kStRecords = 0, kStProject, kStTetSort, kStEmit, kStPairSort, kStRanges, kStComposite, kStAdam, kStShAdjoint };
 
 struct EventPair {
   int stage;
@@ -82,6 +83,9 @@ struct RmeshCtx {
   int width = 0, height = 0, tile_size = 12;
   float min_t = 0.0f;
   uint32_t step = 0;
+  int sh_degree = -1;   // -1: base colours; 0..3: colours from SH coefficients
+  int sh_nc = 0;        // (sh_degree + 1)^2
+  float lr_sh = 0.0f;   // SH learning rate of rmesh_train_step
   std::string err;
   int num_sms = 148;
 
@@ -89,10 +93,12 @@ struct RmeshCtx {
   DevBuf verts, idx, dens, cgrad, base, circ;
   DevBuf m_verts, v_verts, m_dens, v_dens, m_cgrad, v_cgrad, m_base, v_base;
   DevBuf rec, color4, grad_slot, csr_off, csr_ref;
+  DevBuf sh, m_sh, v_sh;  // SH coefficients [M][3][nc] and their Adam moments
 
   // per-run
   DevBuf views_d, counters_d, hp_d, sort_state, sort_status, scan_status;
   DevBuf vis_key, vis_val, vis_tet, vis_cnt, vis_proj, vis_view, vis_key_alt, vis_val_alt, tiles_touched;
+  DevBuf vis_color, vis_dcolor, vis_index;  // SH colours per entry, their gradients, (view, tet) -> entry
   DevBuf pair_key, pair_val, pair_key_alt, pair_val_alt, ranges;
   DevBuf rgba, aux, dl, gt, out_a, out_b, out_c, out_d;
   uint64_t cap_pairs = 0;
@@ -132,6 +138,12 @@ namespace {
 int fail(RmeshCtx* c, int code, const std::string& msg) {
   if (c) c->err = msg;
   return code;
+}
+
+// floats of the gradient buffer: 20 per tet, then (SH) 3 * nc per tet
+size_t grad_floats(const RmeshCtx* c) { return (size_t)c->M * (kGradSlot + (c->sh_degree >= 0 ? 3 * c->sh_nc : 0)); }
+float* sh_grad(const RmeshCtx* c) {
+  return c->sh_degree >= 0 ? c->grad_slot.as<float>() + (size_t)c->M * kGradSlot : nullptr;
 }
 
 #define CK(call)                                                                                  \
@@ -267,6 +279,11 @@ int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t
   CKR(ensure_buf(c, c->vis_cnt, items * 4));
   CKR(ensure_buf(c, c->vis_proj, items * 32));
   CKR(ensure_buf(c, c->vis_view, items * sizeof(TetView)));
+  if (c->sh_degree >= 0) {
+    CKR(ensure_buf(c, c->vis_color, items * 16));
+    CKR(ensure_buf(c, c->vis_dcolor, items * 16));
+    CKR(ensure_buf(c, c->vis_index, items * 4));
+  }
   CKR(ensure_buf(c, c->tiles_touched, items * 4));
   if (c->cap_pairs == 0) c->cap_pairs = std::max<uint64_t>(8 * items, 1u << 16);
   CKR(ensure_buf(c, c->pair_key, c->cap_pairs * 4));
@@ -355,6 +372,10 @@ int run_bin(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t tota
     pa.vis_view = c->vis_view.as<TetView>();
     pa.color4 = c->color4.as<float4>();
     pa.color_view_stride = 0;
+    pa.sh = c->sh_degree >= 0 ? c->sh.as<float>() : nullptr;
+    pa.sh_degree = c->sh_degree;
+    pa.vis_color = c->vis_color.as<float4>();
+    pa.vis_index = c->vis_index.as<uint32_t>();
     pa.tiles_touched = c->tiles_touched.as<uint32_t>();
     pa.status = status;
     pa.ticket = ticket;
@@ -454,9 +475,45 @@ TileArgs base_tile_args(RmeshCtx* c, const ViewParams* views_dev, int n_views, u
   ta.color4 = c->color4.as<float4>();
   ta.color_view_stride = 0;
   ta.grad_slot = c->grad_slot.as<float>();
+  if (c->sh_degree >= 0) {
+    ta.vis_color = c->vis_color.as<float4>();
+    ta.vis_dcolor = c->vis_dcolor.as<float4>();
+  }
   ta.counters = cnt;
   ta.hp = c->hp_d.as<AdamParams>();
   return ta;
+}
+
+// SH colours: clears the per-entry colour gradients before an adjoint launch
+int clear_dcolor(RmeshCtx* c, int n_views) {
+  if (c->sh_degree < 0) return RMESH_OK;
+  CK(cudaMemsetAsync(c->vis_dcolor.p, 0, (size_t)n_views * c->M * 16, c->stream));
+  return RMESH_OK;
+}
+
+// SH colours: the adjoint of the colour evaluation, after an adjoint launch
+int run_sh_backward(RmeshCtx* c, const ViewParams* views_dev, int n_views, bool capturing) {
+  if (c->sh_degree < 0) return RMESH_OK;
+  StageScope sc(c, kStShAdjoint, capturing);
+  ShBackwardArgs sa;
+  sa.M = (int)c->M;
+  sa.n_views = n_views;
+  sa.views = views_dev;
+  sa.rec = c->rec.as<TetRec>();
+  sa.sh = c->sh.as<float>();
+  sa.vis_index = c->vis_index.as<uint32_t>();
+  sa.vis_dcolor = c->vis_dcolor.as<float4>();
+  sa.d_sh = sh_grad(c);
+  sa.grad_slot = c->grad_slot.as<float>();
+  const unsigned blocks = (unsigned)((c->M + 127) / 128);
+  switch (c->sh_degree) {
+    case 0: sh_backward_kernel<0><<<blocks, 128, 0, c->stream>>>(sa); break;
+    case 1: sh_backward_kernel<1><<<blocks, 128, 0, c->stream>>>(sa); break;
+    case 2: sh_backward_kernel<2><<<blocks, 128, 0, c->stream>>>(sa); break;
+    default: sh_backward_kernel<3><<<blocks, 128, 0, c->stream>>>(sa); break;
+  }
+  CKL();
+  return RMESH_OK;
 }
 
 int sync_counters(RmeshCtx* c, int n) {
@@ -515,12 +572,17 @@ int launch_adam(RmeshCtx* c, int n_cnt, bool capturing) {
   aa.m_base = c->m_base.as<float>();
   aa.v_base = c->v_base.as<float>();
   aa.grad_slot = c->grad_slot.as<float>();
+  aa.sh = c->sh_degree >= 0 ? c->sh.as<float>() : nullptr;
+  aa.m_sh = c->m_sh.as<float>();
+  aa.v_sh = c->v_sh.as<float>();
+  aa.d_sh = sh_grad(c);
+  aa.n_sh = c->sh_degree >= 0 ? (long long)c->M * 3 * c->sh_nc : 0;
   aa.csr_off = c->csr_off.as<uint32_t>();
   aa.csr_ref = c->csr_ref.as<uint32_t>();
   aa.hp = c->hp_d.as<AdamParams>();
   aa.counters = c->counters_d.as<Counters>();
   aa.n_counters = n_cnt;
-  const int blocks = (int)std::min<int64_t>((c->N + c->M + 255) / 256, (int64_t)c->num_sms * 16);
+  const int blocks = (int)std::min<int64_t>((c->N + c->M + aa.n_sh + 255) / 256, (int64_t)c->num_sms * 16);
   adam_kernel<<<std::max(1, blocks), 256, 0, c->stream>>>(aa);
   CKL();
   return RMESH_OK;
@@ -557,7 +619,7 @@ int train_views(RmeshCtx* c, const RmeshCamera* cams, int n_views, const float* 
     hp.lr_dens = o->lr_dens;
     hp.lr_grads = o->lr_grads;
     hp.lr_base = o->lr_base;
-    hp.lr_sh = 0.0f;
+    hp.lr_sh = o->lr_sh;
     hp.beta1 = 0.9f;
     hp.beta2 = 0.999f;
     hp.eps = 1e-8f;
@@ -571,23 +633,31 @@ int train_views(RmeshCtx* c, const RmeshCamera* cams, int n_views, const float* 
     auto enqueue = [&](bool capturing) -> int {
       Counters* cnt = c->counters_d.as<Counters>();
       CK(cudaMemsetAsync(cnt, 0, sizeof(Counters) * n_cnt, c->stream));
-      CK(cudaMemsetAsync(c->grad_slot.p, 0, (size_t)c->M * kGradSlot * 4, c->stream));
+      CK(cudaMemsetAsync(c->grad_slot.p, 0, grad_floats(c) * 4, c->stream));
       CKR(run_records(c, capturing));
       ViewParams* vd = c->views_d.as<ViewParams>();
       if (plain) {
         for (int v = 0; v < n_views; ++v) {
           CKR(run_bin(c, vd + v, 1, view_tiles[v], cnt + v, capturing));
-          StageScope sc(c, kStComposite, capturing);
-          TileArgs ta = base_tile_args(c, vd + v, 1, view_tiles[v], cnt + v);
-          ta.gt_rgb = gt_dev;
-          CKR((launch_tile_m<kModeTrain, false>(c, ta, view_tiles[v], false)));
+          CKR(clear_dcolor(c, 1));
+          {
+            StageScope sc(c, kStComposite, capturing);
+            TileArgs ta = base_tile_args(c, vd + v, 1, view_tiles[v], cnt + v);
+            ta.gt_rgb = gt_dev;
+            CKR((launch_tile_m<kModeTrain, false>(c, ta, view_tiles[v], false)));
+          }
+          CKR(run_sh_backward(c, vd + v, 1, capturing));
         }
       } else {
         CKR(run_bin(c, vd, n_views, total_tiles, cnt, capturing));
-        StageScope sc(c, kStComposite, capturing);
-        TileArgs ta = base_tile_args(c, vd, n_views, total_tiles, cnt);
-        ta.gt_rgb = gt_dev;
-        CKR((launch_tile_m<kModeTrain, false>(c, ta, total_tiles, true)));
+        CKR(clear_dcolor(c, n_views));
+        {
+          StageScope sc(c, kStComposite, capturing);
+          TileArgs ta = base_tile_args(c, vd, n_views, total_tiles, cnt);
+          ta.gt_rgb = gt_dev;
+          CKR((launch_tile_m<kModeTrain, false>(c, ta, total_tiles, true)));
+        }
+        CKR(run_sh_backward(c, vd, n_views, capturing));
       }
       if (do_adam) CKR(launch_adam(c, n_cnt, capturing));
       return RMESH_OK;
@@ -696,6 +766,7 @@ int rmesh_create(const RmeshSceneDesc* d, RmeshCtx** out) {
     return RMESH_ERR_INVALID_ARG;
   if (d->n_tets > (int64_t)(1u << 29) || d->n_vertices > (int64_t)(1u << 30)) return RMESH_ERR_INVALID_ARG;
   if (d->aux_dim != 0) return RMESH_ERR_INVALID_ARG;
+  if (d->sh_coeffs && (d->sh_degree < 0 || d->sh_degree > 3)) return RMESH_ERR_INVALID_ARG;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
@@ -707,6 +778,10 @@ int rmesh_create(const RmeshSceneDesc* d, RmeshCtx** out) {
   c->width = d->width;
   c->height = d->height;
   c->tile_size = d->tile_size > 0 ? d->tile_size : 12;
+  if (d->sh_coeffs) {
+    c->sh_degree = d->sh_degree;
+    c->sh_nc = (d->sh_degree + 1) * (d->sh_degree + 1);
+  }
   if (c->tile_size != 8 && c->tile_size != 12 && c->tile_size != 16) {
     delete c;
     return RMESH_ERR_INVALID_ARG;
@@ -745,7 +820,16 @@ int rmesh_create(const RmeshSceneDesc* d, RmeshCtx** out) {
     }
     CKR(ensure_buf(c, c->rec, M * sizeof(TetRec)));
     CKR(ensure_buf(c, c->color4, M * 16));
-    CKR(ensure_buf(c, c->grad_slot, M * kGradSlot * 4));
+    CKR(ensure_buf(c, c->grad_slot, grad_floats(c) * 4));
+    if (c->sh_degree >= 0) {
+      const size_t n_sh = M * 3 * (size_t)c->sh_nc;
+      CKR(ensure_buf(c, c->sh, n_sh * 4));
+      CKR(ensure_buf(c, c->m_sh, n_sh * 4));
+      CKR(ensure_buf(c, c->v_sh, n_sh * 4));
+      CK(cudaMemsetAsync(c->m_sh.p, 0, n_sh * 4, c->stream));
+      CK(cudaMemsetAsync(c->v_sh.p, 0, n_sh * 4, c->stream));
+      CKR(copy_in(c, c->sh, d->sh_coeffs, n_sh * 4));
+    }
     CKR(ensure_buf(c, c->views_d, sizeof(ViewParams) * kMaxViews));
     CKR(ensure_buf(c, c->counters_d, sizeof(Counters) * kMaxViews));
     CKR(ensure_buf(c, c->hp_d, sizeof(AdamParams)));
@@ -832,6 +916,35 @@ int rmesh_get_params(RmeshCtx* c, float* v, float* b, float* d, float* g) {
   return RMESH_OK;
 }
 
+int rmesh_set_lr_sh(RmeshCtx* c, float lr) {
+  if (!c) return RMESH_ERR_INVALID_ARG;
+  c->lr_sh = lr;
+  return RMESH_OK;
+}
+
+int rmesh_update_sh(RmeshCtx* c, const float* sh) {
+  if (!c || !sh) return RMESH_ERR_INVALID_ARG;
+  if (c->sh_degree < 0) return fail(c, RMESH_ERR_STATE, "the context has no SH coefficients");
+  CKR(copy_in(c, c->sh, sh, (size_t)c->M * 3 * c->sh_nc * 4));
+  return RMESH_OK;
+}
+
+int rmesh_get_sh(RmeshCtx* c, float* sh) {
+  if (!c || !sh) return RMESH_ERR_INVALID_ARG;
+  if (c->sh_degree < 0) return fail(c, RMESH_ERR_STATE, "the context has no SH coefficients");
+  CK(cudaMemcpyAsync(sh, c->sh.p, (size_t)c->M * 3 * c->sh_nc * 4, cudaMemcpyDefault, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return RMESH_OK;
+}
+
+int rmesh_get_sh_grad(RmeshCtx* c, float* d_sh) {
+  if (!c || !d_sh) return RMESH_ERR_INVALID_ARG;
+  if (c->sh_degree < 0) return fail(c, RMESH_ERR_STATE, "the context has no SH coefficients");
+  CK(cudaMemcpyAsync(d_sh, sh_grad(c), (size_t)c->M * 3 * c->sh_nc * 4, cudaMemcpyDefault, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return RMESH_OK;
+}
+
 int rmesh_get_info(RmeshCtx* c, RmeshInfo* info) {
   if (!c || !info) return RMESH_ERR_INVALID_ARG;
   memset(info, 0, sizeof(*info));
@@ -852,7 +965,8 @@ int rmesh_get_info(RmeshCtx* c, RmeshInfo* info) {
                    &c->sort_state, &c->sort_status, &c->scan_status, &c->vis_key, &c->vis_val, &c->vis_tet,
                    &c->vis_cnt, &c->vis_proj, &c->vis_view, &c->vis_key_alt, &c->vis_val_alt, &c->tiles_touched, &c->pair_key,
                    &c->pair_val, &c->pair_key_alt, &c->pair_val_alt, &c->ranges, &c->rgba, &c->aux, &c->dl,
-                   &c->gt, &c->out_a, &c->out_b, &c->out_c, &c->out_d};
+                   &c->gt, &c->out_a, &c->out_b, &c->out_c, &c->out_d, &c->sh, &c->m_sh, &c->v_sh,
+                   &c->vis_color, &c->vis_dcolor, &c->vis_index};
   for (DevBuf* b : all) info->device_bytes += b->bytes;
   return RMESH_OK;
 }
@@ -903,10 +1017,11 @@ int rmesh_backward(RmeshCtx* c, const float* dl, float* d_verts, float* d_dens, 
   const uint64_t npix = (uint64_t)v.W * v.H;
   CKR(ensure_buf(c, c->dl, npix * 16));
   CK(cudaMemcpyAsync(c->dl.p, dl, npix * 16, cudaMemcpyDefault, c->stream));
-  CK(cudaMemsetAsync(c->grad_slot.p, 0, (size_t)c->M * kGradSlot * 4, c->stream));
+  CK(cudaMemsetAsync(c->grad_slot.p, 0, grad_floats(c) * 4, c->stream));
   Counters* cnt = c->counters_d.as<Counters>();
   CK(cudaMemsetAsync(&cnt->tile_ticket, 0, sizeof(uint32_t), c->stream));
   ViewParams* vd = c->views_d.as<ViewParams>();
+  CKR(clear_dcolor(c, 1));
   {
     StageScope sc(c, kStComposite, false);
     TileArgs ta = base_tile_args(c, vd, 1, c->last_tiles, cnt);
@@ -914,6 +1029,7 @@ int rmesh_backward(RmeshCtx* c, const float* dl, float* d_verts, float* d_dens, 
     ta.dl_rgba = c->dl.as<float>();
     CKR((launch_tile_m<kModeBackward, false>(c, ta, c->last_tiles, true)));
   }
+  CKR(run_sh_backward(c, vd, 1, false));
   const size_t N = (size_t)c->N, M = (size_t)c->M;
   CKR(ensure_buf(c, c->out_a, 3 * N * 4));
   CKR(ensure_buf(c, c->out_b, M * 4));
@@ -941,6 +1057,7 @@ int rmesh_train_step(RmeshCtx* c, const RmeshCamera* cam, const float* gt, float
   o.lr_dens = lr_dens;
   o.lr_grads = lr_grads;
   o.lr_base = 0.0f;
+  o.lr_sh = c->lr_sh;
   o.loss_type = loss_type;
   o.mode = RMESH_MODE_BATCHED;
   return train_views(c, cam, 1, gt, &o, loss_out);
@@ -963,7 +1080,7 @@ int rmesh_accumulate_views(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views
 int rmesh_grad_slots(RmeshCtx* c, float** ptr, uint64_t* n_floats) {
   if (!c || !ptr || !n_floats) return RMESH_ERR_INVALID_ARG;
   *ptr = c->grad_slot.as<float>();
-  *n_floats = (uint64_t)c->M * kGradSlot;
+  *n_floats = grad_floats(c);
   return RMESH_OK;
 }
 
@@ -975,7 +1092,7 @@ int rmesh_apply_adam(RmeshCtx* c, const RmeshTrainOpts* o) {
   hp.lr_dens = o->lr_dens;
   hp.lr_grads = o->lr_grads;
   hp.lr_base = o->lr_base;
-  hp.lr_sh = 0.0f;
+  hp.lr_sh = o->lr_sh;
   hp.beta1 = 0.9f;
   hp.beta2 = 0.999f;
   hp.eps = 1e-8f;

@@ -7,6 +7,8 @@
 // atomicAdd (project_compute.wgsl:181); here compaction is a single-pass
 // chained scan in (view, tet) order, so downstream order is deterministic.
 #pragma once
+#include <cuda_fp16.h>
+
 #include "common.cuh"
 
 namespace rm {
@@ -98,7 +100,7 @@ __device__ __forceinline__ void scanline_tiles(const float px[4], const float py
 //   cb      colour + dot(g, cam - v0) (the base colour at the camera, :395-396), density
 //   gm      colour gradient g; w = face flip bits (bit f) | behind (bit 4)
 //   px, py  pixel-space vertex projections (c.x/c.w+1)*W/2, (1-c.y/c.w)*H/2 (:163-166)
-//   meta    tet id
+//   meta    tet id, the entry's own index (its per-view colour-gradient slot)
 struct __align__(16) TetView {
   float4 nrm[4];
   float4 cb;
@@ -109,7 +111,7 @@ struct __align__(16) TetView {
 };
 
 __device__ __forceinline__ void write_tet_view(TetView* dst, const TetRec& r, const float4 col, const ViewParams& V,
-                                               uint32_t tet) {
+                                               uint32_t tet, uint32_t j) {
   const float4 vs[4] = {r.a, r.b, r.c, r.d};
   const float camx = V.cam[0], camy = V.cam[1], camz = V.cam[2];
   uint32_t flags = 0u;
@@ -146,8 +148,87 @@ __device__ __forceinline__ void write_tet_view(TetView* dst, const TetRec& r, co
   out.gm = make_float4(gx, gy, gz, __uint_as_float(flags));
   out.px = make_float4(qx[0], qx[1], qx[2], qx[3]);
   out.py = make_float4(qy[0], qy[1], qy[2], qy[3]);
-  out.meta = make_uint4(tet, 0u, 0u, 0u);
+  out.meta = make_uint4(tet, j, 0u, 0u);
   *dst = out;
+}
+
+// ---- SH colour (project_compute.wgsl:264-318) -------------------------------
+constexpr float kC0 = 0.28209479177387814f, kC1 = 0.4886025119029199f;
+constexpr float kC2_0 = 1.0925484305920792f, kC2_1 = -1.0925484305920792f, kC2_2 = 0.31539156525252005f,
+                kC2_3 = -1.0925484305920792f, kC2_4 = 0.5462742152960396f;
+constexpr float kC3_0 = -0.5900435899266435f, kC3_1 = 2.890611442640554f, kC3_2 = -0.4570457994644658f,
+                kC3_3 = 0.3731763325901154f, kC3_4 = -0.4570457994644658f, kC3_5 = 1.445305721320277f,
+                kC3_6 = -0.5900435899266435f;
+
+// Coefficients are stored as fp32 training values; the shader reads them as
+// f16 (crates/rmesh-viewer/src/gpu_state.rs:60-88, round to nearest even).
+__device__ __forceinline__ float sh_f16(float x) { return __half2float(__float2half_rn(x)); }
+
+// softplus with beta 10 (project_compute.wgsl:66-69)
+__device__ __forceinline__ float softplus10(float x) {
+  return fm(x, 10.0f) > 20.0f ? x : fm(0.1f, logf(fa(1.0f, expf(fm(10.0f, x)))));
+}
+
+// Centroid and unit direction camera -> centroid (project_compute.wgsl:268-273).
+__device__ __forceinline__ float sh_direction(const TetRec& r, const float* cam, float3& centroid, float3& dir) {
+  centroid = make_float3(fm(fa(fa(fa(r.a.x, r.b.x), r.c.x), r.d.x), 0.25f),
+                         fm(fa(fa(fa(r.a.y, r.b.y), r.c.y), r.d.y), 0.25f),
+                         fm(fa(fa(fa(r.a.z, r.b.z), r.c.z), r.d.z), 0.25f));
+  const float rx = fs(centroid.x, cam[0]), ry = fs(centroid.y, cam[1]), rz = fs(centroid.z, cam[2]);
+  const float len = __fsqrt_rn(dot3x(rx, ry, rz, rx, ry, rz));
+  dir = len > 0.0f ? make_float3(fdv(rx, len), fdv(ry, len), fdv(rz, len)) : make_float3(0.f, 0.f, 0.f);
+  return len;
+}
+
+// Colour of tet (record r, coefficients q = [3][nc] fp32) seen from cam:
+// softplus(SH(dir) + 0.5 + dot(g, v0 - centroid)), evaluated term by term in
+// the shader's order with explicitly rounded arithmetic.
+template <int DEG>
+__device__ __forceinline__ float4 sh_color(const TetRec& r, const float* __restrict__ q, const float* cam) {
+  constexpr int NC = (DEG + 1) * (DEG + 1);
+  float3 cen, dir;
+  sh_direction(r, cam, cen, dir);
+  const float x = dir.x, y = dir.y, z = dir.z;
+  const float xx = fm(x, x), yy = fm(y, y), zz = fm(z, z);
+  float rgb[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const float* qc = q + c * NC;
+    float val = fm(kC0, sh_f16(qc[0]));
+    if (DEG >= 1) {
+      val = fs(val, fm(fm(kC1, y), sh_f16(qc[1])));
+      val = fa(val, fm(fm(kC1, z), sh_f16(qc[2])));
+      val = fs(val, fm(fm(kC1, x), sh_f16(qc[3])));
+    }
+    if (DEG >= 2) {
+      val = fa(val, fm(fm(kC2_0, fm(x, y)), sh_f16(qc[4])));
+      val = fa(val, fm(fm(kC2_1, fm(y, z)), sh_f16(qc[5])));
+      val = fa(val, fm(fm(kC2_2, fs(fs(fm(2.0f, zz), xx), yy)), sh_f16(qc[6])));
+      val = fa(val, fm(fm(kC2_3, fm(x, z)), sh_f16(qc[7])));
+      val = fa(val, fm(fm(kC2_4, fs(xx, yy)), sh_f16(qc[8])));
+    }
+    if (DEG >= 3) {
+      val = fa(val, fm(fm(fm(kC3_0, y), fs(fm(3.0f, xx), yy)), sh_f16(qc[9])));
+      val = fa(val, fm(fm(fm(fm(kC3_1, x), y), z), sh_f16(qc[10])));
+      val = fa(val, fm(fm(fm(kC3_2, y), fs(fs(fm(4.0f, zz), xx), yy)), sh_f16(qc[11])));
+      val = fa(val, fm(fm(fm(kC3_3, z), fs(fs(fm(2.0f, zz), fm(3.0f, xx)), fm(3.0f, yy))), sh_f16(qc[12])));
+      val = fa(val, fm(fm(fm(kC3_4, x), fs(fs(fm(4.0f, zz), xx), yy)), sh_f16(qc[13])));
+      val = fa(val, fm(fm(fm(kC3_5, z), fs(xx, yy)), sh_f16(qc[14])));
+      val = fa(val, fm(fm(fm(kC3_6, x), fs(xx, fm(3.0f, yy))), sh_f16(qc[15])));
+    }
+    rgb[c] = fa(val, 0.5f);
+  }
+  const float off = dot3x(r.b.w, r.c.w, r.d.w, fs(r.a.x, cen.x), fs(r.a.y, cen.y), fs(r.a.z, cen.z));
+  return make_float4(softplus10(fa(rgb[0], off)), softplus10(fa(rgb[1], off)), softplus10(fa(rgb[2], off)), 0.0f);
+}
+
+__device__ __forceinline__ float4 sh_color_deg(int deg, const TetRec& r, const float* q, const float* cam) {
+  switch (deg) {
+    case 0: return sh_color<0>(r, q, cam);
+    case 1: return sh_color<1>(r, q, cam);
+    case 2: return sh_color<2>(r, q, cam);
+    default: return sh_color<3>(r, q, cam);
+  }
 }
 
 struct ProjectArgs {
@@ -165,6 +246,13 @@ struct ProjectArgs {
   TetView* vis_view;            // per entry: the tile kernel's per-(view, tet) record
   const float4* color4;         // tet colours, [view * color_view_stride + tet]
   uint32_t color_view_stride;
+  // SH colours (sh != nullptr): coefficients [M][3][nc]; the colour of each
+  // tile-touching entry goes to vis_color[j], and vis_index maps every item
+  // (view * M + tet) to its entry j (0xFFFFFFFF when it touches no tile)
+  const float* sh;
+  int sh_degree;
+  float4* vis_color;
+  uint32_t* vis_index;
   uint32_t* tiles_touched;      // optional [n_views*M], indexed by (view, tet id)
   unsigned long long* status;   // chained-scan status, one word per block (zeroed)
   uint32_t* ticket;             // block ticket (zeroed)
@@ -239,6 +327,7 @@ __global__ void __launch_bounds__(256) project_kernel(ProjectArgs a) {
     }
     if (a.tiles_touched) a.tiles_touched[i] = (visible ? count : 0u);
     flag = visible && count > 0u;
+    if (a.vis_index && !flag) a.vis_index[i] = kSentinel;
     if (flag) {
       // depth key (tile_gen_scan_compute.wgsl:136-143)
       const float4 C = a.circ[tet];
@@ -280,9 +369,19 @@ __global__ void __launch_bounds__(256) project_kernel(ProjectArgs a) {
     a.vis_cnt[j] = count;
     a.vis_proj[2 * j] = make_float4(qx[0], qy[0], qx[1], qy[1]);
     a.vis_proj[2 * j + 1] = make_float4(qx[2], qy[2], qx[3], qy[3]);
-    if (a.vis_view)
-      write_tet_view(a.vis_view + j, a.rec[tet], a.color4[(size_t)a.color_view_stride * view + tet], a.views[view],
-                   tet);
+    if (a.vis_view) {
+      const TetRec r = a.rec[tet];
+      float4 col;
+      if (a.sh) {
+        const int nc = (a.sh_degree + 1) * (a.sh_degree + 1);
+        col = sh_color_deg(a.sh_degree, r, a.sh + (size_t)tet * 3 * nc, a.views[view].cam);
+        a.vis_color[j] = col;
+        a.vis_index[i] = (uint32_t)j;
+      } else {
+        col = a.color4[(size_t)a.color_view_stride * view + tet];
+      }
+      write_tet_view(a.vis_view + j, r, col, a.views[view], tet, (uint32_t)j);
+    }
   }
   // the block holding the last item publishes the visible count
   if (threadIdx.x == 0 && (unsigned long long)(blk + 1) * 256ull >= total_items &&

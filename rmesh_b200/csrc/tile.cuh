@@ -68,7 +68,11 @@ struct TileArgs {
   const float* dl_rgba;        // [pixels][4] (backward mode)
   const float* gt_rgb;         // [pixels][3] (train mode)
   float* grad_slot;            // [M][kGradSlot]
-  float* dcolor_slot;          // optional [views*M][4] per-view colour gradient (SH mode)
+  // SH colours: per-entry colours (the min_t path reads them) and per-entry
+  // colour gradients, which then go through the SH adjoint instead of the
+  // base-colour slot
+  const float4* vis_color;
+  float4* vis_dcolor;
   Counters* counters;
   const AdamParams* hp;
   int persistent;
@@ -417,7 +421,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
           nump = numo;
           const float4 gg = tv.gm;
           const float bo = dot3x(gg.x, gg.y, gg.z, fs(oxp, rr.a.x), fs(oyp, rr.a.y), fs(ozp, rr.a.z));
-          const float4 cc = a.color4[(size_t)a.color_view_stride * view + tet];
+          const float4 cc = a.vis_color ? a.vis_color[tv.meta.y] : a.color4[(size_t)a.color_view_stride * view + tet];
           bcr_o = fa(cc.x, bo); bcg_o = fa(cc.y, bo); bcb_o = fa(cc.z, bo);
         }
         float t_min, t_max;
@@ -799,6 +803,11 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
 #pragma unroll
               for (int q = 0; q < 12; ++q) out[7 + q] = clipf(dv[q], kMinVal, kMaxVal);
               out[19] = 0.0f;
+              if (a.vis_dcolor) {  // SH colours: this view's colour gradient of the entry
+                const float4 dc = make_float4(out[1], out[2], out[3], 0.0f);
+                if (dc.x != 0.f || dc.y != 0.f || dc.z != 0.f) atomicAdd(a.vis_dcolor + tv.meta.y, dc);
+                out[1] = out[2] = out[3] = 0.0f;
+              }
               float4* dst = reinterpret_cast<float4*>(a.grad_slot + (size_t)tv.meta.x * kGradSlot);
 #pragma unroll
               for (int c = 0; c < 5; ++c) {

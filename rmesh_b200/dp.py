@@ -43,10 +43,10 @@ class DataParallelStep:
         self._slots = None
 
     def __call__(self, cameras: Sequence, gt_images, lr_verts: float, lr_dens: float, lr_grads: float,
-                 loss_type: int = 1, lr_base: float = 0.0, mode: str = "graph"):
+                 loss_type: int = 1, lr_base: float = 0.0, mode: str = "graph", lr_sh: float = 0.0):
         losses = self.r.accumulate_views(cameras, gt_images, loss_type=loss_type, mode=mode)
         if self._slots is None:
             self._slots = self.r.grad_slots()
         allreduce_sum_(self._slots, self.group, self.stream)
-        self.r.apply_adam(lr_verts, lr_dens, lr_grads, lr_base, loss_type)
+        self.r.apply_adam(lr_verts, lr_dens, lr_grads, lr_base, loss_type, lr_sh)
         return losses

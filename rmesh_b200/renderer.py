@@ -94,7 +94,12 @@ class RMeshRenderer:
     """Tiled differentiable tet-mesh volume renderer on one CUDA device."""
 
     def __init__(self, vertices, indices, base_colors, densities, color_grads, circumdata, width: int,
-                 height: int, aux_dim: int = 0, *, tile_size: int = 12, device: int | None = None):
+                 height: int, aux_dim: int = 0, *, tile_size: int = 12, device: int | None = None,
+                 sh_coeffs=None, sh_degree: int | None = None):
+        """Arguments as the reference's constructor (crates/rmesh-python/src/lib.rs:265-277).
+        ``sh_coeffs`` ([M, 3, (sh_degree+1)^2] floats, no reference counterpart in
+        the binding) switches the colours from ``base_colors`` to the reference
+        shader's view-dependent SH colour (project_compute.wgsl:264-318)."""
         self._lib = _lib.load()
         if int(aux_dim) != 0:
             raise ValueError("aux_dim > 0 is not supported by this build")
@@ -114,8 +119,24 @@ class RMeshRenderer:
         for name, per in (("base_colors", 3), ("densities", 1), ("color_grads", 3), ("circumdata", 4)):
             if _numel(ptrs[name][0]) != per * self._M:
                 raise ValueError(f"{name} must hold {per}*M = {per * self._M} values")
+        self._sh_degree = -1
+        self._nc = 0
+        if sh_coeffs is not None:
+            obj, p_sh = _as_array(sh_coeffs, np.float32, "sh_coeffs")
+            n_sh = _numel(obj)
+            if sh_degree is None:
+                nc = n_sh // (3 * self._M)
+                sh_degree = int(round(nc ** 0.5)) - 1
+            if not 0 <= int(sh_degree) <= 3:
+                raise ValueError("sh_degree must be 0..3")
+            self._sh_degree, self._nc = int(sh_degree), (int(sh_degree) + 1) ** 2
+            if n_sh != 3 * self._nc * self._M:
+                raise ValueError(f"sh_coeffs must hold 3*(sh_degree+1)^2*M = {3 * self._nc * self._M} values")
+            keep.append(obj)
         d = _lib.SceneDesc()
         d.n_vertices, d.n_tets = self._N, self._M
+        if self._sh_degree >= 0:
+            d.sh_coeffs, d.sh_degree = p_sh, self._sh_degree
         d.vertices, d.indices = ptrs["vertices"][1], ptrs["indices"][1]
         d.base_colors, d.densities = ptrs["base_colors"][1], ptrs["densities"][1]
         d.color_grads, d.circumdata = ptrs["color_grads"][1], ptrs["circumdata"][1]
@@ -171,6 +192,11 @@ class RMeshRenderer:
     def n_tets(self) -> int:
         return self._M
 
+    @property
+    def sh_degree(self) -> int:
+        """-1 when colours are base_colors, else the SH degree."""
+        return self._sh_degree
+
     def info(self) -> _lib.Info:
         inf = _lib.Info()
         self._check(self._lib.rmesh_get_info(self._ctx, ctypes.byref(inf)))
@@ -188,8 +214,16 @@ class RMeshRenderer:
         self._check(self._lib.rmesh_set_stream(self._ctx, ctypes.c_void_p(int(stream_handle))))
 
     # ------------------------------------------------------------- parameters
-    def update_params(self, vertices, base_colors, densities, color_grads):
+    def update_params(self, vertices, base_colors, densities, color_grads, sh_coeffs=None):
         keep = []
+        if sh_coeffs is not None:
+            if self._sh_degree < 0:
+                raise ValueError("this renderer has no SH coefficients")
+            obj, p = _as_array(sh_coeffs, np.float32, "sh_coeffs")
+            if _numel(obj) != 3 * self._nc * self._M:
+                raise ValueError("sh_coeffs has the wrong size")
+            keep.append(obj)
+            self._check(self._lib.rmesh_update_sh(self._ctx, p))
         ps = []
         for name, arr, n in (("vertices", vertices, 3 * self._N), ("base_colors", base_colors, 3 * self._M),
                              ("densities", densities, self._M), ("color_grads", color_grads, 3 * self._M)):
@@ -209,6 +243,15 @@ class RMeshRenderer:
         self._check(self._lib.rmesh_get_params(self._ctx, out["vertices"].ctypes.data,
                                                out["base_colors"].ctypes.data, out["densities"].ctypes.data,
                                                out["color_grads"].ctypes.data))
+        if self._sh_degree >= 0:
+            out["sh_coeffs"] = np.empty(3 * self._nc * self._M, np.float32)
+            self._check(self._lib.rmesh_get_sh(self._ctx, out["sh_coeffs"].ctypes.data))
+        return out
+
+    def sh_grad_into(self, out):
+        """Coefficient gradient of the last backward / training call into ``out``."""
+        _, p = _as_array(out, np.float32, "out")
+        self._check(self._lib.rmesh_get_sh_grad(self._ctx, p))
         return out
 
     # -------------------------------------------------------------- the path
@@ -230,7 +273,8 @@ class RMeshRenderer:
         return out
 
     def backward(self, dl_d_image) -> dict:
-        """dict of 1-D float32 arrays d_vertices, d_densities, d_base_colors, d_color_grads."""
+        """dict of 1-D float32 arrays d_vertices, d_densities, d_base_colors, d_color_grads
+        (and d_sh_coeffs when the colours come from SH coefficients)."""
         obj, p = _as_array(dl_d_image, np.float32, "dl_d_image")
         if _numel(obj) != 4 * self._width * self._height:
             raise ValueError("dl_d_image must be [H, W, 4]")
@@ -240,6 +284,8 @@ class RMeshRenderer:
         self._check(self._lib.rmesh_backward(self._ctx, p, out["d_vertices"].ctypes.data,
                                              out["d_densities"].ctypes.data, out["d_base_colors"].ctypes.data,
                                              out["d_color_grads"].ctypes.data))
+        if self._sh_degree >= 0:
+            out["d_sh_coeffs"] = self.sh_grad_into(np.empty(3 * self._nc * self._M, np.float32))
         return out
 
     def backward_into(self, dl_d_image, d_vertices, d_densities, d_base_colors, d_color_grads):
@@ -250,8 +296,9 @@ class RMeshRenderer:
         self._check(self._lib.rmesh_backward(self._ctx, p, *ptrs))
 
     def train_step(self, cam_pos, vp, c2w_intrinsics, gt_image, lr_verts: float, lr_dens: float,
-                   lr_grads: float, loss_type: int) -> float:
+                   lr_grads: float, loss_type: int, lr_sh: float = 0.0) -> float:
         cam = self._cam(cam_pos, vp, c2w_intrinsics)
+        self._check(self._lib.rmesh_set_lr_sh(self._ctx, float(lr_sh)))
         obj, p = _as_array(gt_image, np.float32, "gt_image")
         if _numel(obj) != 3 * self._width * self._height:
             raise ValueError("gt_image must be [H, W, 3]")
@@ -260,7 +307,7 @@ class RMeshRenderer:
                                                float(lr_grads), int(loss_type), ctypes.byref(loss)))
         return float(loss.value)
 
-    def _views_args(self, cameras, gt_images, lr_verts, lr_dens, lr_grads, loss_type, lr_base, mode):
+    def _views_args(self, cameras, gt_images, lr_verts, lr_dens, lr_grads, loss_type, lr_base, mode, lr_sh=0.0):
         n = len(cameras)
         cams = (_lib.Camera * n)()
         total = 0
@@ -277,17 +324,19 @@ class RMeshRenderer:
         o = _lib.TrainOpts()
         o.lr_verts, o.lr_dens, o.lr_grads, o.lr_base = float(lr_verts), float(lr_dens), float(lr_grads), float(lr_base)
         o.loss_type = int(loss_type)
+        o.lr_sh = float(lr_sh)
         o.mode = {"plain": _lib.MODE_PLAIN, "batched": _lib.MODE_BATCHED, "graph": _lib.MODE_GRAPH}[mode]
         return n, cams, obj, p, o
 
     def train_step_views(self, cameras: Sequence, gt_images, lr_verts: float, lr_dens: float, lr_grads: float,
-                         loss_type: int = 1, lr_base: float = 0.0, mode: str = "graph") -> np.ndarray:
+                         loss_type: int = 1, lr_base: float = 0.0, mode: str = "graph",
+                         lr_sh: float = 0.0) -> np.ndarray:
         """One step over several cameras (``rmesh_b200.camera.Camera`` objects) with
         one Adam update.  ``gt_images``: list of [H,W,3] arrays or one flat
         array/tensor holding them back to back.  ``mode``: plain | batched | graph.
         Returns the per-view losses."""
         n, cams, keep, p, o = self._views_args(cameras, gt_images, lr_verts, lr_dens, lr_grads, loss_type,
-                                               lr_base, mode)
+                                               lr_base, mode, lr_sh)
         losses = np.zeros(n, np.float32)
         self._check(self._lib.rmesh_train_step_views(self._ctx, cams, n, p, ctypes.byref(o), losses.ctypes.data))
         return losses
@@ -301,8 +350,9 @@ class RMeshRenderer:
         return losses
 
     def grad_slots(self):
-        """The device gradient slots as a torch CUDA tensor view [M, 20]
-        (density, base rgb, colour-gradient xyz, 4 x vertex xyz, pad)."""
+        """The device gradient buffer as a flat torch CUDA tensor view: [M, 20]
+        slots (density, base rgb, colour-gradient xyz, 4 x vertex xyz, pad), then,
+        with SH colours, the [M, 3, nc] coefficient gradients."""
         import torch
 
         ptr = ctypes.c_void_p()
@@ -313,13 +363,14 @@ class RMeshRenderer:
             __cuda_array_interface__ = {"shape": (int(n.value),), "typestr": "<f4", "data": (ptr.value, False),
                                         "version": 3, "strides": None}
 
-        return torch.as_tensor(_View(), device="cuda").view(-1, 20)
+        return torch.as_tensor(_View(), device="cuda")
 
     def apply_adam(self, lr_verts: float, lr_dens: float, lr_grads: float, lr_base: float = 0.0,
-                   loss_type: int = 1):
+                   loss_type: int = 1, lr_sh: float = 0.0):
         o = _lib.TrainOpts()
         o.lr_verts, o.lr_dens, o.lr_grads, o.lr_base = float(lr_verts), float(lr_dens), float(lr_grads), float(lr_base)
         o.loss_type = int(loss_type)
+        o.lr_sh = float(lr_sh)
         self._check(self._lib.rmesh_apply_adam(self._ctx, ctypes.byref(o)))
 
     # ---------------------------------------------------------- inspection

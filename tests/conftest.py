@@ -56,6 +56,14 @@ def c1_scene():
 
 
 @pytest.fixture(scope="session")
+def c2_scene():
+    """10,000-point 8-component GMM Delaunay mesh with degree-3 SH colours."""
+    from rmesh_b200.scenes import scene_for_config
+
+    return scene_for_config("c2")
+
+
+@pytest.fixture(scope="session")
 def oracle32():
     from oracle import Oracle
 
@@ -75,8 +83,10 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
 
 
-def make_renderer(scene, cam, tile_size=12):
+def make_renderer(scene, cam, tile_size=12, sh=False):
+    """Renderer over a scene dict; sh=True colours it by its SH coefficients."""
     from rmesh_b200 import RMeshRenderer
 
+    kw = dict(sh_coeffs=scene["sh_coeffs"], sh_degree=scene["sh_degree"]) if sh else {}
     return RMeshRenderer(scene["vertices"], scene["indices"], scene["base_colors"], scene["densities"],
-                         scene["color_grads"], scene["circumdata"], cam.width, cam.height, tile_size=tile_size)
+                         scene["color_grads"], scene["circumdata"], cam.width, cam.height, tile_size=tile_size, **kw)

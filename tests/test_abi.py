@@ -37,7 +37,7 @@ def test_library_exports_every_declared_symbol():
 def test_abi_version():
     from rmesh_b200 import _lib
 
-    assert _lib.load().rmesh_abi_version() == 1
+    assert _lib.load().rmesh_abi_version() == 2
 
 
 def test_struct_layouts_match_header(tmp_path):

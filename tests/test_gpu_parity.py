@@ -157,7 +157,7 @@ def test_split_step_equals_train_step(c1_scene):
     la = a.train_step_views(cams, gts, 1e-4, 1e-2, 1e-3, 1, mode="batched")
     lb = b.accumulate_views(cams, gts, 1, mode="batched")
     slots = b.grad_slots()
-    assert slots.shape == (b.n_tets, 20) and float(slots.abs().sum()) > 0
+    assert slots.shape == (b.n_tets * 20,) and float(slots.abs().sum()) > 0
     b.apply_adam(1e-4, 1e-2, 1e-3)
     np.testing.assert_allclose(la, lb, rtol=1e-6)
     pa, pb = a.get_params(), b.get_params()
