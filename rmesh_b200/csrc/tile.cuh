@@ -100,7 +100,7 @@ struct __align__(16) TileSmem {
   uint32_t pmask[TS * TS];
   short2 span[kBatch][TS];
   uint16_t rowpref[kBatch][TS + 1];
-  uint8_t ipix[kBatch * TS * TS];  // pixel of each item of the batch (tet-major)
+  uint16_t ipix[kBatch * TS * TS];  // (tet slot << 8) | pixel of each item of the batch (tet-major)
   uint64_t bar[2];
   float lsum[16];
   uint32_t tile;
@@ -260,17 +260,21 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
 
     // ---------------- batch machinery ----------------
     // dir = -1: front-to-back from `first` downwards (forward); +1: upwards (adjoint)
-    auto issue = [&](int buf, uint32_t first, int nb, int dir) {
+    // Warp 0 lane l loads the record index of the batch's l-th pair one batch
+    // ahead of the copy that uses it, so the load's latency overlaps a batch.
+    auto load_idx = [&](uint32_t first, int nb, int dir) -> uint32_t {
+      if (warp != 0 || lane >= nb) return 0u;
+      return a.pair_val[dir < 0 ? first - (uint32_t)lane : first + (uint32_t)lane];
+    };
+    auto issue = [&](int buf, int nb, uint32_t idx) {
       if (warp == 0) {
         if (lane == 0) {
           fence_proxy_async_smem();
           mbar_arrive_expect_tx(&s.bar[buf], (uint32_t)nb * (uint32_t)sizeof(TetView));
         }
         __syncwarp();
-        if (lane < nb) {
-          const uint32_t pos = dir < 0 ? first - (uint32_t)lane : first + (uint32_t)lane;
-          bulk_copy_g2s(&s.view[buf][lane], a.vis_view + a.pair_val[pos], (uint32_t)sizeof(TetView), &s.bar[buf]);
-        }
+        if (lane < nb)
+          bulk_copy_g2s(&s.view[buf][lane], a.vis_view + idx, (uint32_t)sizeof(TetView), &s.bar[buf]);
       }
     };
     // every thread waits on the phase; the outcome is made block-uniform
@@ -303,6 +307,15 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
           const float vpy[4] = {gy4.x - tile_oy, gy4.y - tile_oy, gy4.z - tile_oy, gy4.w - tile_oy};
           float xl = 1e10f, xr = -1e10f;
           const float yc = fa((float)row, 0.5f);
+          // rows the tet cannot reach: no edge crosses yc (and, for the forward,
+          // no vertex lies in [yc - 0.5, yc + 0.5)), so the span stays empty
+          const float ylo = fminf(fminf(vpy[0], vpy[1]), fminf(vpy[2], vpy[3]));
+          const float yhi = fmaxf(fmaxf(vpy[0], vpy[1]), fmaxf(vpy[2], vpy[3]));
+          const bool reach = vertex_rows ? (yhi >= fs(yc, 0.5f) && ylo < fa(yc, 0.5f)) : (ylo <= yc && yhi > yc);
+          if (!reach) {
+            s.span[k][row] = sp;
+            continue;
+          }
           const int ei[6] = {0, 0, 0, 1, 1, 2};
           const int ej[6] = {1, 2, 3, 2, 3, 3};
 #pragma unroll
@@ -368,20 +381,16 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
         if (sp.x > sp.y) continue;
         const uint32_t base = s.toff[k] + s.rowpref[k][row];
         for (int c = sp.x; c <= sp.y; ++c) {
-          s.ipix[base + (uint32_t)(c - sp.x)] = (uint8_t)(row * TS + c);
+          s.ipix[base + (uint32_t)(c - sp.x)] = (uint16_t)((k << 8) | (row * TS + c));
           atomicOr(&s.pmask[row * TS + c], 1u << k);
         }
       }
     };
     // tet-major item gi -> (tet k, pixel index in tile)
-    auto decode = [&](uint32_t gi, int k0, int k1, int& k, int& p) {
-      int lo = k0, hi = k1 - 1;  // largest k with toff[k] <= gi
-      while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (s.toff[mid] <= gi) lo = mid; else hi = mid - 1;
-      }
-      k = lo;
-      p = s.ipix[gi];
+    auto decode = [&](uint32_t gi, int& k, int& p) {
+      const uint32_t e = s.ipix[gi];
+      k = (int)(e >> 8);
+      p = (int)(e & 255u);
     };
     // item index of (tet k, this thread's pixel) inside the current sub-batch
     auto item_of = [&](int k, uint32_t base) -> uint32_t {
@@ -400,7 +409,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
       const uint32_t n_items = s.toff[k1] - base;
       for (uint32_t i = tid; i < n_items; i += NT) {
         int k, p;
-        decode(base + i, k0, k1, k, p);
+        decode(base + i, k, p);
         const float4 d = s.pdir[p];
         float numo[4];
         const float* nump = nullptr;
@@ -454,7 +463,15 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
     if (MODE == kModeForward || MODE == kModeTrain) {
       bool alive = valid;
       if (re > rs) {
-        issue(0, re - 1u, (int)min((uint32_t)kBatch, re - rs), -1);
+        {
+          const int nb0 = (int)min((uint32_t)kBatch, re - rs);
+          issue(0, nb0, load_idx(re - 1u, nb0, -1));
+        }
+        uint32_t idx_next = 0u;  // record indices of the batch after the current one
+        if (re - rs > (uint32_t)kBatch) {
+          const uint32_t h1 = re - (uint32_t)kBatch;
+          idx_next = load_idx(h1 - 1u, (int)min((uint32_t)kBatch, h1 - rs), -1);
+        }
         int b = 0;
         for (uint32_t hi = re; hi > rs;) {
           const int buf = b & 1;
@@ -462,7 +479,12 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
           const uint32_t next_hi = hi - (uint32_t)nb;
           wait_buf(buf);
           if (failed) break;
-          if (next_hi > rs) issue(buf ^ 1, next_hi - 1u, (int)min((uint32_t)kBatch, next_hi - rs), -1);
+          if (next_hi > rs) {
+            const int nbn = (int)min((uint32_t)kBatch, next_hi - rs);
+            issue(buf ^ 1, nbn, idx_next);
+            const uint32_t h2 = next_hi - (uint32_t)nbn;
+            if (h2 > rs) idx_next = load_idx(h2 - 1u, (int)min((uint32_t)kBatch, h2 - rs), -1);
+          }
           spans(buf, nb, true);
           __syncthreads();
           prefixes(nb);
@@ -583,7 +605,15 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
       if (in_tile) s.pdl[pl] = make_float4(dlr, dlg, dlb, 0.0f);
       if (re > rs) {
         __syncthreads();
-        issue(0, rs, (int)min((uint32_t)kBatch, re - rs), +1);
+        {
+          const int nb0 = (int)min((uint32_t)kBatch, re - rs);
+          issue(0, nb0, load_idx(rs, nb0, +1));
+        }
+        uint32_t idx_next = 0u;
+        if (re - rs > (uint32_t)kBatch) {
+          const uint32_t l1 = rs + (uint32_t)kBatch;
+          idx_next = load_idx(l1, (int)min((uint32_t)kBatch, re - l1), +1);
+        }
         int b = 0;
         for (uint32_t lo = rs; lo < re;) {
           const int buf = b & 1;
@@ -591,7 +621,12 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
           const uint32_t next_lo = lo + (uint32_t)nb;
           wait_buf(buf);
           if (failed) break;
-          if (next_lo < re) issue(buf ^ 1, next_lo, (int)min((uint32_t)kBatch, re - next_lo), +1);
+          if (next_lo < re) {
+            const int nbn = (int)min((uint32_t)kBatch, re - next_lo);
+            issue(buf ^ 1, nbn, idx_next);
+            const uint32_t l2 = next_lo + (uint32_t)nbn;
+            if (l2 < re) idx_next = load_idx(l2, (int)min((uint32_t)kBatch, re - l2), +1);
+          }
           spans(buf, nb, false);  // adjoint: edge crossings only
           __syncthreads();
           prefixes(nb);
@@ -737,17 +772,14 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
                 __syncwarp();
                 if (wq < kMomHalf && wr0 < wr1) {
                   const int col = hm * kMomHalf + wq;
-                  float sum = 0.0f;
-                  int cur = __float_as_int(red[wr0][kMomHalf]);
-                  for (int row = wr0; row < wr1; ++row) {
-                    if (row > wr0 && ((heads >> row) & 1u)) {
-                      if (sum != 0.0f) atomicAdd(&s.mom[cur][col], sum);
-                      sum = 0.0f;
-                      cur = __float_as_int(red[row][kMomHalf]);
-                    }
-                    sum += red[row][wq];
+                  for (int r0 = wr0; r0 < wr1;) {  // one tet segment [r0, r1) at a time
+                    const unsigned later = heads & ~((2u << r0) - 1u);
+                    const int r1 = later ? min(__ffs(later) - 1, wr1) : wr1;
+                    float sum = 0.0f;
+                    for (int row = r0; row < r1; ++row) sum += red[row][wq];
+                    if (sum != 0.0f) atomicAdd(&s.mom[__float_as_int(red[r0][kMomHalf])][col], sum);
+                    r0 = r1;
                   }
-                  if (sum != 0.0f) atomicAdd(&s.mom[cur][col], sum);
                 }
                 __syncwarp();
               }
@@ -755,33 +787,42 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
             __syncthreads();
             k0 = k1;
           }
-          // flush: rebuild each tet's 19 gradients from its moments and add them to
-          // the global slot (five 16-byte vector atomics per tet)
-          if (tid < nb) {
-            const int k = tid;
-            float* mm = s.mom[k];
-            bool any = false;
+          // flush: rebuild each tet's 19 gradients from its moments, four threads
+          // per tet (thread f takes face f's vertex terms, thread 0 also the
+          // density / colour terms), summed by shuffles; thread 0 adds them to the
+          // global slot with five 16-byte vector atomics
+          for (int t0 = 0; t0 < 4 * kBatch; t0 += NT) {  // block-uniform trip count
+            const int task = t0 + tid;
+            const int k = task >> 2, f = task & 3;
+            const bool live = k < nb;
+            float* mm = s.mom[live ? k : 0];
+            const float S = live ? mm[8 + 4 * f] : 0.f, Px = live ? mm[9 + 4 * f] : 0.f;
+            const float Py = live ? mm[10 + 4 * f] : 0.f, Pz = live ? mm[11 + 4 * f] : 0.f;
+            const bool face_any = S != 0.0f || Px != 0.0f || Py != 0.0f || Pz != 0.0f;
+            bool any = face_any;
+            if (live && f == 0) {
 #pragma unroll
-            for (int q = 0; q < kMom; ++q) any = any || (mm[q] != 0.0f);
-            if (any) {
-              const TetView& tv = s.view[buf][k];
+              for (int q = 0; q < 8; ++q) any = any || (mm[q] != 0.0f);
+            }
+            const unsigned grp = (__ballot_sync(0xffffffffu, any) >> (lane & ~3)) & 0xFu;
+            float dv[12];
+#pragma unroll
+            for (int q = 0; q < 12; ++q) dv[q] = 0.0f;
+            float out[7];
+            const TetView& tv = s.view[buf][live ? k : 0];
+            if (live && grp) {
               const TetRec r = a.rec[tv.meta.x];
-              const float4 gg = tv.gm;
-              float out[20];
-              out[0] = mm[0];
-              out[1] = mm[1]; out[2] = mm[2]; out[3] = mm[3];
-              const float sb = mm[4];
-              out[4] = clipf((camx - r.a.x) * sb + mm[5], kMinVal, kMaxVal);
-              out[5] = clipf((camy - r.a.y) * sb + mm[6], kMinVal, kMaxVal);
-              out[6] = clipf((camz - r.a.z) * sb + mm[7], kMinVal, kMaxVal);
-              float dv[12];
-              dv[0] = -gg.x * sb; dv[1] = -gg.y * sb; dv[2] = -gg.z * sb;
-#pragma unroll
-              for (int q = 3; q < 12; ++q) dv[q] = 0.0f;
-#pragma unroll
-              for (int f = 0; f < 4; ++f) {
-                const float S = mm[8 + 4 * f], Px = mm[9 + 4 * f], Py = mm[10 + 4 * f], Pz = mm[11 + 4 * f];
-                if (S == 0.0f && Px == 0.0f && Py == 0.0f && Pz == 0.0f) continue;
+              if (f == 0) {
+                const float4 gg = tv.gm;
+                out[0] = mm[0];
+                out[1] = mm[1]; out[2] = mm[2]; out[3] = mm[3];
+                const float sb = mm[4];
+                out[4] = clipf((camx - r.a.x) * sb + mm[5], kMinVal, kMaxVal);
+                out[5] = clipf((camy - r.a.y) * sb + mm[6], kMinVal, kMaxVal);
+                out[6] = clipf((camz - r.a.z) * sb + mm[7], kMinVal, kMaxVal);
+                dv[0] = -gg.x * sb; dv[1] = -gg.y * sb; dv[2] = -gg.z * sb;
+              }
+              if (face_any) {
                 const int ia = kFaces[f][0], ib = kFaces[f][1], ic = kFaces[f][2];
                 const float4 va = rec_vertex(r, ia), vb = rec_vertex(r, ib), vc = rec_vertex(r, ic);
                 const float4 nf = tv.nrm[f];
@@ -800,22 +841,37 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
                   if (q == ic) { dv[3 * q] += cx; dv[3 * q + 1] += cy; dv[3 * q + 2] += cz; }
                 }
               }
+            }
 #pragma unroll
-              for (int q = 0; q < 12; ++q) out[7 + q] = clipf(dv[q], kMinVal, kMaxVal);
-              out[19] = 0.0f;
+            for (int q = 0; q < 12; ++q) {
+              dv[q] += __shfl_xor_sync(0xffffffffu, dv[q], 1);
+              dv[q] += __shfl_xor_sync(0xffffffffu, dv[q], 2);
+            }
+            if (live && grp && f == 0) {
+              float4* dst = reinterpret_cast<float4*>(a.grad_slot + (size_t)tv.meta.x * kGradSlot);
               if (a.vis_dcolor) {  // SH colours: this view's colour gradient of the entry
                 const float4 dc = make_float4(out[1], out[2], out[3], 0.0f);
                 if (dc.x != 0.f || dc.y != 0.f || dc.z != 0.f) atomicAdd(a.vis_dcolor + tv.meta.y, dc);
                 out[1] = out[2] = out[3] = 0.0f;
               }
-              float4* dst = reinterpret_cast<float4*>(a.grad_slot + (size_t)tv.meta.x * kGradSlot);
+              float o2[20];
+#pragma unroll
+              for (int q = 0; q < 7; ++q) o2[q] = out[q];
+#pragma unroll
+              for (int q = 0; q < 12; ++q) o2[7 + q] = clipf(dv[q], kMinVal, kMaxVal);
+              o2[19] = 0.0f;
 #pragma unroll
               for (int c = 0; c < 5; ++c) {
-                const float4 v4 = make_float4(out[4 * c], out[4 * c + 1], out[4 * c + 2], out[4 * c + 3]);
+                const float4 v4 = make_float4(o2[4 * c], o2[4 * c + 1], o2[4 * c + 2], o2[4 * c + 3]);
                 if (v4.x != 0.f || v4.y != 0.f || v4.z != 0.f || v4.w != 0.f) atomicAdd(dst + c, v4);
               }
+            }
+            if (live) {  // each thread clears what it read
+              mm[8 + 4 * f] = 0.f; mm[9 + 4 * f] = 0.f; mm[10 + 4 * f] = 0.f; mm[11 + 4 * f] = 0.f;
+              if (f == 0) {
 #pragma unroll
-              for (int q = 0; q < kMom; ++q) mm[q] = 0.0f;
+                for (int q = 0; q < 8; ++q) mm[q] = 0.0f;
+              }
             }
           }
           __syncthreads();
