@@ -44,6 +44,11 @@ RES = ((256, 256), (512, 512), (800, 600), (1024, 1024))
 N_VIEWS = 16
 LR = dict(lr_verts=1e-4, lr_dens=1e-2, lr_grads=1e-3)
 LR_SH = 2.5e-3
+# DRAM bytes (read + write) per (tile, tet) pair of the fused compositing
+# kernel, from one ncu capture of this workload's launch
+# (dram__bytes_read.sum + dram__bytes_write.sum = 4.83 GB for 37.74 M pairs);
+# the roofline's "traffic" scales it to the run's pair count.
+TILE_DRAM_BYTES_PER_PAIR = 128.0
 
 
 def res_text(res) -> str:
@@ -238,7 +243,8 @@ def run_gpu(args):
         "gpu_launches": int(total_launches),
         "stage_ms_per_step": {k: round(v / nsteps_prof, 4) for k, v in stage_ms.items()},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": None,
+                     "frac": round(achieved / peak, 4),
+                     "traffic": int(TILE_DRAM_BYTES_PER_PAIR * int(info.n_pairs_last)),
                      "kernel": "tile_kernel<12,kModeTrain> (fused forward+loss+adjoint)",
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                      "fallback 6.65 TB/s", "launch_ms": round(comp_ms, 4), "algorithmic_bytes": alg,
