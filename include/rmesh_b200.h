@@ -181,6 +181,30 @@ RMESH_API int rmesh_accumulate_views(RmeshCtx* ctx, const RmeshCamera* cams, int
 RMESH_API int rmesh_grad_slots(RmeshCtx* ctx, float** device_ptr, uint64_t* n_floats);
 RMESH_API int rmesh_apply_adam(RmeshCtx* ctx, const RmeshTrainOpts* opts);
 
+/* ---- .rmesh scene decode -------------------------------------------------------
+ * The packed sections of a .rmesh file (crates/rmesh-data/src/lib.rs:247-393;
+ * the host parses the header and slices the decompressed bytes) -> the
+ * renderer's fp32 buffers, decoded on the device: densities exp((u8-100)/20),
+ * colour gradients f16 -> f32 (zeros when color_grads is NULL), SH
+ * coefficients [M][3][nc] = mean + weights x basis (PCA), circumdata
+ * [M][4] computed in double with the loader's degenerate-tet rules.  All
+ * pointers are device memory of the current device; asynchronous on stream. */
+typedef struct {
+  uint64_t n_vertices;
+  uint64_t n_tets;
+  uint32_t sh_degree;          /* 0..3 */
+  uint32_t k_components;       /* PCA components in the file (min(k, 3 nc) are stored) */
+  const float* vertices;       /* [3N] */
+  const uint32_t* indices;     /* [4M] */
+  const uint8_t* log_densities;   /* [M] */
+  const uint16_t* sh_mean;     /* [3 nc] f16 */
+  const uint16_t* sh_basis;    /* [k][3 nc] f16 */
+  const uint16_t* sh_weights;  /* [M][k] f16 */
+  const uint16_t* color_grads; /* [3M] f16 or NULL */
+} RmeshPackedScene;
+RMESH_API int rmesh_decode_scene(const RmeshPackedScene* scene, float* densities, float* color_grads,
+                                 float* sh_coeffs, float* circumdata, void* stream);
+
 /* ---- allocation-free tile count ---------------------------------------------
  * No counterpart in the reference.  For callers that must not allocate device
  * memory (a per-frame visibility query in a viewer loop, where cudaMalloc and

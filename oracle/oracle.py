@@ -199,6 +199,29 @@ class Oracle:
                        _ptr(dd, self.rp), _ptr(dg, self.rp), _ptr(db, self.rp), ctypes.c_int(threads))
         return {"d_vertices": dv, "d_densities": dd, "d_color_grads": dg, "d_base_colors": db}
 
+    def rmesh_decode(self, raw: bytes) -> dict:
+        """crates/rmesh-data/src/lib.rs:247-393 on decompressed .rmesh bytes."""
+        buf = np.frombuffer(raw, dtype=np.uint8)
+        hdr = np.zeros(4, np.uint32)
+        if getattr(self.lib, "orc_rmesh_header_" + self.dtype)(_ptr(buf, _u8p), ctypes.c_int64(buf.size),
+                                                                _ptr(hdr, _u32p)) != 0:
+            raise ValueError("truncated .rmesh header")
+        n, m, deg, _ = (int(x) for x in hdr)
+        nc = (deg + 1) ** 2
+        out = {"start_pose": np.zeros(7, np.float32), "vertices": np.zeros(3 * n, np.float32),
+               "indices": np.zeros(4 * m, np.uint32), "densities": np.zeros(m, np.float32),
+               "sh_coeffs": np.zeros(3 * nc * m, np.float32), "color_grads": np.zeros(3 * m, np.float32),
+               "circumdata": np.zeros(4 * m, np.float32)}
+        fn = getattr(self.lib, "orc_rmesh_decode_" + self.dtype)
+        fn.restype = ctypes.c_int64
+        fp = lambda k: _ptr(out[k], _f32p)
+        end = fn(_ptr(buf, _u8p), ctypes.c_int64(buf.size), fp("start_pose"), fp("vertices"),
+                 _ptr(out["indices"], _u32p), fp("densities"), fp("sh_coeffs"), fp("color_grads"), fp("circumdata"))
+        if end < 0:
+            raise ValueError("truncated .rmesh file")
+        out["sh_degree"] = deg
+        return out
+
     def adam(self, params, grads, m, v, step, lr, beta1=0.9, beta2=0.999, eps=1e-8):
         """In place on float arrays of this oracle's dtype."""
         self._adam(ctypes.c_int64(params.size), _ptr(params, self.rp), _ptr(self._r(grads), self.rp),

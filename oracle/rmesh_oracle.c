@@ -1035,6 +1035,131 @@ EXPORT void SFX(orc_adam)(int64_t n, R* params, const R* grads, R* m, R* v, uint
     }
 }
 
+/* ======================================================================== */
+/* .rmesh scene file (crates/rmesh-data/src/lib.rs:142-393), on the        */
+/* decompressed bytes.  Layout: u32 N, M, sh_degree, k; f32 pose[8];       */
+/* f32 vertices[3N]; u32 indices[4M]; u8 log-densities[M]; align 4;        */
+/* f16 SH mean[D], basis[k'][D], weights[M][k'] (D = 3 (deg+1)^2,          */
+/* k' = min(k, D)); align 4; f16 colour gradients[3M] (zeros when a tagged */
+/* "RMTX" section starts there, zero-padded when the file is short).       */
+/* ======================================================================== */
+static float half_bits_to_float(uint16_t h) {
+    uint32_t sgn = (uint32_t)(h >> 15) << 31, e = (h >> 10) & 0x1Fu, m = h & 0x3FFu, bits;
+    if (e == 0) {
+        if (m == 0) {
+            bits = sgn;
+        } else { /* subnormal: renormalise */
+            int ee = 127 - 15 + 1;
+            while (!(m & 0x400u)) { m <<= 1; ee--; }
+            bits = sgn | ((uint32_t)ee << 23) | ((m & 0x3FFu) << 13);
+        }
+    } else if (e == 31) {
+        bits = sgn | 0x7F800000u | (m << 13);
+    } else {
+        bits = sgn | ((e - 15 + 127) << 23) | (m << 13);
+    }
+    float f;
+    memcpy(&f, &bits, 4);
+    return f;
+}
+
+static uint32_t rd_u32(const uint8_t* d, int64_t off) { uint32_t v; memcpy(&v, d + off, 4); return v; }
+static uint16_t rd_u16(const uint8_t* d, int64_t off) { uint16_t v; memcpy(&v, d + off, 2); return v; }
+
+/* header -> hdr[0..3] = N, M, sh_degree, k; returns -1 when too short */
+EXPORT int SFX(orc_rmesh_header)(const uint8_t* d, int64_t len, uint32_t* hdr) {
+    if (len < 48) return -1;
+    for (int i = 0; i < 4; ++i) hdr[i] = rd_u32(d, 4 * i);
+    return 0;
+}
+
+/* Circumsphere of one tet in double precision with the loader's degenerate
+ * handling (lib.rs:601-707). */
+typedef struct { double x, y, z; } D3;
+static D3 d3(double x, double y, double z) { D3 r = {x, y, z}; return r; }
+static D3 d3sub(D3 a, D3 b) { return d3(a.x - b.x, a.y - b.y, a.z - b.z); }
+static D3 d3add(D3 a, D3 b) { return d3(a.x + b.x, a.y + b.y, a.z + b.z); }
+static D3 d3scale(D3 a, double s) { return d3(a.x * s, a.y * s, a.z * s); }
+static double d3dot(D3 a, D3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+static D3 d3cross(D3 a, D3 b) { return d3(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y); }
+static double d3len(D3 a) { return sqrt(d3dot(a, a)); }
+
+static void circumsphere_f64(const float* verts, const uint32_t* q, float* out) {
+    D3 v[4];
+    for (int k = 0; k < 4; ++k)
+        v[k] = d3((double)verts[3 * q[k]], (double)verts[3 * q[k] + 1], (double)verts[3 * q[k] + 2]);
+    D3 a = d3sub(v[1], v[0]), b = d3sub(v[2], v[0]), c = d3sub(v[3], v[0]);
+    double aa = d3dot(a, a), bb = d3dot(b, b), cc = d3dot(c, c);
+    D3 bc = d3cross(b, c), ca = d3cross(c, a), ab = d3cross(a, b);
+    double denom = 2.0 * d3dot(a, bc);
+    if (fabs(denom) < 1e-10) {
+        double md = d3len(d3sub(v[1], v[0]));
+        md = fmax(md, d3len(d3sub(v[2], v[0])));
+        md = fmax(md, d3len(d3sub(v[3], v[0])));
+        md = fmax(md, d3len(d3sub(v[2], v[1])));
+        md = fmax(md, d3len(d3sub(v[3], v[1])));
+        md = fmax(md, d3len(d3sub(v[3], v[2])));
+        D3 cen = d3scale(d3add(d3add(d3add(v[0], v[1]), v[2]), v[3]), 0.25);
+        out[0] = (float)cen.x; out[1] = (float)cen.y; out[2] = (float)cen.z;
+        if (md < 1e-7) {
+            double r = d3len(d3sub(v[0], cen));
+            r = fmin(r, d3len(d3sub(v[1], cen)));
+            r = fmin(r, d3len(d3sub(v[2], cen)));
+            r = fmin(r, d3len(d3sub(v[3], cen)));
+            out[3] = (float)(r * r);
+        } else {
+            out[3] = 1e20f;
+        }
+        return;
+    }
+    D3 num = d3add(d3add(d3scale(bc, aa), d3scale(ca, bb)), d3scale(ab, cc));
+    D3 rel = d3(num.x / denom, num.y / denom, num.z / denom);
+    D3 cen = d3add(v[0], rel);
+    out[0] = (float)cen.x; out[1] = (float)cen.y; out[2] = (float)cen.z;
+    out[3] = (float)d3dot(rel, rel);
+}
+
+/* Decodes the whole file; arrays sized from the header.  Returns the byte
+ * offset after the colour gradients, or -1 when the file is too short. */
+EXPORT int64_t SFX(orc_rmesh_decode)(const uint8_t* d, int64_t len, float* pose7, float* verts, uint32_t* idx,
+                                     float* dens, float* sh, float* grads, float* circ) {
+    uint32_t N = rd_u32(d, 0), M = rd_u32(d, 4), deg = rd_u32(d, 8), k = rd_u32(d, 12);
+    int64_t off = 16;
+    for (int i = 0; i < 7; ++i) memcpy(&pose7[i], d + off + 4 * i, 4);
+    off += 32;
+    const uint32_t nc = (deg + 1u) * (deg + 1u), D = 3u * nc, K = k < D ? k : D;
+    int64_t need = off + 12ll * N + 16ll * M + M;
+    if (len < need) return -1;
+    memcpy(verts, d + off, 12ull * N); off += 12ll * N;
+    memcpy(idx, d + off, 16ull * M); off += 16ll * M;
+    for (uint32_t t = 0; t < M; ++t) dens[t] = expf(((float)d[off + t] - 100.0f) / 20.0f);
+    off += M;
+    off = (off + 3) & ~(int64_t)3;
+    if (len < off + 2ll * (D + (int64_t)K * D + (int64_t)M * K)) return -1;
+    const int64_t mean_off = off, basis_off = off + 2ll * D, w_off = basis_off + 2ll * K * D;
+    off = w_off + 2ll * M * K;
+    for (uint32_t t = 0; t < M; ++t)
+        for (uint32_t f = 0; f < D; ++f) {
+            float val = half_bits_to_float(rd_u16(d, mean_off + 2ll * f));
+            for (uint32_t q = 0; q < K; ++q)
+                val += half_bits_to_float(rd_u16(d, w_off + 2ll * ((int64_t)t * K + q))) *
+                       half_bits_to_float(rd_u16(d, basis_off + 2ll * ((int64_t)q * D + f)));
+            sh[(int64_t)t * D + f] = val;
+        }
+    off = (off + 3) & ~(int64_t)3;
+    const int64_t ng = 3ll * M;
+    if (off + 4 <= len && rd_u32(d, off) == 0x524D5458u) {
+        memset(grads, 0, sizeof(float) * ng);
+    } else {
+        int64_t avail = (len - off) / 2;
+        if (avail > ng) avail = ng;
+        for (int64_t i = 0; i < ng; ++i) grads[i] = i < avail ? half_bits_to_float(rd_u16(d, off + 2 * i)) : 0.0f;
+        off += 2 * avail;
+    }
+    for (uint32_t t = 0; t < M; ++t) circumsphere_f64(verts, idx + 4ull * t, circ + 4ull * t);
+    return off;
+}
+
 EXPORT void SFX(orc_set_threads)(int n) {
 #ifdef _OPENMP
     if (n > 0) omp_set_num_threads(n);

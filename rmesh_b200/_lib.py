@@ -36,6 +36,7 @@ EXPORTED = (
     "rmesh_debug_tiles_touched", "rmesh_debug_pairs", "rmesh_debug_ranges", "rmesh_set_profiling",
     "rmesh_stage_times", "rmesh_accumulate_views", "rmesh_grad_slots", "rmesh_apply_adam",
     "rmesh_count_tiles_static", "rmesh_update_sh", "rmesh_get_sh", "rmesh_get_sh_grad", "rmesh_set_lr_sh",
+    "rmesh_decode_scene",
 )
 
 COUNTERS_BYTES = 792  # sizeof(rm::Counters), read back once per training run
@@ -49,6 +50,15 @@ class SceneDesc(ctypes.Structure):
         ("width", ctypes.c_int32), ("height", ctypes.c_int32), ("aux_dim", ctypes.c_int32),
         ("tile_size", ctypes.c_int32), ("device", ctypes.c_int32), ("sh_degree", ctypes.c_int32),
         ("sh_coeffs", ctypes.c_void_p), ("reserved", ctypes.c_int32 * 2),
+    ]
+
+
+class PackedScene(ctypes.Structure):
+    _fields_ = [
+        ("n_vertices", ctypes.c_uint64), ("n_tets", ctypes.c_uint64), ("sh_degree", ctypes.c_uint32),
+        ("k_components", ctypes.c_uint32), ("vertices", ctypes.c_void_p), ("indices", ctypes.c_void_p),
+        ("log_densities", ctypes.c_void_p), ("sh_mean", ctypes.c_void_p), ("sh_basis", ctypes.c_void_p),
+        ("sh_weights", ctypes.c_void_p), ("color_grads", ctypes.c_void_p),
     ]
 
 
@@ -119,6 +129,7 @@ def load() -> ctypes.CDLL:
         "rmesh_get_sh": ([vp, vp], ctypes.c_int),
         "rmesh_get_sh_grad": ([vp, vp], ctypes.c_int),
         "rmesh_set_lr_sh": ([vp, f32], ctypes.c_int),
+        "rmesh_decode_scene": ([P(PackedScene), vp, vp, vp, vp, vp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -24,6 +24,7 @@
 #include "bin.cuh"
 #include "common.cuh"
 #include "project.cuh"
+#include "rmesh_file.cuh"
 #include "sh.cuh"
 #include "sort.cuh"
 #include "tile.cuh"
@@ -1427,6 +1428,60 @@ extern "C" int rmesh_count_tiles_static(const float* vertices, uint64_t n_vertic
   }
   count_tiles_static_kernel<<<nblk, 256, 0, st>>>(vertices, n_vertices, indices, densities, (uint32_t)M, V,
                                                    tiles_touched, visible_tets, counts, scratch);
+  if (cudaGetLastError() != cudaSuccess) return RMESH_ERR_CUDA;
+  return RMESH_OK;
+}
+
+// ============================================================================
+// .rmesh scene decode (rmesh_decode_scene): the host slices the file into its
+// sections and uploads them; the kernels in rmesh_file.cuh decode them.
+// ============================================================================
+extern "C" int rmesh_decode_scene(const RmeshPackedScene* in, float* densities, float* color_grads, float* sh_coeffs,
+                                  float* circumdata, void* stream) {
+  using namespace rm;
+  if (!in || !densities || !color_grads || !sh_coeffs || !circumdata) return RMESH_ERR_INVALID_ARG;
+  if (in->n_tets == 0 || in->n_vertices == 0 || in->sh_degree > 3 || in->n_tets > (1ull << 31))
+    return RMESH_ERR_INVALID_ARG;
+  if (!in->vertices || !in->indices || !in->log_densities || !in->sh_mean || !in->sh_basis || !in->sh_weights)
+    return RMESH_ERR_INVALID_ARG;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
+    cudaGetLastError();
+    return RMESH_ERR_NO_DEVICE;
+  }
+  const uint64_t M = in->n_tets, N = in->n_vertices;
+  const uint32_t nc = (in->sh_degree + 1) * (in->sh_degree + 1), D = 3 * nc;
+  const uint32_t K = std::min<uint32_t>(in->k_components, D);
+  if (!device_range_ok(in->vertices, 12 * N, dev) || !device_range_ok(in->indices, 16 * M, dev) ||
+      !device_range_ok(in->log_densities, M, dev) || !device_range_ok(in->sh_mean, 2ull * D, dev) ||
+      (K > 0 && !device_range_ok(in->sh_basis, 2ull * K * D, dev)) ||
+      (K > 0 && !device_range_ok(in->sh_weights, 2ull * K * M, dev)) ||
+      (in->color_grads && !device_range_ok(in->color_grads, 6 * M, dev)) || !device_range_ok(densities, 4 * M, dev) ||
+      !device_range_ok(color_grads, 12 * M, dev) || !device_range_ok(sh_coeffs, 4ull * D * M, dev) ||
+      !device_range_ok(circumdata, 16 * M, dev))
+    return RMESH_ERR_INVALID_ARG;
+  SceneDecodeArgs a;
+  a.M = M;
+  a.D = D;
+  a.K = K;
+  a.verts = in->vertices;
+  a.idx = in->indices;
+  a.log_dens = in->log_densities;
+  a.mean = in->sh_mean;
+  a.basis = in->sh_basis;
+  a.weights = in->sh_weights;
+  a.grads16 = in->color_grads;
+  a.dens = densities;
+  a.grads = color_grads;
+  a.sh = sh_coeffs;
+  a.circ = reinterpret_cast<float4*>(circumdata);
+  for (int i = 0; i < 256; ++i) a.table.v[i] = std::exp(((float)i - 100.0f) / 20.0f);  // the loader's f32 expf
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const unsigned b1 = (unsigned)std::min<uint64_t>((M + 255) / 256, 65535ull * 8);
+  decode_tets_kernel<<<b1, 256, 0, st>>>(a);
+  if (cudaGetLastError() != cudaSuccess) return RMESH_ERR_CUDA;
+  const unsigned b2 = (unsigned)std::min<uint64_t>((M * D + 255) / 256, 65535ull * 8);
+  pca_decode_kernel<<<b2, 256, 0, st>>>(a);
   if (cudaGetLastError() != cudaSuccess) return RMESH_ERR_CUDA;
   return RMESH_OK;
 }
