@@ -156,6 +156,16 @@ RMESH_API int rmesh_forward_tiled(RmeshCtx* ctx, const RmeshCamera* cam, float* 
 RMESH_API int rmesh_backward(RmeshCtx* ctx, const float* dl_d_image, float* d_vertices, float* d_densities,
                    float* d_base_colors, float* d_color_grads);
 
+/* forward_error, lib.rs:1621-1710 (the kernel: crates/rmesh-error/src/wgsl/
+ * error_tiled_compute.wgsl): per-tet error statistics over the tile lists of
+ * the last rmesh_forward_tiled.  pixel_err, ssim_err [H*W]; outputs
+ * tet_err [M][16] f32 (0 weight, 1 weight*L1, 2 weight*L1^2, 5 weight*SSIM,
+ * 6..8 weight*entry point, 9..11 weight*exit point, 12 weight,
+ * 13..15 weight*centroid; weight = T * optical depth) and tet_count [M][2]
+ * i32 (covered pixels, max of int(65535 * weight)), cleared by the call. */
+RMESH_API int rmesh_forward_error(RmeshCtx* ctx, const float* pixel_err, const float* ssim_err, float* tet_err,
+                                  int32_t* tet_count);
+
 /* train_step, lib.rs:2405-2636: forward, loss, adjoint, Adam on vertices,
  * densities and color_grads; step += 1.  gt_rgb [H][W][3].  *loss_out receives
  * sum over pixels and RGB of (r-gt)^2 / n_pixels (L2) or |r-gt| / n_pixels (L1);

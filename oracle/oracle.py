@@ -199,6 +199,22 @@ class Oracle:
                        _ptr(dd, self.rp), _ptr(dg, self.rp), _ptr(db, self.rp), ctypes.c_int(threads))
         return {"d_vertices": dv, "d_densities": dd, "d_color_grads": dg, "d_base_colors": db}
 
+    def error_stats(self, scene, cam, fwd, pixel_err, ssim_err, tile_size=12, min_t=0.0):
+        """Per-tet error statistics (error_tiled_compute.wgsl:90-373) over the
+        tile lists of the forward ``fwd``: (tet_err [M, 16] f64, tet_count [M, 2] i32)."""
+        vp, c2w, intr, cp, W, H = self._cam(cam)
+        m = scene["indices"].size // 4
+        err = np.zeros(16 * m, np.float64)
+        cnt = np.zeros(2 * m, np.int32)
+        fn = getattr(self.lib, "orc_error_stats_" + self.dtype)
+        fn(_ptr(self._r(scene["vertices"]), self.rp), _ptr(self._u(scene["indices"]), _u32p),
+           _ptr(self._r(scene["densities"]), self.rp), _ptr(self._u(fwd["vals"]), _u32p),
+           _ptr(self._u(fwd["ranges"]), _u32p), _ptr(vp, self.rp), _ptr(c2w, self.rp), _ptr(intr, self.rp),
+           _ptr(cp, self.rp), ctypes.c_int(W), ctypes.c_int(H), ctypes.c_int(tile_size), self._rt(min_t),
+           _ptr(self._r(pixel_err), self.rp), _ptr(self._r(ssim_err), self.rp), _ptr(err, _f64p),
+           _ptr(cnt, ctypes.POINTER(ctypes.c_int32)))
+        return err.reshape(m, 16), cnt.reshape(m, 2)
+
     def rmesh_decode(self, raw: bytes) -> dict:
         """crates/rmesh-data/src/lib.rs:247-393 on decompressed .rmesh bytes."""
         buf = np.frombuffer(raw, dtype=np.uint8)

@@ -750,6 +750,75 @@ EXPORT void SFX(orc_rasterize)(const R* verts, const uint32_t* idx, const R* col
 }
 
 /* ======================================================================== */
+/* orc_error_stats -- crates/rmesh-error/src/wgsl/error_tiled_compute.wgsl:  */
+/* 90-373: the forward's front-to-back tile walk (vertex-row spans, no end   */
+/* trimming), skipping pixels whose log transmittance fell below -5.5; each  */
+/* covered pixel with T >= 1e-6 adds, with w = T * od, to its tet:           */
+/* tet_err[16t + 0] w, [1] w pe, [2] w pe^2, [5] w se, [6..8] w entry,       */
+/* [9..11] w exit, [12] w, [13..15] w centroid; tet_count[2t] += 1,          */
+/* tet_count[2t+1] = max(., i32(65535 w)).  Serial, accumulated in double.   */
+/* ======================================================================== */
+EXPORT void SFX(orc_error_stats)(const R* verts, const uint32_t* idx, const R* dens, const uint32_t* vals,
+                                 const uint32_t* ranges, const R* vp, const R* c2w, const R* intr, const R* cam3,
+                                 int W, int H, int TS, R min_t, const R* pixel_err, const R* ssim_err,
+                                 double* tet_err, int32_t* tet_count) {
+    Cam cm = {vp, c2w, intr, cam3, W, H, TS, min_t};
+    uint32_t tiles_x = (uint32_t)((W + TS - 1) / TS), tiles_y = (uint32_t)((H + TS - 1) / TS);
+    int64_t ntiles = (int64_t)tiles_x * tiles_y;
+    V3 cam = v3(cam3[0], cam3[1], cam3[2]);
+    for (int64_t tile = 0; tile < ntiles; ++tile) {
+        uint32_t tile_x = (uint32_t)(tile % tiles_x), tile_y = (uint32_t)(tile / tiles_x);
+        R tile_ox = (R)(tile_x * (uint32_t)TS), tile_oy = (R)(tile_y * (uint32_t)TS);
+        R logt[256];
+        for (int i = 0; i < 256; ++i) logt[i] = 0;
+        uint32_t rs = ranges[2 * tile], re = ranges[2 * tile + 1];
+        uint32_t cursor = re;
+        while (cursor > rs) {
+            cursor -= 1u;
+            uint32_t t = vals[cursor];
+            V3 v[4];
+            for (int k = 0; k < 4; ++k) v[k] = load_v3(verts, idx[4 * t + k]);
+            R px4[4], py4[4];
+            int any_behind = tile_proj(&cm, v, tile_ox, tile_oy, px4, py4);
+            V3 n[4];
+            face_normals(v, n);
+            V3 cen = vscale(vadd(vadd(vadd(v[0], v[1]), v[2]), v[3]), (R)0.25);
+            for (int r = 0; r < TS; ++r) {
+                int32_t xa, xb;
+                if (!row_span(any_behind, px4, py4, (uint32_t)r, TS, 1, &xa, &xb)) continue;
+                for (int32_t cc = xa; cc <= xb; ++cc) {
+                    int pl = r * TS + cc;
+                    uint32_t pxg = tile_x * (uint32_t)TS + (uint32_t)cc, pyg = tile_y * (uint32_t)TS + (uint32_t)r;
+                    if (pxg >= (uint32_t)W || pyg >= (uint32_t)H) continue;
+                    if (logt[pl] < (R)-5.5) continue;
+                    V3 d = pixel_dir(&cm, pxg, pyg);
+                    V3 o = vadd(cam, vscale(d, min_t));
+                    R tmin, tmax;
+                    int efi;
+                    if (!intersect(v, n, o, d, &tmin, &tmax, &efi, NULL)) continue;
+                    R od = clipr(dens[t] * (tmax - tmin), (R)1e-8, (R)88.0);
+                    R trans = safe_exp(logt[pl]);
+                    if (trans < (R)1e-6) continue;
+                    R w = trans * od;
+                    V3 en = vadd(o, vscale(d, tmin)), ex = vadd(o, vscale(d, tmax));
+                    size_t pidx = (size_t)pyg * (size_t)W + pxg;
+                    double pe = (double)pixel_err[pidx], se = (double)ssim_err[pidx], wd = (double)w;
+                    double* e = tet_err + 16 * (size_t)t;
+                    e[0] += wd; e[1] += wd * pe; e[2] += wd * pe * pe; e[5] += wd * se;
+                    e[6] += wd * en.x; e[7] += wd * en.y; e[8] += wd * en.z;
+                    e[9] += wd * ex.x; e[10] += wd * ex.y; e[11] += wd * ex.z;
+                    e[12] += wd; e[13] += wd * cen.x; e[14] += wd * cen.y; e[15] += wd * cen.z;
+                    tet_count[2 * t] += 1;
+                    int32_t q = f2i((R)65535 * w);
+                    if (q > tet_count[2 * t + 1]) tet_count[2 * t + 1] = q;
+                    logt[pl] -= od;
+                }
+            }
+        }
+    }
+}
+
+/* ======================================================================== */
 /* orc_loss -- loss_compute.wgsl:24-72 plus the host loss value the         */
 /* reference tests compute (kernel_tests.rs:869-878): sum over pixels and   */
 /* RGB of (r-gt)^2 / n_pixels (L2) or |r-gt| / n_pixels (L1), in double.   */

@@ -102,6 +102,7 @@ struct RmeshCtx {
   DevBuf vis_color, vis_dcolor, vis_index;  // SH colours per entry, their gradients, (view, tet) -> entry
   DevBuf pair_key, pair_val, pair_key_alt, pair_val_alt, ranges;
   DevBuf rgba, aux, dl, gt, out_a, out_b, out_c, out_d;
+  DevBuf err_in, err_out;  // per-pixel error inputs, per-tet error statistics
   uint64_t cap_pairs = 0;
   uint64_t generation = 0;  // bumped whenever a buffer is reallocated
 
@@ -967,7 +968,7 @@ int rmesh_get_info(RmeshCtx* c, RmeshInfo* info) {
                    &c->vis_cnt, &c->vis_proj, &c->vis_view, &c->vis_key_alt, &c->vis_val_alt, &c->tiles_touched, &c->pair_key,
                    &c->pair_val, &c->pair_key_alt, &c->pair_val_alt, &c->ranges, &c->rgba, &c->aux, &c->dl,
                    &c->gt, &c->out_a, &c->out_b, &c->out_c, &c->out_d, &c->sh, &c->m_sh, &c->v_sh,
-                   &c->vis_color, &c->vis_dcolor, &c->vis_index};
+                   &c->vis_color, &c->vis_dcolor, &c->vis_index, &c->err_in, &c->err_out};
   for (DevBuf* b : all) info->device_bytes += b->bytes;
   return RMESH_OK;
 }
@@ -1045,6 +1046,37 @@ int rmesh_backward(RmeshCtx* c, const float* dl, float* d_verts, float* d_dens, 
   if (d_dens) CK(cudaMemcpyAsync(d_dens, c->out_b.p, M * 4, cudaMemcpyDefault, c->stream));
   if (d_base) CK(cudaMemcpyAsync(d_base, c->out_c.p, 3 * M * 4, cudaMemcpyDefault, c->stream));
   if (d_cgrad) CK(cudaMemcpyAsync(d_cgrad, c->out_d.p, 3 * M * 4, cudaMemcpyDefault, c->stream));
+  CKR(sync_counters(c, 1));
+  return status_from_bits(c);
+}
+
+int rmesh_forward_error(RmeshCtx* c, const float* pixel_err, const float* ssim_err, float* tet_err,
+                        int32_t* tet_count) {
+  if (!c || !pixel_err || !ssim_err || !tet_err || !tet_count) return RMESH_ERR_INVALID_ARG;
+  if (!c->have_forward) return fail(c, RMESH_ERR_STATE, "forward_error() must follow forward_tiled()");
+  const ViewParams& v = c->views_h[0];
+  const uint64_t npix = (uint64_t)v.W * v.H;
+  const size_t M = (size_t)c->M;
+  CKR(ensure_buf(c, c->err_in, npix * 8));
+  CKR(ensure_buf(c, c->err_out, M * 18 * 4));
+  float* pe = c->err_in.as<float>();
+  CK(cudaMemcpyAsync(pe, pixel_err, npix * 4, cudaMemcpyDefault, c->stream));
+  CK(cudaMemcpyAsync(pe + npix, ssim_err, npix * 4, cudaMemcpyDefault, c->stream));
+  CK(cudaMemsetAsync(c->err_out.p, 0, M * 18 * 4, c->stream));
+  Counters* cnt = c->counters_d.as<Counters>();
+  CK(cudaMemsetAsync(&cnt->tile_ticket, 0, sizeof(uint32_t), c->stream));
+  ViewParams* vd = c->views_d.as<ViewParams>();
+  {
+    StageScope sc(c, kStComposite, false);
+    TileArgs ta = base_tile_args(c, vd, 1, c->last_tiles, cnt);
+    ta.pixel_err = pe;
+    ta.ssim_err = pe + npix;
+    ta.tet_err = c->err_out.as<float>();
+    ta.tet_count = reinterpret_cast<int*>(c->err_out.as<float>() + M * 16);
+    CKR((launch_tile_m<kModeError, false>(c, ta, c->last_tiles, true)));
+  }
+  CK(cudaMemcpyAsync(tet_err, c->err_out.p, M * 16 * 4, cudaMemcpyDefault, c->stream));
+  CK(cudaMemcpyAsync(tet_count, c->err_out.as<float>() + M * 16, M * 8, cudaMemcpyDefault, c->stream));
   CKR(sync_counters(c, 1));
   return status_from_bits(c);
 }

@@ -51,7 +51,7 @@ constexpr int kBatch = 32;
 constexpr int kMom = 24;      // adjoint moments per tet (see phase 2)
 constexpr int kMomHalf = 12;  // moments transposed per reduction pass
 
-enum TileMode : int { kModeForward = 0, kModeBackward = 1, kModeTrain = 2 };
+enum TileMode : int { kModeForward = 0, kModeBackward = 1, kModeTrain = 2, kModeError = 3 };
 
 struct TileArgs {
   const ViewParams* views;
@@ -67,6 +67,10 @@ struct TileArgs {
   float* aux;                  // [pixels][8] (optional, forward only)
   const float* dl_rgba;        // [pixels][4] (backward mode)
   const float* gt_rgb;         // [pixels][3] (train mode)
+  const float* pixel_err;      // [pixels] (error mode)
+  const float* ssim_err;       // [pixels] (error mode)
+  float* tet_err;              // [M][16] (error mode, accumulated)
+  int* tet_count;              // [M][2] (error mode, accumulated)
   float* grad_slot;            // [M][kGradSlot]
   // SH colours: per-entry colours (the min_t path reads them) and per-entry
   // colour gradients, which then go through the SH adjoint instead of the
@@ -451,8 +455,9 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
                             clipf(I.ceb * I.w0 + I.csb * I.w1, lo, kMaxVal), I.od);
           out2 = make_float4(t_min, t_max, __uint_as_float(pack_item(fmin, fmax, k, p)), I.alpha_t);
         }
+        if (MODE == kModeError && hit) out.x = out.y = out.z = 0.0f;  // (weight, counted) filled by phase 1
         s.item[i] = out;
-        if (AUX || !fwd) s.itemx[i] = out2;
+        if (AUX || !fwd || MODE == kModeError) s.itemx[i] = out2;
       }
     };
 
@@ -558,6 +563,162 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
         if (AUX && a.aux) {
           reinterpret_cast<float4*>(a.aux)[2 * pix] = make_float4(nd0, nd1, nd2, nd3);
           reinterpret_cast<float4*>(a.aux)[2 * pix + 1] = make_float4(en0, en1, en2, en3);
+        }
+      }
+    }
+
+    // =============== error statistics (front to back) ===============
+    // crates/rmesh-error/src/wgsl/error_tiled_compute.wgsl:90-373: the forward's
+    // walk with a -5.5 log-transmittance cut; each covered pixel with T >= 1e-6
+    // gives its tet the weight w = T * od.  Phase 1 (per pixel, in order) sets
+    // the item to (w, 1); phase 2 reduces per tet (w, w pe, w pe^2, w se,
+    // w entry, w exit, count, max 65535 w) and the flush adds them to tet_err /
+    // tet_count.
+    if (MODE == kModeError) {
+      bool alive = valid;
+      if (in_tile) s.pdl[pl] = valid ? make_float4(a.pixel_err[pix], a.ssim_err[pix], 0.f, 0.f)
+                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+      if (re > rs) {
+        {
+          const int nb0 = (int)min((uint32_t)kBatch, re - rs);
+          issue(0, nb0, load_idx(re - 1u, nb0, -1));
+        }
+        uint32_t idx_next = 0u;
+        if (re - rs > (uint32_t)kBatch) {
+          const uint32_t h1 = re - (uint32_t)kBatch;
+          idx_next = load_idx(h1 - 1u, (int)min((uint32_t)kBatch, h1 - rs), -1);
+        }
+        int b = 0;
+        for (uint32_t hi = re; hi > rs;) {
+          const int buf = b & 1;
+          const int nb = (int)min((uint32_t)kBatch, hi - rs);
+          const uint32_t next_hi = hi - (uint32_t)nb;
+          wait_buf(buf);
+          if (failed) break;
+          if (next_hi > rs) {
+            const int nbn = (int)min((uint32_t)kBatch, next_hi - rs);
+            issue(buf ^ 1, nbn, idx_next);
+            const uint32_t h2 = next_hi - (uint32_t)nbn;
+            if (h2 > rs) idx_next = load_idx(h2 - 1u, (int)min((uint32_t)kBatch, h2 - rs), -1);
+          }
+          spans(buf, nb, true);
+          __syncthreads();
+          prefixes(nb);
+          __syncthreads();
+          fill(nb);
+          __syncthreads();
+          for (int k0 = 0; k0 < nb;) {
+            const int k1 = sub_end(k0, nb);
+            const uint32_t base = s.toff[k0];
+            const uint32_t n_items = s.toff[k1] - base;
+            phase0(buf, k0, k1, true);
+            __syncthreads();
+            if (alive) {
+              uint32_t m = s.pmask[pl] & ((k1 >= 32 ? 0xffffffffu : ((1u << k1) - 1u)) & ~((1u << k0) - 1u));
+              while (m) {
+                const int k = __ffs(m) - 1;
+                m &= m - 1u;
+                if (logT < -5.5f) break;
+                const uint32_t it = item_of(k, base);
+                const float od = s.item[it].w;
+                if (od < 0.0f) continue;  // ray miss
+                const float Tj = __expf(clipf(logT, -88.0f, kLogMax));
+                if (Tj >= 1e-6f) {
+                  s.item[it] = make_float4(Tj * od, 1.0f, 0.0f, od);
+                  logT -= od;
+                }
+              }
+              if (logT < -5.5f) alive = false;
+            }
+            __syncthreads();
+            // phase 2: per-tet sums of the item statistics (12 columns; column 11
+            // is a maximum), a segment of rows per lane as in the adjoint
+            float(*red)[kMomHalf + 1] = s.red[warp];
+            for (uint32_t chunk = (uint32_t)warp * 32u; chunk < n_items; chunk += (uint32_t)NT) {
+              const uint32_t i = chunk + (uint32_t)lane;
+              float m[kMomHalf];
+#pragma unroll
+              for (int q = 0; q < kMomHalf; ++q) m[q] = 0.0f;
+              int k = -1;
+              if (i < n_items) {
+                const float4 st = s.item[i];
+                const float4 ix = s.itemx[i];
+                const uint32_t pk = __float_as_uint(ix.z);
+                k = (int)((pk >> 5) & 31u);
+                if (st.y > 0.5f) {
+                  const int p = (int)(pk >> 10);
+                  const float w = st.x;
+                  const float4 d = s.pdir[p];
+                  const float4 e = s.pdl[p];
+                  const float ox = camx + d.x * V.min_t, oy = camy + d.y * V.min_t, oz = camz + d.z * V.min_t;
+                  m[0] = w;
+                  m[1] = w * e.x;
+                  m[2] = w * e.x * e.x;
+                  m[3] = w * e.y;
+                  m[4] = w * (ox + d.x * ix.x); m[5] = w * (oy + d.y * ix.x); m[6] = w * (oz + d.z * ix.x);
+                  m[7] = w * (ox + d.x * ix.y); m[8] = w * (oy + d.y * ix.y); m[9] = w * (oz + d.z * ix.y);
+                  m[10] = 1.0f;
+                  m[11] = __int_as_float(__float2int_rz(65535.0f * w));
+                }
+              }
+              const int kp = __shfl_up_sync(0xffffffffu, k, 1);
+              const unsigned heads = __ballot_sync(0xffffffffu, k >= 0 && (lane == 0 || kp != k));
+              const int n_rows = __popc(__ballot_sync(0xffffffffu, k >= 0));
+#pragma unroll
+              for (int q = 0; q < kMomHalf; ++q) red[lane][q] = m[q];
+              red[lane][kMomHalf] = __int_as_float(k);
+              __syncwarp();
+              const int wq = lane & 15, wr0 = (lane >> 4) * 16;
+              const int wr1 = min(wr0 + 16, n_rows);
+              if (wq < kMomHalf && wr0 < wr1) {
+                for (int r0 = wr0; r0 < wr1;) {
+                  const unsigned later = heads & ~((2u << r0) - 1u);
+                  const int r1 = later ? min(__ffs(later) - 1, wr1) : wr1;
+                  const int kk = __float_as_int(red[r0][kMomHalf]);
+                  if (wq == 11) {
+                    int mx = 0;
+                    for (int row = r0; row < r1; ++row) mx = max(mx, __float_as_int(red[row][wq]));
+                    if (mx > 0) atomicMax(reinterpret_cast<int*>(&s.mom[kk][11]), mx);
+                  } else {
+                    float sum = 0.0f;
+                    for (int row = r0; row < r1; ++row) sum += red[row][wq];
+                    if (sum != 0.0f) atomicAdd(&s.mom[kk][wq], sum);
+                  }
+                  r0 = r1;
+                }
+              }
+              __syncwarp();
+            }
+            __syncthreads();
+            k0 = k1;
+          }
+          // flush the batch's per-tet sums
+          if (tid < nb) {
+            float* mm = s.mom[tid];
+            if (mm[10] != 0.0f) {
+              const TetView& tv = s.view[buf][tid];
+              const uint32_t t = tv.meta.x;
+              const TetRec r = a.rec[t];
+              const float cx = (r.a.x + r.b.x + r.c.x + r.d.x) * 0.25f, cy = (r.a.y + r.b.y + r.c.y + r.d.y) * 0.25f,
+                          cz = (r.a.z + r.b.z + r.c.z + r.d.z) * 0.25f;
+              float* e = a.tet_err + 16 * (size_t)t;
+              atomicAdd(e + 0, mm[0]); atomicAdd(e + 1, mm[1]); atomicAdd(e + 2, mm[2]); atomicAdd(e + 5, mm[3]);
+              atomicAdd(e + 6, mm[4]); atomicAdd(e + 7, mm[5]); atomicAdd(e + 8, mm[6]);
+              atomicAdd(e + 9, mm[7]); atomicAdd(e + 10, mm[8]); atomicAdd(e + 11, mm[9]);
+              atomicAdd(e + 12, mm[0]);
+              atomicAdd(e + 13, mm[0] * cx); atomicAdd(e + 14, mm[0] * cy); atomicAdd(e + 15, mm[0] * cz);
+              atomicAdd(a.tet_count + 2 * (size_t)t, (int)mm[10]);
+              atomicMax(a.tet_count + 2 * (size_t)t + 1, __float_as_int(mm[11]));
+            }
+#pragma unroll
+            for (int q = 0; q < kMomHalf; ++q) mm[q] = 0.0f;
+          }
+          hi = next_hi;
+          ++b;
+          if (__syncthreads_count(alive) == 0) {  // every pixel below the cut
+            if (hi > rs) wait_buf(buf ^ 1);
+            break;
+          }
         }
       }
     }

@@ -295,6 +295,23 @@ class RMeshRenderer:
                 for t in (d_vertices, d_densities, d_base_colors, d_color_grads)]
         self._check(self._lib.rmesh_backward(self._ctx, p, *ptrs))
 
+    def forward_error(self, pixel_err, ssim_err):
+        """Per-tet error statistics over the last forward_tiled's tile lists
+        (lib.rs:1621-1710): (tet_err [M, 16] float32, tet_count [M, 2] int32)."""
+        n = self._width * self._height
+        keep = []
+        ps = []
+        for name, arr in (("pixel_err", pixel_err), ("ssim_err", ssim_err)):
+            obj, p = _as_array(arr, np.float32, name)
+            if _numel(obj) != n:
+                raise ValueError(f"{name} must have {n} elements, got {_numel(obj)}")
+            keep.append(obj)
+            ps.append(p)
+        err = np.empty((self._M, 16), np.float32)
+        cnt = np.empty((self._M, 2), np.int32)
+        self._check(self._lib.rmesh_forward_error(self._ctx, ps[0], ps[1], err.ctypes.data, cnt.ctypes.data))
+        return err, cnt
+
     def train_step(self, cam_pos, vp, c2w_intrinsics, gt_image, lr_verts: float, lr_dens: float,
                    lr_grads: float, loss_type: int, lr_sh: float = 0.0) -> float:
         cam = self._cam(cam_pos, vp, c2w_intrinsics)
