@@ -1,0 +1,71 @@
+"""Edge cases of the CUDA path vs the oracle (needs a B200): a view that sees
+nothing, a camera inside the mesh (negative depth keys, vertices behind the
+camera), and a multi-view step whose tiles exceed 2^16 in total."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import make_renderer, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def test_view_that_sees_nothing(c1_scene, oracle32):
+    from rmesh_b200.camera import make_camera
+
+    cam = make_camera((0.0, -6.0, 0.0), (0.0, -20.0, 0.0), 40.0, 96, 64)  # looking away from the mesh
+    assert np.isfinite(cam.vp).all()
+    r = make_renderer(c1_scene, cam)
+    img = r.forward_tiled(cam.cam_pos, cam.vp, cam.c2w_intrinsics)
+    ref = oracle32.forward_tiled(c1_scene, cam)
+    assert ref["P"] == 0 and r.info().n_pairs_last == 0
+    assert np.all(img == 0.0) and np.all(ref["image"] == 0.0)
+    g = r.backward(np.ones((64, 96, 4), np.float32))
+    assert all(np.all(v == 0.0) for v in g.values())
+    gt = np.full((64, 96, 3), 0.5, np.float32)
+    loss = r.train_step(cam.cam_pos, cam.vp, cam.c2w_intrinsics, gt, 1e-4, 1e-2, 1e-3, 1)
+    assert abs(loss - 3 * 0.25) < 1e-6
+    np.testing.assert_array_equal(r.get_params()["vertices"], c1_scene["vertices"])
+
+
+def test_camera_inside_the_mesh(c1_scene, oracle32):
+    """Tets around the eye have vertices behind the camera (no tiles) and
+    circumspheres containing it (negative depth keys, which sort first)."""
+    from rmesh_b200.camera import make_camera
+
+    cam = make_camera((0.05, -0.1, 0.02), (1.0, 0.3, 0.2), 70.0, 160, 120)
+    r = make_renderer(c1_scene, cam)
+    img = r.forward_tiled(cam.cam_pos, cam.vp, cam.c2w_intrinsics)
+    ref = oracle32.forward_tiled(c1_scene, cam)
+    assert ref["P"] > 0
+    np.testing.assert_array_equal(r.debug_tiles_touched(), np.where(ref["visible"] > 0, ref["tiles_touched"], 0))
+    tiles, tets = r.debug_pairs()
+    np.testing.assert_array_equal(tiles, ref["key_hi"])
+    np.testing.assert_array_equal(tets, ref["vals"])
+    assert np.abs(img - ref["image"]).max() <= 1e-4
+    gt = np.random.default_rng(3).uniform(0, 1, (120, 160, 3)).astype(np.float32)
+    _, dl = oracle32.loss(ref["image"], gt, 1)
+    g = r.backward(dl)
+    go = oracle32.backward(c1_scene, cam, dl, ref)
+    for k in go:
+        assert rel_l2(g[k], go[k]) <= 1e-3, k
+
+
+def test_many_tiles_batched_step(c1_scene, oracle32):
+    """8 views of 1024x1024 (59,168 tiles of 12x12... times 8 = 473k > 2^16):
+    the batched and graph steps' per-view losses equal the oracle's."""
+    from rmesh_b200.camera import orbit_cameras
+
+    cams = orbit_cameras(8, seed=12, radius=(2.6, 3.4), resolutions=((1024, 1024),))
+    rng = np.random.default_rng(9)
+    gts = [rng.uniform(0, 1, (c.height, c.width, 3)).astype(np.float32) for c in cams]
+    want = []
+    for c, g in zip(cams, gts):
+        f = oracle32.forward_tiled(c1_scene, c)
+        want.append(oracle32.loss(f["image"], g, 1)[0])
+    for mode in ("batched", "graph"):
+        r = make_renderer(c1_scene, cams[0])
+        losses = r.train_step_views(cams, gts, 0.0, 0.0, 0.0, 1, mode=mode)
+        np.testing.assert_allclose(losses, want, rtol=1e-4)
+        assert r.info().n_views_last == 8
