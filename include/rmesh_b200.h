@@ -62,7 +62,7 @@ typedef struct {
   const float* circumdata;   /* [4M] */
   int32_t width;             /* default view size */
   int32_t height;
-  int32_t aux_dim;           /* reference aux_dim (only 0 is supported) */
+  int32_t aux_dim;           /* custom per-tet aux channels, 0..RMESH_MAX_AUX_DIM (lib.rs:264-266) */
   int32_t tile_size;         /* 0 -> 12, the reference's hard-coded value (lib.rs:442) */
   int32_t device;            /* CUDA device ordinal, -1 = current */
   int32_t sh_degree;         /* 0..3, used when sh_coeffs is set */
@@ -135,6 +135,13 @@ RMESH_API int rmesh_get_params(RmeshCtx* ctx, float* vertices, float* base_color
 /* getters step/width/height, lib.rs:2688-2705 */
 RMESH_API int rmesh_get_info(RmeshCtx* ctx, RmeshInfo* info);
 
+/* set_aux_data / get_aux_data, lib.rs:892-921: the [M][aux_dim] custom
+ * per-tet channels that forward_tiled's aux output composites after its eight
+ * fixed channels (aux_out [H][W][8 + aux_dim]); zeros until set. */
+#define RMESH_MAX_AUX_DIM 64
+RMESH_API int rmesh_set_aux_data(RmeshCtx* ctx, const float* aux_data);
+RMESH_API int rmesh_get_aux_data(RmeshCtx* ctx, float* aux_data);
+
 /* SH coefficients of a context created with sh_coeffs (no reference
  * counterpart: the reference's binding trains base colours only).  get/update
  * copy [M][3][nc] floats; get_sh_grad returns the coefficient gradient of the
@@ -147,7 +154,7 @@ RMESH_API int rmesh_set_lr_sh(RmeshCtx* ctx, float lr_sh);
 
 /* ---- the path ------------------------------------------------------------- */
 /* forward_tiled, lib.rs:1041-1204: project -> bin -> sort -> ranges -> composite.
- * rgba_out [H][W][4]; aux_out [H][W][8] or NULL (render_aux). */
+ * rgba_out [H][W][4]; aux_out [H][W][8 + aux_dim] or NULL (render_aux). */
 RMESH_API int rmesh_forward_tiled(RmeshCtx* ctx, const RmeshCamera* cam, float* rgba_out, float* aux_out);
 
 /* backward, lib.rs:1894-2031: must follow rmesh_forward_tiled on the same context;

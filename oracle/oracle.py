@@ -75,7 +75,7 @@ class Oracle:
         self._rt = rt
         self._raster.argtypes = [self.rp, _u32p, self.rp, self.rp, self.rp, _u32p, _u32p, self.rp, self.rp,
                                  self.rp, self.rp, ctypes.c_int, ctypes.c_int, ctypes.c_int, rt,
-                                 self.rp, self.rp, _u32p]
+                                 self.rp, self.rp, _u32p, self.rp, ctypes.c_int]
         self._adam.argtypes = [ctypes.c_int64, self.rp, self.rp, self.rp, self.rp, ctypes.c_uint32, rt, rt, rt, rt]
         if threads > 0:
             getattr(L, "orc_set_threads" + s)(int(threads))
@@ -156,20 +156,24 @@ class Oracle:
         self._ranges(ctypes.c_int64(hi_sorted.size), _ptr(self._u(hi_sorted), _u32p), _ptr(ranges, _u32p))
         return ranges
 
-    def rasterize(self, scene, cam, colors, vals, ranges, tile_size=12, min_t=0.0, aux=False, stats=False):
+    def rasterize(self, scene, cam, colors, vals, ranges, tile_size=12, min_t=0.0, aux=False, stats=False,
+                  aux_data=None):
+        """aux_data: optional [M * aux_dim] custom channels composited after the 8 fixed aux ones."""
         vp, c2w, intr, cp, W, H = self._cam(cam)
+        m = scene["indices"].size // 4
+        aux_dim = 0 if aux_data is None else int(np.asarray(aux_data).size // m)
         rgba = np.zeros(H * W * 4, dtype=self.np)
-        auxb = np.zeros(H * W * 8, dtype=self.np) if aux else None
+        auxb = np.zeros(H * W * (8 + aux_dim), dtype=self.np) if aux else None
         st = np.zeros(H * W * 4, dtype=np.uint32) if stats else None
         self._raster(_ptr(self._r(scene["vertices"]), self.rp), _ptr(self._u(scene["indices"]), _u32p),
                      _ptr(self._r(colors), self.rp), _ptr(self._r(scene["densities"]), self.rp),
                      _ptr(self._r(scene["color_grads"]), self.rp), _ptr(self._u(vals), _u32p),
                      _ptr(self._u(ranges), _u32p), _ptr(vp, self.rp), _ptr(c2w, self.rp), _ptr(intr, self.rp),
                      _ptr(cp, self.rp), W, H, tile_size, self._rt(min_t), _ptr(rgba, self.rp), _ptr(auxb, self.rp),
-                     _ptr(st, _u32p))
+                     _ptr(st, _u32p), _ptr(None if aux_data is None else self._r(aux_data), self.rp), aux_dim)
         out = {"image": rgba.reshape(H, W, 4)}
         if aux:
-            out["aux"] = auxb.reshape(H, W, 8)
+            out["aux"] = auxb.reshape(H, W, 8 + aux_dim)
         if stats:
             out["stats"] = st.reshape(H, W, 4)
         return out
@@ -246,7 +250,7 @@ class Oracle:
 
     # ---- host sequencing --------------------------------------------------
     def forward_tiled(self, scene, cam, tile_size=12, min_t=0.0, aux=False, stats=False,
-                      sh=None, sh_degree=0):
+                      sh=None, sh_degree=0, aux_data=None):
         """lib.rs:1041-1204.  Returns the image plus every intermediate buffer.
         sh: coefficient values (see sh_values) selecting the SH colour branch."""
         W, H = int(cam.width), int(cam.height)
@@ -257,7 +261,7 @@ class Oracle:
         lo, hi, vals, emitted = self.emit(scene, cam, visible, tt, tile_size)
         slo, shi, svals = self.sort_pairs(lo, hi, vals, num_tiles)
         ranges = self.tile_ranges(shi, num_tiles)
-        out = self.rasterize(scene, cam, colors, svals, ranges, tile_size, min_t, aux, stats)
+        out = self.rasterize(scene, cam, colors, svals, ranges, tile_size, min_t, aux, stats, aux_data)
         out.update(visible=visible, tiles_touched=tt, colors=colors, key_lo=slo, key_hi=shi, vals=svals,
                    ranges=ranges, P=int(lo.size), emitted=emitted, num_tiles=num_tiles,
                    unsorted=(lo, hi, vals))

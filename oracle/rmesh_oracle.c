@@ -651,7 +651,7 @@ static int intersect(const V3 v[4], const V3 n[4], V3 o, V3 d, R* tmin, R* tmax,
 EXPORT void SFX(orc_rasterize)(const R* verts, const uint32_t* idx, const R* colors, const R* dens,
                                const R* cgrad, const uint32_t* vals, const uint32_t* ranges, const R* vp,
                                const R* c2w, const R* intr, const R* cam3, int W, int H, int TS, R min_t,
-                               R* rgba, R* aux, uint32_t* stats) {
+                               R* rgba, R* aux, uint32_t* stats, const R* aux_data, int aux_dim) {
     Cam cm = {vp, c2w, intr, cam3, W, H, TS, min_t};
     uint32_t tiles_x = (uint32_t)((W + TS - 1) / TS), tiles_y = (uint32_t)((H + TS - 1) / TS);
     int64_t ntiles = (int64_t)tiles_x * tiles_y;
@@ -662,6 +662,7 @@ EXPORT void SFX(orc_rasterize)(const R* verts, const uint32_t* idx, const R* col
         R tile_ox = (R)(tile_x * (uint32_t)TS), tile_oy = (R)(tile_y * (uint32_t)TS);
         int np = TS * TS;
         R col[256][4], nd[256][4], ent[256][4];
+        R* cust = aux_dim > 0 ? (R*)calloc((size_t)256 * aux_dim, sizeof(R)) : NULL;  /* :458-462 */
         uint32_t st[256][4];
         memset(col, 0, sizeof(col)); memset(nd, 0, sizeof(nd)); memset(ent, 0, sizeof(ent)); memset(st, 0, sizeof(st));
         uint32_t rs = ranges[2 * tile], re = ranges[2 * tile + 1];
@@ -730,6 +731,7 @@ EXPORT void SFX(orc_rasterize)(const R* verts, const uint32_t* idx, const R* col
                         ent[pl][1] += wt > (R)1e-20 ? wt * RLOG(wt) : (R)0;
                         ent[pl][2] += wt * cmid;
                         ent[pl][3] += wc > (R)1e-20 ? wc * RLOG(wc) : (R)0;
+                        for (int ai = 0; ai < aux_dim; ++ai) cust[pl * aux_dim + ai] += ta * aux_data[(size_t)t * aux_dim + ai];
                     }
                 }
             }
@@ -742,10 +744,13 @@ EXPORT void SFX(orc_rasterize)(const R* verts, const uint32_t* idx, const R* col
             rgba[4 * p + 0] = col[i][0]; rgba[4 * p + 1] = col[i][1]; rgba[4 * p + 2] = col[i][2];
             rgba[4 * p + 3] = (R)1 - safe_exp(col[i][3]);
             if (aux) {
-                for (int k = 0; k < 4; ++k) { aux[8 * p + k] = nd[i][k]; aux[8 * p + 4 + k] = ent[i][k]; }
+                size_t st_ = (size_t)(8 + aux_dim);
+                for (int k = 0; k < 4; ++k) { aux[st_ * p + k] = nd[i][k]; aux[st_ * p + 4 + k] = ent[i][k]; }
+                for (int ai = 0; ai < aux_dim; ++ai) aux[st_ * p + 8 + ai] = cust[i * aux_dim + ai];
             }
             if (stats) for (int k = 0; k < 4; ++k) stats[4 * p + k] = st[i][k];
         }
+        free(cust);
     }
 }
 

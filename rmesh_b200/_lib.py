@@ -36,7 +36,7 @@ EXPORTED = (
     "rmesh_debug_tiles_touched", "rmesh_debug_pairs", "rmesh_debug_ranges", "rmesh_set_profiling",
     "rmesh_stage_times", "rmesh_accumulate_views", "rmesh_grad_slots", "rmesh_apply_adam",
     "rmesh_count_tiles_static", "rmesh_update_sh", "rmesh_get_sh", "rmesh_get_sh_grad", "rmesh_set_lr_sh",
-    "rmesh_decode_scene", "rmesh_forward_error",
+    "rmesh_decode_scene", "rmesh_forward_error", "rmesh_set_aux_data", "rmesh_get_aux_data",
 )
 
 COUNTERS_BYTES = 792  # sizeof(rm::Counters), read back once per training run
@@ -131,6 +131,8 @@ def load() -> ctypes.CDLL:
         "rmesh_set_lr_sh": ([vp, f32], ctypes.c_int),
         "rmesh_decode_scene": ([P(PackedScene), vp, vp, vp, vp, vp], ctypes.c_int),
         "rmesh_forward_error": ([vp, vp, vp, vp, vp], ctypes.c_int),
+        "rmesh_set_aux_data": ([vp, vp], ctypes.c_int),
+        "rmesh_get_aux_data": ([vp, vp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

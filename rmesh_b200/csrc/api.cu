@@ -87,6 +87,7 @@ struct RmeshCtx {
   int sh_degree = -1;   // -1: base colours; 0..3: colours from SH coefficients
   int sh_nc = 0;        // (sh_degree + 1)^2
   float lr_sh = 0.0f;   // SH learning rate of rmesh_train_step
+  int aux_dim = 0;      // custom per-tet aux channels
   std::string err;
   int num_sms = 148;
 
@@ -95,6 +96,7 @@ struct RmeshCtx {
   DevBuf m_verts, v_verts, m_dens, v_dens, m_cgrad, v_cgrad, m_base, v_base;
   DevBuf rec, color4, grad_slot, csr_off, csr_ref;
   DevBuf sh, m_sh, v_sh;  // SH coefficients [M][3][nc] and their Adam moments
+  DevBuf aux_data;        // [M][aux_dim] custom aux channels
 
   // per-run
   DevBuf views_d, counters_d, hp_d, sort_state, sort_status, scan_status;
@@ -767,7 +769,7 @@ int rmesh_create(const RmeshSceneDesc* d, RmeshCtx** out) {
       !d->color_grads || !d->circumdata)
     return RMESH_ERR_INVALID_ARG;
   if (d->n_tets > (int64_t)(1u << 29) || d->n_vertices > (int64_t)(1u << 30)) return RMESH_ERR_INVALID_ARG;
-  if (d->aux_dim != 0) return RMESH_ERR_INVALID_ARG;
+  if (d->aux_dim < 0 || d->aux_dim > RMESH_MAX_AUX_DIM) return RMESH_ERR_INVALID_ARG;
   if (d->sh_coeffs && (d->sh_degree < 0 || d->sh_degree > 3)) return RMESH_ERR_INVALID_ARG;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -780,6 +782,7 @@ int rmesh_create(const RmeshSceneDesc* d, RmeshCtx** out) {
   c->width = d->width;
   c->height = d->height;
   c->tile_size = d->tile_size > 0 ? d->tile_size : 12;
+  c->aux_dim = d->aux_dim;
   if (d->sh_coeffs) {
     c->sh_degree = d->sh_degree;
     c->sh_nc = (d->sh_degree + 1) * (d->sh_degree + 1);
@@ -823,6 +826,10 @@ int rmesh_create(const RmeshSceneDesc* d, RmeshCtx** out) {
     CKR(ensure_buf(c, c->rec, M * sizeof(TetRec)));
     CKR(ensure_buf(c, c->color4, M * 16));
     CKR(ensure_buf(c, c->grad_slot, grad_floats(c) * 4));
+    if (c->aux_dim > 0) {
+      CKR(ensure_buf(c, c->aux_data, M * (size_t)c->aux_dim * 4));
+      CK(cudaMemsetAsync(c->aux_data.p, 0, M * (size_t)c->aux_dim * 4, c->stream));
+    }
     if (c->sh_degree >= 0) {
       const size_t n_sh = M * 3 * (size_t)c->sh_nc;
       CKR(ensure_buf(c, c->sh, n_sh * 4));
@@ -918,6 +925,21 @@ int rmesh_get_params(RmeshCtx* c, float* v, float* b, float* d, float* g) {
   return RMESH_OK;
 }
 
+int rmesh_set_aux_data(RmeshCtx* c, const float* aux_data) {
+  if (!c || !aux_data) return RMESH_ERR_INVALID_ARG;
+  if (c->aux_dim == 0) return fail(c, RMESH_ERR_INVALID_ARG, "aux_dim is 0; create the context with aux_dim > 0");
+  CKR(copy_in(c, c->aux_data, aux_data, (size_t)c->M * c->aux_dim * 4));
+  return RMESH_OK;
+}
+
+int rmesh_get_aux_data(RmeshCtx* c, float* aux_data) {
+  if (!c || !aux_data) return RMESH_ERR_INVALID_ARG;
+  if (c->aux_dim == 0) return fail(c, RMESH_ERR_INVALID_ARG, "aux_dim is 0; no aux data");
+  CK(cudaMemcpyAsync(aux_data, c->aux_data.p, (size_t)c->M * c->aux_dim * 4, cudaMemcpyDefault, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return RMESH_OK;
+}
+
 int rmesh_set_lr_sh(RmeshCtx* c, float lr) {
   if (!c) return RMESH_ERR_INVALID_ARG;
   c->lr_sh = lr;
@@ -968,7 +990,7 @@ int rmesh_get_info(RmeshCtx* c, RmeshInfo* info) {
                    &c->vis_cnt, &c->vis_proj, &c->vis_view, &c->vis_key_alt, &c->vis_val_alt, &c->tiles_touched, &c->pair_key,
                    &c->pair_val, &c->pair_key_alt, &c->pair_val_alt, &c->ranges, &c->rgba, &c->aux, &c->dl,
                    &c->gt, &c->out_a, &c->out_b, &c->out_c, &c->out_d, &c->sh, &c->m_sh, &c->v_sh,
-                   &c->vis_color, &c->vis_dcolor, &c->vis_index, &c->err_in, &c->err_out};
+                   &c->vis_color, &c->vis_dcolor, &c->vis_index, &c->err_in, &c->err_out, &c->aux_data};
   for (DevBuf* b : all) info->device_bytes += b->bytes;
   return RMESH_OK;
 }
@@ -980,7 +1002,7 @@ int rmesh_forward_tiled(RmeshCtx* c, const RmeshCamera* cam, float* rgba_out, fl
     CKR(fill_view(c, *cam, c->views_h[0], 0, 0));
     const uint32_t tiles = (uint32_t)(c->views_h[0].tiles_x * c->views_h[0].tiles_y);
     CKR(ensure_run_buffers(c, 1, npix, tiles));
-    if (aux_out) CKR(ensure_buf(c, c->aux, npix * 32));
+    if (aux_out) CKR(ensure_buf(c, c->aux, npix * (8 + (uint64_t)c->aux_dim) * 4));
     CKR(upload_views(c, 1));
     Counters* cnt = c->counters_d.as<Counters>();
     CK(cudaMemsetAsync(cnt, 0, sizeof(Counters), c->stream));
@@ -993,6 +1015,8 @@ int rmesh_forward_tiled(RmeshCtx* c, const RmeshCamera* cam, float* rgba_out, fl
       ta.rgba = c->rgba.as<float>();
       if (aux_out) {
         ta.aux = c->aux.as<float>();
+        ta.aux_data = c->aux_data.as<float>();
+        ta.aux_dim = c->aux_dim;
         CKR((launch_tile_m<kModeForward, true>(c, ta, tiles, true)));
       } else {
         CKR((launch_tile_m<kModeForward, false>(c, ta, tiles, true)));
@@ -1002,7 +1026,7 @@ int rmesh_forward_tiled(RmeshCtx* c, const RmeshCamera* cam, float* rgba_out, fl
     if ((c->last_err_bits & kErrPairOverflow) && grow_pairs(c)) continue;
     CKR(status_from_bits(c));
     CK(cudaMemcpyAsync(rgba_out, c->rgba.p, npix * 16, cudaMemcpyDefault, c->stream));
-    if (aux_out) CK(cudaMemcpyAsync(aux_out, c->aux.p, npix * 32, cudaMemcpyDefault, c->stream));
+    if (aux_out) CK(cudaMemcpyAsync(aux_out, c->aux.p, npix * (8 + (uint64_t)c->aux_dim) * 4, cudaMemcpyDefault, c->stream));
     CK(cudaStreamSynchronize(c->stream));
     c->have_forward = true;
     c->last_tiles = tiles;

@@ -64,7 +64,9 @@ struct TileArgs {
   const float4* color4;
   uint32_t color_view_stride;  // 0: colours shared by all views; M: per-view colours
   float* rgba;                 // [pixels][4] (forward output; optional in train mode)
-  float* aux;                  // [pixels][8] (optional, forward only)
+  float* aux;                  // [pixels][8 + aux_dim] (optional, forward only)
+  const float* aux_data;       // [M][aux_dim] per-tet custom channels (aux_dim > 0)
+  int aux_dim;
   const float* dl_rgba;        // [pixels][4] (backward mode)
   const float* gt_rgb;         // [pixels][3] (train mode)
   const float* pixel_err;      // [pixels] (error mode)
@@ -467,6 +469,13 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
     // =============== forward (front to back) ===============
     if (MODE == kModeForward || MODE == kModeTrain) {
       bool alive = valid;
+      // custom aux channels accumulate in place in the output row of the pixel
+      // (rasterize_compute.wgsl:458-462), so they start at zero
+      float* aux_px = nullptr;
+      if (AUX && a.aux && a.aux_dim > 0 && valid) {
+        aux_px = a.aux + pix * (size_t)(8 + a.aux_dim) + 8;
+        for (int ai = 0; ai < a.aux_dim; ++ai) aux_px[ai] = 0.0f;
+      }
       if (re > rs) {
         {
           const int nb0 = (int)min((uint32_t)kBatch, re - rs);
@@ -541,6 +550,10 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
                     en1 += wt > 1e-20f ? wt * logf(wt) : 0.0f;
                     en2 += wt * cmid;
                     en3 += wc > 1e-20f ? wc * logf(wc) : 0.0f;
+                    if (aux_px) {
+                      const float* ad = a.aux_data + (size_t)s.view[buf][k].meta.x * a.aux_dim;
+                      for (int ai = 0; ai < a.aux_dim; ++ai) aux_px[ai] += ta * ad[ai];
+                    }
                   }
                 }
               }
@@ -560,9 +573,13 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
       if (valid && (MODE == kModeForward || a.rgba != nullptr)) {
         const float A = 1.0f - safe_exp(logT);
         reinterpret_cast<float4*>(a.rgba)[pix] = make_float4(Cr, Cg, Cb, A);
-        if (AUX && a.aux) {
+        if (AUX && a.aux && a.aux_dim == 0) {
           reinterpret_cast<float4*>(a.aux)[2 * pix] = make_float4(nd0, nd1, nd2, nd3);
           reinterpret_cast<float4*>(a.aux)[2 * pix + 1] = make_float4(en0, en1, en2, en3);
+        } else if (AUX && a.aux) {  // [normal.xyz, depth, entropy.4, custom...] (:486-500)
+          float* o = a.aux + pix * (size_t)(8 + a.aux_dim);
+          o[0] = nd0; o[1] = nd1; o[2] = nd2; o[3] = nd3;
+          o[4] = en0; o[5] = en1; o[6] = en2; o[7] = en3;
         }
       }
     }

@@ -101,8 +101,9 @@ class RMeshRenderer:
         the binding) switches the colours from ``base_colors`` to the reference
         shader's view-dependent SH colour (project_compute.wgsl:264-318)."""
         self._lib = _lib.load()
-        if int(aux_dim) != 0:
-            raise ValueError("aux_dim > 0 is not supported by this build")
+        if not 0 <= int(aux_dim) <= 64:
+            raise ValueError("aux_dim must be 0..64")
+        self._aux_dim = int(aux_dim)
         keep = []
         ptrs = {}
         for name, arr, dt in (("vertices", vertices, np.float32), ("indices", indices, np.uint32),
@@ -140,7 +141,7 @@ class RMeshRenderer:
         d.vertices, d.indices = ptrs["vertices"][1], ptrs["indices"][1]
         d.base_colors, d.densities = ptrs["base_colors"][1], ptrs["densities"][1]
         d.color_grads, d.circumdata = ptrs["color_grads"][1], ptrs["circumdata"][1]
-        d.width, d.height, d.aux_dim, d.tile_size = int(width), int(height), 0, int(tile_size)
+        d.width, d.height, d.aux_dim, d.tile_size = int(width), int(height), self._aux_dim, int(tile_size)
         d.device = -1 if device is None else int(device)
         ctx = ctypes.c_void_p()
         rc = self._lib.rmesh_create(ctypes.byref(d), ctypes.byref(ctx))
@@ -255,11 +256,28 @@ class RMeshRenderer:
         return out
 
     # -------------------------------------------------------------- the path
+    def set_aux_data(self, aux_data):
+        """Per-tet custom aux channels [M * aux_dim] (lib.rs:892-910)."""
+        if self._aux_dim == 0:
+            raise ValueError("aux_dim is 0; construct with aux_dim > 0 to use custom aux channels")
+        obj, p = _as_array(aux_data, np.float32, "aux_data")
+        if _numel(obj) != self._M * self._aux_dim:
+            raise ValueError(f"Expected {self._M * self._aux_dim} elements (tet_count={self._M} * "
+                             f"aux_dim={self._aux_dim}), got {_numel(obj)}")
+        self._check(self._lib.rmesh_set_aux_data(self._ctx, p))
+
+    def get_aux_data(self) -> np.ndarray:
+        if self._aux_dim == 0:
+            raise ValueError("aux_dim is 0; no aux data to read")
+        out = np.empty(self._M * self._aux_dim, np.float32)
+        self._check(self._lib.rmesh_get_aux_data(self._ctx, out.ctypes.data))
+        return out
+
     def forward_tiled(self, cam_pos, vp, c2w_intrinsics, render_aux: bool = False):
-        """[H, W, 4] premultiplied RGBA (and [H, W, 8] aux when ``render_aux``)."""
+        """[H, W, 4] premultiplied RGBA (and [H, W, 8 + aux_dim] aux when ``render_aux``)."""
         cam = self._cam(cam_pos, vp, c2w_intrinsics)
         rgba = np.empty((self._height, self._width, 4), np.float32)
-        aux = np.empty((self._height, self._width, 8), np.float32) if render_aux else None
+        aux = np.empty((self._height, self._width, 8 + self._aux_dim), np.float32) if render_aux else None
         self._check(self._lib.rmesh_forward_tiled(self._ctx, ctypes.byref(cam), rgba.ctypes.data,
                                                   aux.ctypes.data if render_aux else None))
         return (rgba, aux) if render_aux else rgba

@@ -122,7 +122,7 @@ def test_renderer_validates_before_device_use():
                       sc["color_grads"], sc["circumdata"], 64, 64)
     with pytest.raises(ValueError):
         RMeshRenderer(sc["vertices"], sc["indices"], sc["base_colors"], sc["densities"], sc["color_grads"],
-                      sc["circumdata"], 64, 64, aux_dim=2)
+                      sc["circumdata"], 64, 64, aux_dim=65)
 
 
 def test_library_is_built_for_sm100a():

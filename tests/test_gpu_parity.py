@@ -67,6 +67,29 @@ def test_c1_forward_aux(c1_scene, oracle32):
     assert np.abs(aux - ref["aux"]).max() <= 1e-3
 
 
+def test_custom_aux_channels(c1_scene, oracle32):
+    """aux_dim > 0 (lib.rs:264-266, 892-921; rasterize_compute.wgsl:458-500):
+    per-tet channels composited with weight T * alpha after the eight fixed ones."""
+    from rmesh_b200 import RMeshRenderer
+
+    cam = c1_camera(160, 128)
+    sc = c1_scene
+    m = sc["densities"].size
+    ad = np.random.default_rng(6).uniform(-1, 1, 3 * m).astype(np.float32)
+    r = RMeshRenderer(sc["vertices"], sc["indices"], sc["base_colors"], sc["densities"], sc["color_grads"],
+                      sc["circumdata"], cam.width, cam.height, aux_dim=3)
+    np.testing.assert_array_equal(r.get_aux_data(), np.zeros(3 * m, np.float32))
+    r.set_aux_data(ad)
+    np.testing.assert_array_equal(r.get_aux_data(), ad)
+    img, aux = r.forward_tiled(cam.cam_pos, cam.vp, cam.c2w_intrinsics, render_aux=True)
+    ref = oracle32.forward_tiled(sc, cam, aux=True, aux_data=ad)
+    assert aux.shape == (128, 160, 11)
+    assert np.abs(img - ref["image"]).max() <= IMG_TOL
+    assert np.abs(aux[..., :8] - ref["aux"][..., :8]).max() <= 1e-3
+    assert np.abs(aux[..., 8:] - ref["aux"][..., 8:]).max() <= IMG_TOL
+    assert np.abs(ref["aux"][..., 8:]).max() > 0.1
+
+
 def test_c1_backward_parity(c1_scene, oracle32):
     cam = c1_camera(256, 256)
     r = make_renderer(c1_scene, cam)
