@@ -443,3 +443,50 @@ def test_sh_fd_gradients(oracle64):
             checked += 1
     assert checked >= 100
     assert len(fails) <= 2, fails  # a vertex step may cross a pixel-coverage edge
+
+
+def test_c2_fd_gradients_200_per_group(oracle64):
+    """The 10,000-point degree-3 configuration's gradient check: central finite
+    differences in float64, step 1e-4, on 200 sampled parameters per group
+    (SH coefficients, colour gradients, densities, vertices), against the
+    adjoint (tile walk + SH colour adjoint).  Parameters are drawn among those
+    with a non-zero gradient so each sample tests something; SH values are the
+    f16-rounded ones the renderer reads, perturbed in float64."""
+    from rmesh_b200.scenes import scene_for_config
+
+    sc = {k: (np.asarray(v, np.float64) if isinstance(v, np.ndarray) and v.dtype.kind == "f" else v)
+          for k, v in scene_for_config("c2").items()}
+    deg = sc["sh_degree"]
+    cam = _cam((1.2, -2.5, 1.1), (0, 0, 0), 50.0, 64, 64)
+    gt = np.random.default_rng(8).uniform(0, 1, (64, 64, 3))
+    sh = oracle64.sh_values(sc["sh_coeffs"]).astype(np.float64)
+
+    def loss_of(scene, shv):
+        f = oracle64.forward_tiled(scene, cam, sh=shv, sh_degree=deg)
+        return oracle64.loss(f["image"], gt, 1)[0]
+
+    f = oracle64.forward_tiled(sc, cam, sh=sh, sh_degree=deg)
+    _, dl = oracle64.loss(f["image"], gt, 1)
+    g = oracle64.backward(sc, cam, dl, f, sh=sh, sh_degree=deg, threads=0)
+    rng = np.random.default_rng(13)
+    eps = 1e-4
+    # per sample: relative error <= tol or absolute <= 1e-8; the loss has kinks
+    # (ReLU'd segment colours, pixel coverage for vertices) where a central
+    # difference straddles a non-smooth point, so a few samples may miss
+    for key, gkey, tol, min_pass in (("sh", "d_sh", 1e-3, 0.97), ("color_grads", "d_color_grads", 1e-3, 0.97),
+                                     ("densities", "d_densities", 1e-3, 0.95), ("vertices", "d_vertices", 1e-2, 0.9)):
+        arr = sh if key == "sh" else sc[key]
+        cand = np.nonzero(np.abs(g[gkey]) > 1e-7)[0]
+        idx = rng.choice(cand, size=min(200, cand.size), replace=False)
+        num = np.empty(idx.size)
+        for j, i in enumerate(idx):
+            vals = []
+            for sgn in (+1, -1):
+                a2 = arr.copy()
+                a2[i] += sgn * eps
+                vals.append(loss_of(sc, a2) if key == "sh" else loss_of({**sc, key: a2}, sh))
+            num[j] = (vals[0] - vals[1]) / (2 * eps)
+        ana = g[gkey][idx]
+        err = np.abs(ana - num)
+        ok = (err <= tol * np.maximum(np.abs(ana), np.abs(num))) | (err <= 1e-8)
+        assert idx.size >= 100 and ok.mean() >= min_pass, (key, ok.mean(), float(np.median(err / np.abs(num))))
