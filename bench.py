@@ -64,12 +64,17 @@ def peaks():
         return 6650.0, "fallback"
 
 
-def build_workload(points: int, seed: int, rank: int, n_views: int = N_VIEWS, res=RES, sh_degree: int = 3):
+def build_workload(points: int, seed: int, rank: int, n_views: int = N_VIEWS, res=RES, sh_degree: int = 3,
+                   cloud: str = "gmm"):
     from rmesh_b200.camera import orbit_cameras
-    from rmesh_b200.scenes import gmm_cloud, make_scene
+    from rmesh_b200.scenes import gmm_cloud, make_scene, shell_cloud, uniform_cloud
 
     rng = np.random.default_rng(seed)
-    scene = make_scene(gmm_cloud(points, rng), rng, sh_degree=max(sh_degree, 0))
+    if cloud == "gmm":
+        pts = gmm_cloud(points, rng)
+    else:  # uniform in [-1,1]^3 plus 10 % jittered near a random sphere shell
+        pts = np.concatenate([uniform_cloud(points, rng), shell_cloud(points // 10, rng)], axis=0)
+    scene = make_scene(pts, rng, sh_degree=max(sh_degree, 0))
     cams = orbit_cameras(n_views, seed=seed + 1 + 1000 * rank, radius=(2.5, 4.0), resolutions=res)
     trng = np.random.default_rng(seed + 2 + 1000 * rank)
     gts = [trng.uniform(0, 1, (c.height, c.width, 3)).astype(np.float32) for c in cams]
@@ -148,7 +153,7 @@ def run_gpu(args):
     from rmesh_b200 import RMeshRenderer
     from rmesh_b200 import _lib
 
-    scene, cams, gts = build_workload(args.points, args.seed, rank, args.views, args.res, args.sh_degree)
+    scene, cams, gts = build_workload(args.points, args.seed, rank, args.views, args.res, args.sh_degree, args.cloud)
     sh_kw = dict(sh_coeffs=scene["sh_coeffs"], sh_degree=args.sh_degree) if args.sh_degree >= 0 else {}
     lr_sh = LR_SH if args.sh_degree >= 0 else 0.0
     r = RMeshRenderer(scene["vertices"], scene["indices"], scene["base_colors"], scene["densities"],
@@ -221,7 +226,7 @@ def run_gpu(args):
 
     steps_per_s = world * 1000.0 / ms_graph
     out = {
-        "metric": "fwd+bwd train-steps/s (16 mixed-resolution views, batched graph-captured step)",
+        "metric": metric_name(args),
         "value": round(steps_per_s, 4),
         "unit": "train-steps/s",
         "n_gpus": world,
@@ -232,7 +237,7 @@ def run_gpu(args):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f32",
-        "data": "synthetic (seeded GMM Delaunay mesh, seeded targets)",
+        "data": "synthetic (seeded Delaunay mesh, seeded targets)",
         "config": workload_config(args, r.n_tets, r.n_vertices, n_pix, world),
         "mpix_per_s": round(world * n_pix / (ms_graph * 1e-3) / 1e6, 2),
         "plain": {"value": round(world * 1000.0 / ms_plain, 4), "unit": "train-steps/s", "ms_per_step": round(ms_plain, 4)},
@@ -241,6 +246,7 @@ def run_gpu(args):
                 "h2d_bytes_per_step": int(n_pix * 12 + args.views * 160 + 48),
                 "d2h_bytes_per_step": int(_lib.COUNTERS_BYTES)},
         "gpu_launches": int(total_launches),
+        "device_memory_gb": round(int(info.device_bytes) / 1e9, 2),
         "stage_ms_per_step": {k: round(v / nsteps_prof, 4) for k, v in stage_ms.items()},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
@@ -261,10 +267,17 @@ def run_gpu(args):
         dist.destroy_process_group()
 
 
+def metric_name(args) -> str:
+    return (f"fwd+bwd train-steps/s ({args.views} views, batched graph-captured step)" if args.workload == "large"
+            else "fwd+bwd train-steps/s (16 mixed-resolution views, batched graph-captured step)")
+
+
 def workload_config(args, n_tets, n_vertices, n_pix, world):
     """The config object of the JSON line (both arms)."""
+    mesh = ("8-component GMM" if args.cloud == "gmm" else
+            f"uniform [-1,1]^3 + {args.points // 10}-point sphere-shell")
     return {
-        "workload": f"batched: {args.points}-point 8-component GMM Delaunay mesh ({n_tets} tets), "
+        "workload": f"{args.workload}: {args.points}-point {mesh} Delaunay mesh ({n_tets} tets), "
                     f"{args.views} views from {{{res_text(args.res)}}}, L2 loss, Adam",
         "n_tets": n_tets, "n_vertices": n_vertices, "views_per_gpu": args.views,
         "pixels_per_step_per_gpu": n_pix, "tile_size": args.tile_size,
@@ -319,7 +332,7 @@ def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    scene, cams, gts = build_workload(args.points, args.seed, 0, args.views, args.res, args.sh_degree)
+    scene, cams, gts = build_workload(args.points, args.seed, 0, args.views, args.res, args.sh_degree, args.cloud)
     n_pix = sum(c.width * c.height for c in cams)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import Oracle
@@ -347,10 +360,10 @@ def run_reference(args):
     sample = (f"one {cam.width}x{cam.height} view per step ({cam.width * cam.height} px), scaled by pixels to the "
               f"{n_pix}-px {args.views}-view step; C port of the reference kernels, OpenMP {threads} threads")
     print(json.dumps({
-        "impl": "reference", "metric": "fwd+bwd train-steps/s (16 mixed-resolution views, batched graph-captured step)",
+        "impl": "reference", "metric": metric_name(args),
         "value": v, "unit": "train-steps/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(t_step * 1e3, 3), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded GMM Delaunay mesh, seeded targets)",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Delaunay mesh, seeded targets)",
         "config": workload_config(args, scene["indices"].size // 4, scene["vertices"].size // 3, n_pix,
                                   int(os.environ.get("WORLD_SIZE", "1"))),
         "cpu_baseline": {"value": v, "unit": "train-steps/s", "cores": threads, "kind": "port", "sample": sample},
@@ -365,17 +378,28 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--points", type=int, default=100_000)
+    ap.add_argument("--workload", default="batched", choices=["batched", "large"],
+                    help="batched: 100k-point GMM mesh, 16 mixed views (default); large: 1M-point mesh, 8 views 1080p")
+    ap.add_argument("--points", type=int, default=None)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--tile-size", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--views", type=int, default=N_VIEWS, help="views per step (default: the 16-view workload)")
+    ap.add_argument("--views", type=int, default=None, help="views per step (default: the workload's)")
     ap.add_argument("--sh-degree", type=int, default=3, choices=[-1, 0, 1, 2, 3],
                     help="SH degree of the colours (-1: base colours)")
     ap.add_argument("--res", default=None,
                     help="comma-separated WxH choices for the views (default 256x256,512x512,800x600,1024x1024); "
                          "smaller cases serve profiler captures")
     args = ap.parse_args()
+    if args.workload == "large":  # memory-bound configuration: 1M uniform + 10 % shell points, 8 HD views
+        args.points = 1_000_000 if args.points is None else args.points
+        args.views = 8 if args.views is None else args.views
+        args.res = args.res or "1920x1080"
+        args.cloud = "uniform+shell"
+    else:
+        args.points = 100_000 if args.points is None else args.points
+        args.views = N_VIEWS if args.views is None else args.views
+        args.cloud = "gmm"
     args.res = RES if args.res is None else tuple(tuple(int(v) for v in x.split("x")) for x in args.res.split(","))
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
