@@ -854,9 +854,12 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
             const uint32_t n_valid = n_items;
             for (uint32_t chunk = (uint32_t)warp * 32u; chunk < n_items; chunk += (uint32_t)NT) {
               const uint32_t i = chunk + (uint32_t)lane;
-              float m[kMom];
+              float m[8];  // density, base colour, sum(sb), d * d(dc/dt)
 #pragma unroll
-              for (int q = 0; q < kMom; ++q) m[q] = 0.0f;
+              for (int q = 0; q < 8; ++q) m[q] = 0.0f;
+              // the two faces the ray crosses: (face, s, s t d) for entry and exit
+              int fs0 = 0, fs1 = 0;
+              float sv0 = 0.f, px0 = 0.f, py0 = 0.f, pz0 = 0.f, sv1 = 0.f, px1 = 0.f, py1 = 0.f, pz1 = 0.f;
               int k = -1;
               if (i < n_valid) {
                 const float4 st = s.item[i];
@@ -921,15 +924,8 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
                     const float inv_den = fabsf(den) < kTiny ? clipf(1.0f / kTiny, kMinVal, kMaxVal)
                                                              : clipf(__fdividef(1.0f, den), kMinVal, kMaxVal);
                     const float sv = dt * inv_den, st_ = sv * tt;
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                      if (q == f) {
-                        m[8 + 4 * q] += sv;
-                        m[9 + 4 * q] += st_ * d.x;
-                        m[10 + 4 * q] += st_ * d.y;
-                        m[11 + 4 * q] += st_ * d.z;
-                      }
-                    }
+                    if (side == 0) { fs0 = f; sv0 = sv; px0 = st_ * d.x; py0 = st_ * d.y; pz0 = st_ * d.z; }
+                    else { fs1 = f; sv1 = sv; px1 = st_ * d.x; py1 = st_ * d.y; pz1 = st_ * d.z; }
                   }
                 }
               }
@@ -944,8 +940,28 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
               const int wr1 = min(wr0 + 16, n_rows);
 #pragma unroll
               for (int hm = 0; hm < 2; ++hm) {
+                // row layout: half 0 = m[0..7] + face 0's (S, P); half 1 = faces 1..3,
+                // the two crossed faces placed by index (they differ unless both are
+                // face 0, which half 0 sums)
+                if (hm == 0) {
 #pragma unroll
-                for (int q = 0; q < kMomHalf; ++q) red[lane][q] = m[hm * kMomHalf + q];
+                  for (int q = 0; q < 8; ++q) red[lane][q] = m[q];
+                  red[lane][8] = (fs0 == 0 ? sv0 : 0.f) + (fs1 == 0 ? sv1 : 0.f);
+                  red[lane][9] = (fs0 == 0 ? px0 : 0.f) + (fs1 == 0 ? px1 : 0.f);
+                  red[lane][10] = (fs0 == 0 ? py0 : 0.f) + (fs1 == 0 ? py1 : 0.f);
+                  red[lane][11] = (fs0 == 0 ? pz0 : 0.f) + (fs1 == 0 ? pz1 : 0.f);
+                } else {
+#pragma unroll
+                  for (int q = 0; q < kMomHalf; ++q) red[lane][q] = 0.0f;
+                  if (fs0 > 0) {
+                    float* r4 = &red[lane][4 * (fs0 - 1)];
+                    r4[0] = sv0; r4[1] = px0; r4[2] = py0; r4[3] = pz0;
+                  }
+                  if (fs1 > 0) {
+                    float* r4 = &red[lane][4 * (fs1 - 1)];
+                    r4[0] = sv1; r4[1] = px1; r4[2] = py1; r4[3] = pz1;
+                  }
+                }
                 red[lane][kMomHalf] = __int_as_float(k);
                 __syncwarp();
                 if (wq < kMomHalf && wr0 < wr1) {
