@@ -260,6 +260,12 @@ RMESH_API int rmesh_debug_pairs(RmeshCtx* ctx, uint32_t* tile_ids, uint32_t* tet
 /* [start, end) per tile of the last forward ([2 * tiles]). */
 RMESH_API int rmesh_debug_ranges(RmeshCtx* ctx, uint32_t* ranges, uint64_t n_tiles);
 
+/* No reference counterpart: runs the path's two bounded waits (chained-scan
+ * look-back, TMA mbarrier) on conditions that never resolve and returns, in
+ * bits_out[0..1], the error bits each wait recorded after giving up (2 =
+ * RMESH spin timeout).  The device stays usable; used by the failure tests. */
+RMESH_API int rmesh_debug_timeouts(uint32_t* bits_out);
+
 /* ---- profiling -------------------------------------------------------------- */
 /* When enabled, CUDA events bracket each stage on the context stream; the
  * accumulated milliseconds are returned by rmesh_stage_times in the order

@@ -754,6 +754,22 @@ int build_csr(RmeshCtx* c) {
 
 }  // namespace
 
+// Exercises the two bounded waits of the path on conditions that never
+// resolve: a chained-scan look-back whose predecessor never publishes
+// (status[0] stays 0) and an mbarrier phase that never completes.  Each wait
+// gives up after its limit and records kErrSpinTimeout in bits[0] / bits[1];
+// the kernel then returns normally.
+__global__ void timeout_probe_kernel(unsigned long long* status, uint32_t* bits) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x < 32) chained_lookback(status, 1u, 1ull, &bits[0]);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0 && !mbar_wait_bounded(&bar, 0u, 1u << 16)) atomicOr(&bits[1], kErrSpinTimeout);
+}
+
 // ===================================================================== C ABI
 extern "C" {
 
@@ -1197,6 +1213,28 @@ int rmesh_debug_ranges(RmeshCtx* c, uint32_t* ranges, uint64_t n_tiles) {
   CK(cudaMemcpyAsync(ranges, c->ranges.p, k * 8, cudaMemcpyDefault, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return RMESH_OK;
+}
+
+int rmesh_debug_timeouts(uint32_t* bits_out) {
+  if (!bits_out) return RMESH_ERR_INVALID_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return RMESH_ERR_NO_DEVICE;
+  }
+  void* buf = nullptr;
+  if (cudaMalloc(&buf, 64) != cudaSuccess) return RMESH_ERR_OOM;
+  int rc = RMESH_OK;
+  if (cudaMemset(buf, 0, 64) != cudaSuccess) rc = RMESH_ERR_CUDA;
+  if (rc == RMESH_OK) {
+    timeout_probe_kernel<<<1, 64>>>(reinterpret_cast<unsigned long long*>(buf),
+                                    reinterpret_cast<uint32_t*>(static_cast<char*>(buf) + 32));
+    if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
+        cudaMemcpy(bits_out, static_cast<char*>(buf) + 32, 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+      rc = RMESH_ERR_CUDA;
+  }
+  cudaFree(buf);
+  return rc;
 }
 
 int rmesh_set_profiling(RmeshCtx* c, int32_t on) {
