@@ -166,6 +166,10 @@ def run_gpu(args):
     gt_dev = gt_host.to(f"cuda:{local}")
     torch.cuda.synchronize()
 
+    # tile size (and with it threads per tile and the pair-key width) picked by
+    # timing the step's forward + adjoint at 8, 12 and 16 (parameters unchanged)
+    tune_ms = None if args.no_autotune else r.autotune(cams, gt_dev, loss_type=1)
+    tile_size = int(r.info().tile_size)
     slots = r.grad_slots() if world > 1 else None
 
     def step(mode, gt):
@@ -238,7 +242,8 @@ def run_gpu(args):
         "vs_baseline": None,
         "dtype": "f32",
         "data": "synthetic (seeded Delaunay mesh, seeded targets)",
-        "config": workload_config(args, r.n_tets, r.n_vertices, n_pix, world),
+        "config": {**workload_config(args, r.n_tets, r.n_vertices, n_pix, world), "tile_size": tile_size,
+                   "autotune_ms_per_run": None if tune_ms is None else {str(k): round(v, 2) for k, v in tune_ms.items()}},
         "mpix_per_s": round(world * n_pix / (ms_graph * 1e-3) / 1e6, 2),
         "plain": {"value": round(world * 1000.0 / ms_plain, 4), "unit": "train-steps/s", "ms_per_step": round(ms_plain, 4)},
         "batched_graph_vs_plain": round(ms_plain / ms_graph, 3),
@@ -251,7 +256,7 @@ def run_gpu(args):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
                      "traffic": int(TILE_DRAM_BYTES_PER_PAIR * int(info.n_pairs_last)),
-                     "kernel": "tile_kernel<12,kModeTrain> (fused forward+loss+adjoint)",
+                     "kernel": f"tile_kernel<{tile_size},kModeTrain> (fused forward+loss+adjoint)",
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                      "fallback 6.65 TB/s", "launch_ms": round(comp_ms, 4), "algorithmic_bytes": alg,
                      "n_pairs": int(info.n_pairs_last)},
@@ -384,6 +389,7 @@ def main():
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--tile-size", type=int, default=12)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep --tile-size instead of timing 8/12/16")
     ap.add_argument("--views", type=int, default=None, help="views per step (default: the workload's)")
     ap.add_argument("--sh-degree", type=int, default=3, choices=[-1, 0, 1, 2, 3],
                     help="SH degree of the colours (-1: base colours)")

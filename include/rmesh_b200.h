@@ -196,6 +196,15 @@ RMESH_API int rmesh_train_step_views(RmeshCtx* ctx, const RmeshCamera* cams, int
 RMESH_API int rmesh_accumulate_views(RmeshCtx* ctx, const RmeshCamera* cams, int32_t n_views, const float* gt_rgb,
                                      const RmeshTrainOpts* opts, float* loss_out);
 RMESH_API int rmesh_grad_slots(RmeshCtx* ctx, float** device_ptr, uint64_t* n_floats);
+
+/* Tile-size autotuner (no reference counterpart; the reference fixes 12):
+ * times the batched forward + loss + adjoint of these views (no Adam, so the
+ * parameters are unchanged) at tile sizes 8, 12 and 16 -- which also sets the
+ * threads per tile (64, 160, 256) and the pair-sort key width -- keeps the
+ * fastest and returns it in *tile_size_out; ms_out (optional, [3]) receives
+ * the milliseconds per run of each size. */
+RMESH_API int rmesh_autotune_tile_size(RmeshCtx* ctx, const RmeshCamera* cams, int32_t n_views, const float* gt_rgb,
+                                       const RmeshTrainOpts* opts, int32_t* tile_size_out, float* ms_out);
 RMESH_API int rmesh_apply_adam(RmeshCtx* ctx, const RmeshTrainOpts* opts);
 
 /* ---- .rmesh scene decode -------------------------------------------------------

@@ -37,7 +37,7 @@ EXPORTED = (
     "rmesh_stage_times", "rmesh_accumulate_views", "rmesh_grad_slots", "rmesh_apply_adam",
     "rmesh_count_tiles_static", "rmesh_update_sh", "rmesh_get_sh", "rmesh_get_sh_grad", "rmesh_set_lr_sh",
     "rmesh_decode_scene", "rmesh_forward_error", "rmesh_set_aux_data", "rmesh_get_aux_data",
-    "rmesh_debug_timeouts",
+    "rmesh_debug_timeouts", "rmesh_autotune_tile_size",
 )
 
 COUNTERS_BYTES = 792  # sizeof(rm::Counters), read back once per training run
@@ -135,6 +135,7 @@ def load() -> ctypes.CDLL:
         "rmesh_set_aux_data": ([vp, vp], ctypes.c_int),
         "rmesh_get_aux_data": ([vp, vp], ctypes.c_int),
         "rmesh_debug_timeouts": ([vp], ctypes.c_int),
+        "rmesh_autotune_tile_size": ([vp, P(Camera), i32, vp, P(TrainOpts), P(i32), vp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -1150,6 +1150,49 @@ int rmesh_accumulate_views(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views
   return train_views(c, cams, n_views, gt, opts, loss_out, false);
 }
 
+int rmesh_autotune_tile_size(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views, const float* gt,
+                             const RmeshTrainOpts* opts, int32_t* tile_size_out, float* ms_out) {
+  if (!c || !opts || !tile_size_out) return RMESH_ERR_INVALID_ARG;
+  RmeshTrainOpts o = *opts;
+  o.mode = RMESH_MODE_BATCHED;
+  const int sizes[3] = {8, 12, 16};
+  float best_ms = 0.f;
+  int best = c->tile_size;
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  int rc = RMESH_OK;
+  for (int i = 0; i < 3 && rc == RMESH_OK; ++i) {
+    c->tile_size = sizes[i];
+    c->have_forward = false;
+    // a warm-up run sizes the buffers; then two timed runs (no Adam: the
+    // parameters are left as they were, the gradient slots hold the last run)
+    rc = train_views(c, cams, n_views, gt, &o, nullptr, false);
+    if (rc != RMESH_OK) break;
+    float ms = 0.f;
+    if (cudaEventRecord(e0, c->stream) != cudaSuccess) { rc = RMESH_ERR_CUDA; break; }
+    for (int r = 0; r < 2 && rc == RMESH_OK; ++r) rc = train_views(c, cams, n_views, gt, &o, nullptr, false);
+    if (rc != RMESH_OK) break;
+    if (cudaEventRecord(e1, c->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
+        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
+      rc = RMESH_ERR_CUDA;
+      break;
+    }
+    ms *= 0.5f;
+    if (ms_out) ms_out[i] = ms;
+    if (i == 0 || ms < best_ms) {
+      best_ms = ms;
+      best = sizes[i];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->tile_size = best;
+  c->have_forward = false;
+  *tile_size_out = best;
+  return rc;
+}
+
 int rmesh_grad_slots(RmeshCtx* c, float** ptr, uint64_t* n_floats) {
   if (!c || !ptr || !n_floats) return RMESH_ERR_INVALID_ARG;
   *ptr = c->grad_slot.as<float>();

@@ -384,6 +384,18 @@ class RMeshRenderer:
         self._check(self._lib.rmesh_accumulate_views(self._ctx, cams, n, p, ctypes.byref(o), losses.ctypes.data))
         return losses
 
+    def autotune(self, cameras: Sequence, gt_images, loss_type: int = 1) -> dict:
+        """Times the batched forward + loss + adjoint of ``cameras`` at tile
+        sizes 8, 12 and 16 (parameters unchanged), keeps the fastest and
+        returns {tile_size: ms per run}."""
+        n, cams, keep, p, o = self._views_args(cameras, gt_images, 0.0, 0.0, 0.0, loss_type, 0.0, "batched")
+        best = ctypes.c_int32(0)
+        ms = np.zeros(3, np.float32)
+        self._check(self._lib.rmesh_autotune_tile_size(self._ctx, cams, n, p, ctypes.byref(o), ctypes.byref(best),
+                                                       ms.ctypes.data))
+        self._tile_size = int(best.value)
+        return {8: float(ms[0]), 12: float(ms[1]), 16: float(ms[2])}
+
     def grad_slots(self):
         """The device gradient buffer as a flat torch CUDA tensor view: [M, 20]
         slots (density, base rgb, colour-gradient xyz, 4 x vertex xyz, pad), then,

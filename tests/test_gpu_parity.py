@@ -168,6 +168,24 @@ def test_tile_size_invariance(c1_scene, oracle32, ts):
     assert np.abs(img - ref12["image"]).max() <= 1e-3
 
 
+def test_autotune_keeps_parameters(c1_scene):
+    from rmesh_b200.camera import orbit_cameras
+
+    cams = orbit_cameras(3, seed=21, radius=(2.5, 3.5), resolutions=((128, 128),))
+    gts = [np.random.default_rng(i).uniform(0, 1, (128, 128, 3)).astype(np.float32) for i in range(3)]
+    r = make_renderer(c1_scene, cams[0])
+    before = r.get_params()
+    ms = r.autotune(cams, gts)
+    assert set(ms) == {8, 12, 16} and all(v > 0 for v in ms.values())
+    ts = r.info().tile_size
+    assert ms[ts] == min(ms.values())
+    after = r.get_params()
+    for k in before:
+        np.testing.assert_array_equal(before[k], after[k])
+    losses = r.train_step_views(cams, gts, 1e-4, 1e-2, 1e-3, 1, mode="graph")
+    assert np.all(np.isfinite(losses)) and r.step == 1
+
+
 def test_split_step_equals_train_step(c1_scene):
     """accumulate_views + apply_adam (the data-parallel split) == train_step_views."""
     from rmesh_b200.camera import orbit_cameras
