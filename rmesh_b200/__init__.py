@@ -7,8 +7,9 @@ Adam, as hand-written sm_100a CUDA behind the C ABI in include/rmesh_b200.h.
 ``RMeshModule`` mirror its torch autograd wrapper.
 """
 from .renderer import RMeshError, RMeshRenderer
+from .staging import TargetStager
 
-__all__ = ["RMeshRenderer", "RMeshError", "RMeshForward", "RMeshModule"]
+__all__ = ["RMeshRenderer", "RMeshError", "RMeshForward", "RMeshModule", "TargetStager"]
 
 
 def __getattr__(name):

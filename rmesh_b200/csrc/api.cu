@@ -123,10 +123,21 @@ struct RmeshCtx {
   uint64_t last_n_vis = 0, last_n_pairs = 0;
   int last_cnt = 1;  // Counters blocks written by the last training run
 
-  // CUDA graph of the batched train step
-  cudaGraphExec_t graph = nullptr;
-  std::vector<int64_t> graph_sig;
-  int graph_kernels = 0;  // kernels per replay (counted at capture)
+  // CUDA graphs of the batched train step, most recently used first; a step
+  // whose signature (views, sizes, buffers, target pointer, ...) matches one
+  // replays it, so callers alternating a few target buffers keep their graphs
+  struct CachedGraph {
+    std::vector<int64_t> sig;
+    cudaGraphExec_t exec = nullptr;
+    int kernels = 0;  // kernels per replay (counted at capture)
+  };
+  std::vector<CachedGraph> graphs;
+  static constexpr size_t kMaxGraphs = 4;
+  void drop_graphs() {
+    for (auto& g : graphs)
+      if (g.exec) cudaGraphExecDestroy(g.exec);
+    graphs.clear();
+  }
 
   // profiling
   bool profiling = false;
@@ -674,29 +685,43 @@ int train_views(RmeshCtx* c, const RmeshCamera* cams, int n_views, const float* 
         sig.push_back(cams[v].width);
         sig.push_back(cams[v].height);
       }
-      if (!c->graph || sig != c->graph_sig) {
-        if (c->graph) {
-          cudaGraphExecDestroy(c->graph);
-          c->graph = nullptr;
+      // graphs captured before a reallocation point at freed buffers
+      for (size_t i = c->graphs.size(); i-- > 0;)
+        if (c->graphs[i].sig[3] != sig[3]) {
+          cudaGraphExecDestroy(c->graphs[i].exec);
+          c->graphs.erase(c->graphs.begin() + i);
         }
+      size_t gi = 0;
+      while (gi < c->graphs.size() && c->graphs[gi].sig != sig) ++gi;
+      if (gi == c->graphs.size()) {
+        RmeshCtx::CachedGraph cg;
         cudaGraph_t g;
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
         const int before = c->kernel_launches;
         int r = enqueue(true);
-        c->graph_kernels = c->kernel_launches - before;
+        cg.kernels = c->kernel_launches - before;
         c->kernel_launches = before;
         cudaError_t e = cudaStreamEndCapture(c->stream, &g);
         if (r != RMESH_OK) return r;
         if (e != cudaSuccess) return fail(c, RMESH_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-        e = cudaGraphInstantiate(&c->graph, g, 0);
+        e = cudaGraphInstantiate(&cg.exec, g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return fail(c, RMESH_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-        c->graph_sig = sig;
+        cg.sig = sig;
+        if (c->graphs.size() == RmeshCtx::kMaxGraphs) {
+          cudaGraphExecDestroy(c->graphs.back().exec);
+          c->graphs.pop_back();
+        }
+        c->graphs.insert(c->graphs.begin(), std::move(cg));
+        gi = 0;
+      } else if (gi > 0) {
+        std::rotate(c->graphs.begin(), c->graphs.begin() + gi, c->graphs.begin() + gi + 1);
+        gi = 0;
       }
       {
         StageScope sc(c, kStComposite, false);  // whole graph accounted as one span
-        CK(cudaGraphLaunch(c->graph, c->stream));
-        c->kernel_launches += c->graph_kernels;
+        CK(cudaGraphLaunch(c->graphs[0].exec, c->stream));
+        c->kernel_launches += c->graphs[0].kernels;
       }
     } else {
       CKR(enqueue(false));
@@ -881,7 +906,7 @@ int rmesh_create(const RmeshSceneDesc* d, RmeshCtx** out) {
 int rmesh_destroy(RmeshCtx* c) {
   if (!c) return RMESH_OK;
   if (c->stream) cudaStreamSynchronize(c->stream);
-  if (c->graph) cudaGraphExecDestroy(c->graph);
+  c->drop_graphs();
   for (auto& e : c->events) {
     cudaEventDestroy(e.a);
     cudaEventDestroy(e.b);
@@ -901,10 +926,7 @@ int rmesh_set_stream(RmeshCtx* c, void* s) {
   if (c->own_stream) cudaStreamDestroy(c->stream);
   c->own_stream = false;
   c->stream = (cudaStream_t)s;
-  if (c->graph) {
-    cudaGraphExecDestroy(c->graph);
-    c->graph = nullptr;
-  }
+  c->drop_graphs();
   return RMESH_OK;
 }
 

@@ -21,11 +21,13 @@ host round trip; ``train_step_views`` trains on several cameras per step.
 from __future__ import annotations
 
 import ctypes
+import sys
 from typing import Sequence
 
 import numpy as np
 
 from . import _lib
+from .staging import StagedTargets
 
 __all__ = ["RMeshRenderer", "RMeshError"]
 
@@ -150,6 +152,12 @@ class RMeshRenderer:
         self._ctx = ctx
         self._width, self._height = int(width), int(height)
         self._tile_size = int(tile_size)
+        torch = sys.modules.get("torch")
+        if device is None and torch is not None and torch.cuda.is_available():
+            device = torch.cuda.current_device()
+        self._device_index = None if device is None else int(device)
+        self._stream_handle = None  # set by set_stream
+        self._torch_stream = None
 
     # ------------------------------------------------------------------ utils
     def _check(self, rc: int):
@@ -213,6 +221,31 @@ class RMeshRenderer:
 
     def set_stream(self, stream_handle: int):
         self._check(self._lib.rmesh_set_stream(self._ctx, ctypes.c_void_p(int(stream_handle))))
+        self._stream_handle = int(stream_handle)
+        self._torch_stream = None
+
+    @property
+    def device_index(self) -> int:
+        """The CUDA device ordinal of this renderer."""
+        if self._device_index is None:
+            import torch
+
+            self._device_index = torch.cuda.current_device()
+        return self._device_index
+
+    def torch_stream(self):
+        """The renderer's CUDA stream as a torch stream.  Without an earlier
+        ``set_stream`` this creates a torch stream and makes it the renderer's."""
+        import torch
+
+        if self._torch_stream is None:
+            if self._stream_handle is None:
+                st = torch.cuda.Stream(device=self.device_index)
+                self.set_stream(st.cuda_stream)
+                self._torch_stream = st
+            else:
+                self._torch_stream = torch.cuda.ExternalStream(self._stream_handle, device=self.device_index)
+        return self._torch_stream
 
     # ------------------------------------------------------------- parameters
     def update_params(self, vertices, base_colors, densities, color_grads, sh_coeffs=None):
@@ -349,13 +382,19 @@ class RMeshRenderer:
         for i, c in enumerate(cameras):
             cams[i] = _camera_struct(c.cam_pos, c.vp, c.c2w_intrinsics, c.width, c.height)
             total += 3 * c.width * c.height
-        if isinstance(gt_images, (list, tuple)):
+        if isinstance(gt_images, StagedTargets):
+            if gt_images._stager._lib_stream is not self.torch_stream():
+                raise ValueError("staged targets belong to another renderer or stream")
+            obj, p = gt_images, None
+        elif isinstance(gt_images, (list, tuple)):
             flat = np.concatenate([np.asarray(_to_numpy(g), np.float32).ravel() for g in gt_images])
             obj, p = flat, flat.ctypes.data
         else:
             obj, p = _as_array(gt_images, np.float32, "gt_images")
         if _numel(obj) != total:
             raise ValueError("gt images do not match the cameras' sizes")
+        if p is None:
+            p = obj._before_step()  # the renderer's stream waits for the targets' copy
         o = _lib.TrainOpts()
         o.lr_verts, o.lr_dens, o.lr_grads, o.lr_base = float(lr_verts), float(lr_dens), float(lr_grads), float(lr_base)
         o.loss_type = int(loss_type)
@@ -455,6 +494,6 @@ class RMeshRenderer:
 
 
 def _numel(x) -> int:
-    if _is_torch(x):
+    if _is_torch(x) or isinstance(x, StagedTargets):
         return int(x.numel())
     return int(np.asarray(x).size)
