@@ -83,6 +83,27 @@ def build_workload(points: int, seed: int, rank: int, n_views: int = N_VIEWS, re
     return scene, cams, gts
 
 
+def build_training(args):
+    """Training-loop workload: a seeded GMM teacher mesh with randomised SH
+    colours and densities, ``args.targets`` target cameras, one held-out camera,
+    and the student: the teacher perturbed (SH + N(0, 0.3), log-density +
+    N(0, 0.5), vertices + N(0, 0.01)) on the same topology."""
+    from rmesh_b200.camera import orbit_cameras
+    from rmesh_b200.scenes import gmm_cloud, make_scene
+
+    rng = np.random.default_rng(args.seed)
+    teacher = make_scene(gmm_cloud(args.points, rng), rng, sh_degree=args.sh_degree)
+    cams = orbit_cameras(args.targets, seed=args.seed + 1, radius=(2.5, 4.0), resolutions=args.res)
+    hold = orbit_cameras(1, seed=args.seed + 99, radius=(3.0, 3.0), resolutions=args.res)[0]
+    prng = np.random.default_rng(args.seed + 2)
+    student = dict(teacher)
+    student["sh_coeffs"] = (teacher["sh_coeffs"] + prng.normal(0, 0.3, teacher["sh_coeffs"].shape)).astype(np.float32)
+    student["densities"] = np.exp(np.log(teacher["densities"]) + prng.normal(0, 0.5, teacher["densities"].shape)
+                                  ).astype(np.float32)
+    student["vertices"] = (teacher["vertices"] + prng.normal(0, 0.01, teacher["vertices"].shape)).astype(np.float32)
+    return teacher, student, cams, hold
+
+
 class Clocks:
     """nvidia-smi sampling during the timed region."""
 
@@ -286,6 +307,9 @@ def run_gpu(args):
 
 
 def metric_name(args) -> str:
+    if args.workload == "training":
+        return (f"fwd+bwd train-steps/s (training loop: {args.views} of {args.targets} {res_text(args.res)} "
+                f"teacher views per graph-captured step)")
     return (f"fwd+bwd train-steps/s ({args.views} views, batched graph-captured step)" if args.workload == "large"
             else "fwd+bwd train-steps/s (16 mixed-resolution views, batched graph-captured step)")
 
@@ -294,9 +318,16 @@ def workload_config(args, n_tets, n_vertices, n_pix, world):
     """The config object of the JSON line (both arms)."""
     mesh = ("8-component GMM" if args.cloud == "gmm" else
             f"uniform [-1,1]^3 + {args.points // 10}-point sphere-shell")
+    if args.workload == "training":
+        text = (f"training: {args.points}-point {mesh} teacher/student Delaunay mesh ({n_tets} tets), "
+                f"{args.targets} target views at {res_text(args.res)}, {args.views} per step in fixed batches, "
+                f"{args.steps} steps, L2 loss, Adam (lr_sh {LR_SH}, lr_verts {LR['lr_verts']}, "
+                f"lr_dens {LR['lr_dens']}, lr_grads {LR['lr_grads']})")
+    else:
+        text = (f"{args.workload}: {args.points}-point {mesh} Delaunay mesh ({n_tets} tets), "
+                f"{args.views} views from {{{res_text(args.res)}}}, L2 loss, Adam")
     return {
-        "workload": f"{args.workload}: {args.points}-point {mesh} Delaunay mesh ({n_tets} tets), "
-                    f"{args.views} views from {{{res_text(args.res)}}}, L2 loss, Adam",
+        "workload": text,
         "n_tets": n_tets, "n_vertices": n_vertices, "views_per_gpu": args.views,
         "pixels_per_step_per_gpu": n_pix, "tile_size": args.tile_size,
         "color_mode": f"sh_degree {args.sh_degree}" if args.sh_degree >= 0 else "base_colors",
@@ -344,13 +375,175 @@ def cpu_baseline(scene, cams, gts, args, budget_s=20.0):
             "mpix_per_s": round(px_done / dt / 1e6, 4)}
 
 
+def run_training(args):
+    """The training loop: the teacher renders the targets on the GPU, then a
+    fresh student renderer takes ``args.steps`` graph-replayed Adam steps of
+    ``args.views`` views each, cycling through the targets in fixed batches.
+    The timed region is the whole loop from the unperturbed start (the first
+    pass over the batches captures their CUDA graphs, inside it).  e2e repeats
+    the loop on another fresh student with the targets in pinned host memory,
+    uploaded each step through TargetStager; its loss trajectory must follow
+    the first run's."""
+    import torch
+
+    from rmesh_b200 import RMeshRenderer, TargetStager
+    from rmesh_b200 import _lib
+
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+        raise SystemExit("the training-loop workload runs on one GPU")
+    torch.cuda.set_device(0)
+    teacher, student, cams, hold = build_training(args)
+    W, H = cams[0].width, cams[0].height
+
+    def renderer(sc, tile):
+        r = RMeshRenderer(sc["vertices"], sc["indices"], sc["base_colors"], sc["densities"], sc["color_grads"],
+                          sc["circumdata"], W, H, tile_size=tile, sh_coeffs=sc["sh_coeffs"],
+                          sh_degree=args.sh_degree)
+        st = torch.cuda.Stream()
+        r.set_stream(st.cuda_stream)
+        return r, st
+
+    rt, _ = renderer(teacher, args.tile_size)
+    targets = [rt.forward_tiled(c.cam_pos, c.vp, c.c2w_intrinsics)[..., :3].copy() for c in cams]
+    want = rt.forward_tiled(hold.cam_pos, hold.vp, hold.c2w_intrinsics)
+    rt.close()
+    vps = args.views
+    nb = len(cams) // vps
+    batches = [cams[k * vps:(k + 1) * vps] for k in range(nb)]
+    host = [torch.from_numpy(np.concatenate([t.ravel() for t in targets[k * vps:(k + 1) * vps]])).pin_memory()
+            for k in range(nb)]
+    dev = [h.cuda() for h in host]
+    n_pix = sum(c.width * c.height for c in batches[0])
+
+    # warm-up on a disposable student: module load, allocator, tile-size autotune
+    rw, _ = renderer(student, args.tile_size)
+    tune_ms = None if args.no_autotune else rw.autotune(batches[0], dev[0], loss_type=1)
+    tile = int(rw.info().tile_size)
+    for i in range(args.warmup):
+        rw.train_step_views(batches[i % nb], dev[i % nb], loss_type=1, mode="graph", lr_sh=LR_SH, **LR)
+    r0, _ = renderer(student, tile)
+    before = float(np.abs(r0.forward_tiled(hold.cam_pos, hold.vp, hold.c2w_intrinsics) - want).mean())
+    r0.close()
+    rw.close()
+
+    lr = dict(LR, lr_verts=LR["lr_verts"] if args.lr_verts is None else args.lr_verts)
+
+    def loop(mode, staged, steps):
+        """Returns (renderer, ms per step, per-step mean losses, per-step ms)."""
+        r, st = renderer(student, tile)
+        stager = TargetStager(r, host[0].numel()) if staged else None
+        losses = []
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        ev[0].record(st)
+        nxt = stager.put(host[0]) if staged else None
+        for i in range(steps):
+            k = i % nb
+            if staged:
+                cur = nxt
+                if i + 1 < steps:
+                    nxt = stager.put(host[(i + 1) % nb])
+            else:
+                cur = dev[k]
+            losses.append(float(np.mean(r.train_step_views(batches[k], cur, loss_type=1, mode=mode, lr_sh=LR_SH,
+                                                           **lr))))
+            ev[i + 1].record(st)
+        ev[-1].synchronize()
+        per = np.array([ev[i].elapsed_time(ev[i + 1]) for i in range(steps)])
+        return r, ev[0].elapsed_time(ev[-1]) / steps, np.array(losses), per
+
+    clk = Clocks(0)
+    r1, ms_graph, losses, per_step = loop("graph", False, args.steps)
+    clocks = clk.stop()
+    _, _, total_launches = r1.stage_times()
+    after = float(np.abs(r1.forward_tiled(hold.cam_pos, hold.vp, hold.c2w_intrinsics) - want).mean())
+    r1.set_profiling(True)
+    for k in range(nb):
+        r1.train_step_views(batches[k], dev[k], loss_type=1, mode="batched", lr_sh=LR_SH, **lr)
+    stage_ms, stage_n, _ = r1.stage_times()
+    r1.set_profiling(False)
+    info = r1.info()
+    dev_gb = int(info.device_bytes) / 1e9
+    r1.close()
+    r2, ms_e2e, losses_e2e, _ = loop("graph", True, args.steps)
+    r2.close()
+    n_plain = min(args.steps, 40)
+    r3, ms_plain, _, _ = loop("plain", False, n_plain)
+    r3.close()
+
+    def diverged_at(ls):
+        """First step whose mean loss is not finite or above 10x the first pass's."""
+        bad = ~np.isfinite(ls) | (ls > 10.0 * ls[:nb].mean())
+        return int(np.argmax(bad)) if bad.any() else None
+
+    def fin(x):
+        return round(float(x), 6) if np.isfinite(x) else None
+
+    d1, d2 = diverged_at(losses), diverged_at(losses_e2e)
+    n_ok = min(d for d in (d1, d2, args.steps) if d is not None)
+    healthy = per_step[:d1] if d1 else per_step
+
+    comp_ms = stage_ms["composite"] / max(stage_n["composite"], 1)
+    n_tets, n_verts = student["indices"].size // 4, student["vertices"].size // 3
+    alg = algorithmic_bytes(int(info.n_pairs_last), n_pix, n_verts, n_tets)
+    peak, peak_kind = peaks()
+    achieved = alg / (comp_ms * 1e-3) / 1e9
+    out = {
+        "metric": metric_name(args), "value": round(1000.0 / ms_graph, 4), "unit": "train-steps/s", "n_gpus": 1,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_graph, 4), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded GMM teacher mesh renders the targets; perturbed student)",
+        "config": {**workload_config(args, n_tets, n_verts, n_pix, 1), "tile_size": tile,
+                   "autotune_ms_per_run": None if tune_ms is None else {str(k): round(v, 2)
+                                                                        for k, v in tune_ms.items()}},
+        "mpix_per_s": round(n_pix / (ms_graph * 1e-3) / 1e6, 2),
+        "plain": {"value": round(1000.0 / ms_plain, 4), "unit": "train-steps/s", "ms_per_step": round(ms_plain, 4),
+                  "steps": n_plain},
+        "batched_graph_vs_plain": round(ms_plain / ms_graph, 3),
+        "e2e": {"value": round(1000.0 / ms_e2e, 4), "unit": "train-steps/s",
+                "h2d_bytes_per_step": int(n_pix * 12 + vps * 160 + 48), "d2h_bytes_per_step": int(_lib.COUNTERS_BYTES)},
+        "gpu_launches": int(total_launches),
+        "device_memory_gb": round(dev_gb, 2),
+        "stage_ms_per_step": {k: round(v / nb, 4) for k, v in stage_ms.items()},
+        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(achieved / peak, 4),
+                     "traffic": int(TILE_DRAM_BYTES_PER_PAIR * int(info.n_pairs_last)),
+                     "kernel": f"tile_kernel<{tile},kModeTrain> (fused forward+loss+adjoint)",
+                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
+                     "fallback 6.65 TB/s", "launch_ms": round(comp_ms, 4), "algorithmic_bytes": alg,
+                     "n_pairs": int(info.n_pairs_last)},
+        "clocks": clocks,
+        "training": {"lr_verts": lr["lr_verts"],
+                     "loss_first_pass": fin(losses[:nb].mean()), "loss_last_pass": fin(losses[-nb:].mean()),
+                     "loss_min": fin(np.nanmin(np.where(np.isfinite(losses), losses, np.nan))),
+                     "loss_min_step": int(np.nanargmin(np.where(np.isfinite(losses), losses, np.nan))),
+                     "diverged_at_step": d1, "e2e_diverged_at_step": d2,
+                     "ms_per_step_before_divergence": round(float(healthy.mean()), 4),
+                     "heldout_l1_before": fin(before), "heldout_l1_after": fin(after),
+                     "e2e_trajectory_max_rel_diff_before_divergence":
+                         fin(np.max(np.abs(losses_e2e[:n_ok] - losses[:n_ok]) / losses[:n_ok])),
+                     "loss_every_25": [fin(x) for x in losses[::25]]},
+    }
+    if not args.no_cpu_baseline:
+        trng = np.random.default_rng(args.seed + 3)
+        gts = [trng.uniform(0, 1, (c.height, c.width, 3)).astype(np.float32) for c in batches[0]]
+        out["cpu_baseline"] = cpu_baseline(student, batches[0], gts, args)
+    print(json.dumps(out), flush=True)
+
+
 def run_reference(args):
     """CPU port of the reference kernels (the reference's wgpu pipeline needs a
     Vulkan/Metal device, unavailable on this machine)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    scene, cams, gts = build_workload(args.points, args.seed, 0, args.views, args.res, args.sh_degree, args.cloud)
+    if args.workload == "training":  # the student scene and one step's batch (uniform targets: same cost)
+        _, scene, cams, _ = build_training(args)
+        cams = cams[:args.views]
+        trng = np.random.default_rng(args.seed + 3)
+        gts = [trng.uniform(0, 1, (c.height, c.width, 3)).astype(np.float32) for c in cams]
+    else:
+        scene, cams, gts = build_workload(args.points, args.seed, 0, args.views, args.res, args.sh_degree, args.cloud)
     n_pix = sum(c.width * c.height for c in cams)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from oracle import Oracle
@@ -396,8 +589,11 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="batched", choices=["batched", "large"],
-                    help="batched: 100k-point GMM mesh, 16 mixed views (default); large: 1M-point mesh, 8 views 1080p")
+    ap.add_argument("--workload", default="batched", choices=["batched", "large", "training"],
+                    help="batched: 100k-point GMM mesh, 16 mixed views (default); large: 1M-point mesh, 8 views "
+                         "1080p; training: 250k-point teacher/student loop, 8 of 32 800^2 views per step, 500 steps")
+    ap.add_argument("--targets", type=int, default=32, help="target views of the training loop")
+    ap.add_argument("--lr-verts", type=float, default=None, help="training loop: vertex learning rate (1e-4)")
     ap.add_argument("--points", type=int, default=None)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--tile-size", type=int, default=12)
@@ -410,7 +606,16 @@ def main():
                     help="comma-separated WxH choices for the views (default 256x256,512x512,800x600,1024x1024); "
                          "smaller cases serve profiler captures")
     args = ap.parse_args()
-    if args.workload == "large":  # memory-bound configuration: 1M uniform + 10 % shell points, 8 HD views
+    steps_given = any(a == "--steps" or a.startswith("--steps=") for a in sys.argv[1:])
+    if args.workload == "training":  # teacher/student loop
+        args.points = 250_000 if args.points is None else args.points
+        args.views = 8 if args.views is None else args.views
+        args.res = args.res or "800x800"
+        args.cloud = "gmm"
+        args.steps = args.steps if steps_given else 500
+        if args.sh_degree < 0 or args.targets % args.views:
+            raise SystemExit("training needs SH colours and a target count divisible by --views")
+    elif args.workload == "large":  # memory-bound configuration: 1M uniform + 10 % shell points, 8 HD views
         args.points = 1_000_000 if args.points is None else args.points
         args.views = 8 if args.views is None else args.views
         args.res = args.res or "1920x1080"
@@ -423,6 +628,8 @@ def main():
     args.warmup = max(3, args.warmup)
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "training":
+        run_training(args)
     else:
         run_gpu(args)
 

@@ -322,11 +322,32 @@ class OracleTrainer:
         self.v = {k: z(k) for k in groups}
 
     def train_step(self, cam, gt, lr_verts, lr_dens, lr_grads, loss_type=1, lr_sh=0.0):
+        loss, fwd, g = self._view_grads(cam, gt, loss_type, threads=1)
+        self._adam_all(g, lr_verts, lr_dens, lr_grads, lr_sh)
+        return loss, fwd, g
+
+    def train_step_views(self, cams, gts, lr_verts, lr_dens, lr_grads, loss_type=1, lr_sh=0.0, threads=1):
+        """The multi-view step of the B200 library (no reference counterpart): the
+        gradient of the sum of the per-view losses (each the single-view loss of
+        lib.rs:2405-2636 over its own pixels), then one Adam update.  Returns the
+        per-view losses."""
+        losses, total = [], None
+        for cam, gt in zip(cams, gts):
+            loss, _, g = self._view_grads(cam, gt, loss_type, threads)
+            losses.append(loss)
+            total = g if total is None else {k: total[k] + g[k] for k in total}
+        self._adam_all(total, lr_verts, lr_dens, lr_grads, lr_sh)
+        return np.array(losses)
+
+    def _view_grads(self, cam, gt, loss_type, threads):
         shv = self.o.sh_values(self.sh) if self.use_sh else None
         deg = self.sh_degree if self.use_sh else 0
         fwd = self.o.forward_tiled(self.scene, cam, self.tile_size, sh=shv, sh_degree=deg)
         loss, dl = self.o.loss(fwd["image"], gt, loss_type)
-        g = self.o.backward(self.scene, cam, dl, fwd, self.tile_size, sh=shv, sh_degree=deg)
+        g = self.o.backward(self.scene, cam, dl, fwd, self.tile_size, threads=threads, sh=shv, sh_degree=deg)
+        return loss, fwd, g
+
+    def _adam_all(self, g, lr_verts, lr_dens, lr_grads, lr_sh):
         self.step += 1
         for key, gk, lr in (("vertices", "d_vertices", lr_verts), ("densities", "d_densities", lr_dens),
                             ("color_grads", "d_color_grads", lr_grads)):
@@ -335,4 +356,3 @@ class OracleTrainer:
             p = self.sh.astype(self.o.np)
             self.o.adam(p, g["d_sh"], self.m_sh, self.v_sh, self.step, lr_sh)
             self.sh = p.astype(np.float32)
-        return loss, fwd, g

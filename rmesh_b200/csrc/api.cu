@@ -132,7 +132,7 @@ struct RmeshCtx {
     int kernels = 0;  // kernels per replay (counted at capture)
   };
   std::vector<CachedGraph> graphs;
-  static constexpr size_t kMaxGraphs = 4;
+  static constexpr size_t kMaxGraphs = 8;
   void drop_graphs() {
     for (auto& g : graphs)
       if (g.exec) cudaGraphExecDestroy(g.exec);

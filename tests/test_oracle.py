@@ -366,6 +366,34 @@ def test_single_tet_loss_decreases():
     assert losses[-1] < 0.01 * losses[0], (losses[0], losses[-1])
 
 
+def test_trainer_views_step_is_the_sum_of_single_view_gradients():
+    """The multi-view step: one view equals the single-view train_step; two
+    views move the parameters as one Adam step on the summed gradients."""
+    from oracle import OracleTrainer
+
+    sc = _sh_scene(seed=5, points=40)
+    rng = np.random.default_rng(6)
+    cams = [_cam(np.array(e), np.zeros(3)) for e in ((2.2, 0.3, 0.4), (-0.5, 2.0, 1.0))]
+    gts = [rng.uniform(0, 1, (H, W, 3)).astype(np.float32) for _ in cams]
+    lrs = (1e-3, 1e-2, 1e-2)
+    a, b = OracleTrainer(sc, use_sh=True), OracleTrainer(sc, use_sh=True)
+    la = a.train_step_views(cams[:1], gts[:1], *lrs, 1, lr_sh=1e-2)
+    lb = b.train_step(cams[0], gts[0], *lrs, 1, lr_sh=1e-2)[0]
+    assert la[0] == lb
+    for k in ("vertices", "densities", "color_grads"):
+        np.testing.assert_array_equal(a.scene[k], b.scene[k])
+    np.testing.assert_array_equal(a.sh, b.sh)
+
+    c, d = OracleTrainer(sc, use_sh=True), OracleTrainer(sc, use_sh=True)
+    lc = c.train_step_views(cams, gts, *lrs, 1, lr_sh=1e-2)
+    g = [d._view_grads(cam, gt, 1, 1)[2] for cam, gt in zip(cams, gts)]
+    d._adam_all({k: g[0][k] + g[1][k] for k in g[0]}, *lrs, 1e-2)
+    assert lc.shape == (2,) and np.all(lc > 0)
+    for k in ("vertices", "densities", "color_grads"):
+        np.testing.assert_array_equal(c.scene[k], d.scene[k])
+    assert np.any(c.scene["densities"] != sc["densities"])
+
+
 def _sh_scene(seed=3, points=60, degree=3):
     from rmesh_b200.scenes import make_scene, uniform_cloud
 
