@@ -19,6 +19,7 @@ Line printed by rank 0 (one JSON object):
   plain          train-steps/s of the one-view-per-launch path on the same step
   roofline       dominant kernel (fused forward+loss+adjoint compositing):
                  algorithmic bytes / measured launch time vs measured HBM peak
+  issue_roofline the same kernel against its real ceiling, instruction issue
   cpu_baseline   the CPU oracle (C port of the reference kernels) on all host
                  cores, timed on a sample of the step and scaled to the metric
 
@@ -48,9 +49,25 @@ LR = dict(lr_verts=1e-4, lr_dens=1e-2, lr_grads=1e-3)
 LR_SH = 2.5e-3
 # DRAM bytes (read + write) per (tile, tet) pair of the fused compositing
 # kernel, from one ncu capture of this workload's launch
-# (dram__bytes_read.sum + dram__bytes_write.sum = 4.83 GB for 37.74 M pairs);
+# (dram__bytes_read.sum + dram__bytes_write.sum = 4.84 GB for 37.54 M pairs);
 # the roofline's "traffic" scales it to the run's pair count.
 TILE_DRAM_BYTES_PER_PAIR = 128.0
+# Warp instructions per (tile, tet) pair of the same kernel, from one ncu
+# capture of this workload's launch (smsp__inst_executed.sum = 59.42 G for
+# 37.54 M pairs); the issue ceiling is 148 SMs x 4 schedulers x one
+# instruction per clock.
+TILE_WARP_INST_PER_PAIR = 1583.0
+
+
+def issue_roofline(n_pairs: int, launch_ms: float, sm_mhz) -> dict:
+    """The tile kernel's bound in practice: instruction issue, not HBM."""
+    mhz = float(sm_mhz) if sm_mhz else 1965.0
+    peak = 148 * 4 * mhz * 1e6 / 1e12
+    achieved = TILE_WARP_INST_PER_PAIR * n_pairs / (launch_ms * 1e-3) / 1e12
+    return {"achieved": round(achieved, 4), "peak": round(peak, 4), "unit": "T warp-instructions/s",
+            "frac": round(achieved / peak, 4),
+            "basis": f"{TILE_WARP_INST_PER_PAIR:.0f} warp instructions per pair (ncu) x pairs / launch time; "
+                     f"peak 148 SMs x 4 schedulers x {mhz:.0f} MHz"}
 
 
 def res_text(res) -> str:
@@ -294,6 +311,7 @@ def run_gpu(args):
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                      "fallback 6.65 TB/s", "launch_ms": round(comp_ms, 4), "algorithmic_bytes": alg,
                      "n_pairs": int(info.n_pairs_last)},
+        "issue_roofline": issue_roofline(int(info.n_pairs_last), comp_ms, clocks.get("sm_mhz")),
         "clocks": clocks,
     }
     if rank == 0 and not args.no_cpu_baseline:
@@ -512,6 +530,7 @@ def run_training(args):
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                      "fallback 6.65 TB/s", "launch_ms": round(comp_ms, 4), "algorithmic_bytes": alg,
                      "n_pairs": int(info.n_pairs_last)},
+        "issue_roofline": issue_roofline(int(info.n_pairs_last), comp_ms, clocks.get("sm_mhz")),
         "clocks": clocks,
         "training": {"lr_verts": lr["lr_verts"],
                      "loss_first_pass": fin(losses[:nb].mean()), "loss_last_pass": fin(losses[-nb:].mean()),
