@@ -69,3 +69,38 @@ def test_many_tiles_batched_step(c1_scene, oracle32):
         losses = r.train_step_views(cams, gts, 0.0, 0.0, 0.0, 1, mode=mode)
         np.testing.assert_allclose(losses, want, rtol=1e-4)
         assert r.info().n_views_last == 8
+
+
+def test_pair_buffer_overflow_grows_and_retries(oracle32):
+    """One tet filling 16 views of 1400x1400: 119,158 (tile, tet) pairs in
+    total overflow the initial 65,536-slot pair buffer; the step grows the
+    buffer and redoes the run inside the same call (no error reaches the
+    caller), the per-view losses equal the oracle's, and a graph-mode step
+    after the growth (new buffers, new capture) agrees as well."""
+    from conftest import known_tet_scene
+
+    from rmesh_b200.camera import make_camera
+
+    sc = known_tet_scene()
+    n = 16
+    i = np.arange(n) + 0.5
+    phi = np.arccos(1 - 2 * i / n)
+    th = np.pi * (1 + 5 ** 0.5) * i
+    dirs = np.stack([np.cos(th) * np.sin(phi), np.sin(th) * np.sin(phi), np.cos(phi)], 1)
+    cams = [make_camera(tuple(1.6 * d), (0.0, 0.0, 0.0), 45.0, 1400, 1400) for d in dirs]
+    rng = np.random.default_rng(17)
+    gts = [rng.uniform(0, 1, (1400, 1400, 3)).astype(np.float32) for _ in cams]
+    want, total = [], 0
+    for c, g in zip(cams, gts):
+        f = oracle32.forward_tiled(sc, c)
+        total += int(f["P"])
+        want.append(oracle32.loss(f["image"], g, 1)[0])
+    assert total > 65536
+    r = make_renderer(sc, cams[0])
+    assert r.info().pair_capacity <= 65536 or r.info().pair_capacity == 0
+    for mode in ("batched", "graph", "graph"):
+        losses = r.train_step_views(cams, gts, 0.0, 0.0, 0.0, 1, mode=mode)
+        np.testing.assert_allclose(losses, want, rtol=1e-4)
+        assert r.info().n_pairs_last == total
+    assert r.info().pair_capacity >= total
+    r.close()
