@@ -104,6 +104,7 @@ struct RmeshCtx {
   DevBuf vis_color, vis_dcolor, vis_index;  // SH colours per entry, their gradients, (view, tet) -> entry
   DevBuf pair_key, pair_val, pair_key_alt, pair_val_alt, ranges;
   DevBuf rgba, aux, dl, gt, out_a, out_b, out_c, out_d;
+  DevBuf span_cache;  // per-CTA adjoint span cache of persistent train launches
   DevBuf err_in, err_out;  // per-pixel error inputs, per-tet error statistics
   uint64_t cap_pairs = 0;
   uint64_t generation = 0;  // bumped whenever a buffer is reallocated
@@ -284,6 +285,16 @@ int setup_sort_attrs() {
 }
 
 // ---------------------------------------------------------------- buffers
+// Adjoint span cache: tile-list entries per CTA slot, and slots for a
+// persistent grid (resident CTAs per SM the kernel is built for x SMs; a
+// larger grid runs without the cache)
+constexpr uint32_t kSpanCacheTets = 2048;
+uint64_t span_cache_slots(const RmeshCtx* c) {
+  const int minb = c->tile_size == 16 ? TileCfg<16, false>::MINB
+                                      : (c->tile_size == 12 ? TileCfg<12, false>::MINB : TileCfg<8, false>::MINB);
+  return (uint64_t)minb * (uint64_t)c->num_sms;
+}
+
 int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t total_tiles) {
   const uint64_t items = (uint64_t)n_views * (uint64_t)c->M;
   CKR(ensure_buf(c, c->vis_key, items * 8));
@@ -294,6 +305,7 @@ int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t
   CKR(ensure_buf(c, c->vis_cnt, items * 4));
   CKR(ensure_buf(c, c->vis_proj, items * 32));
   CKR(ensure_buf(c, c->vis_view, items * sizeof(TetView)));
+  CKR(ensure_buf(c, c->span_cache, span_cache_slots(c) * kSpanCacheTets * (uint64_t)c->tile_size * sizeof(short2)));
   if (c->sh_degree >= 0) {
     CKR(ensure_buf(c, c->vis_color, items * 16));
     CKR(ensure_buf(c, c->vis_dcolor, items * 16));
@@ -461,6 +473,11 @@ int launch_tile_t(RmeshCtx* c, TileArgs& ta, uint32_t n_tiles, bool persistent) 
     grid = std::min<unsigned>(grid, std::max<uint32_t>(n_tiles, 1));
   }
   ta.persistent = persistent ? 1 : 0;
+  if (MODE == kModeTrain && persistent && c->span_cache.p &&
+      (uint64_t)grid * kSpanCacheTets * TS * sizeof(short2) <= c->span_cache.bytes) {
+    ta.span_cache = c->span_cache.as<short2>();
+    ta.span_cache_tets = kSpanCacheTets;
+  }
   if (grid == 0) return RMESH_OK;
   tile_kernel<TS, MODE, AUX><<<grid, NT, smem, c->stream>>>(ta);
   CKL();

@@ -82,6 +82,11 @@ struct TileArgs {
   Counters* counters;
   const AdamParams* hp;
   int persistent;
+  // train mode, persistent launches: per-CTA cache of the adjoint's pixel
+  // spans (span_cache_tets entries of TS rows per CTA), written by the forward
+  // pass of the same tile; nullptr disables it
+  short2* span_cache;
+  uint32_t span_cache_tets;
 };
 
 template <int TS, bool AUX>
@@ -220,6 +225,10 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
   uint32_t phase_bits = 0u;  // parity of the next phase of bar[0] (bit 0) and bar[1] (bit 1)
   bool failed = false;
 
+  // this CTA's span cache slot (persistent train launches only)
+  short2* const scache = (MODE == kModeTrain && a.span_cache)
+                             ? a.span_cache + (size_t)blockIdx.x * a.span_cache_tets * TS
+                             : nullptr;
   const uint32_t first_tile = blockIdx.x;
   while (true) {
     if (tid == 0) s.tile = a.persistent ? atomicAdd(&a.counters->tile_ticket, 1u) : first_tile;
@@ -301,11 +310,31 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
     // px/py, minus the tile origin): spans include pixels up to 0.001 px
     // outside the silhouette, where the exact ray test misses anyway, so a
     // last-bit difference in a span end changes no pixel value.
-    auto spans = [&](int buf, int nb, bool vertex_rows) {
+    // span of pixel columns [xl, xr] of one row (empty when xl > xr)
+    auto span_of = [&](float xl, float xr) -> short2 {
+      short2 sp = make_short2(0, -1);
+      if (xl <= xr) {
+        const int32_t lo = max(__float2int_rz(ceilf(xl - 0.5f - 0.001f)), 0);
+        const int32_t hi = min(min(__float2int_rz(floorf(xr - 0.5f + 0.001f)), TS - 1), valid_cols - 1);
+        if (lo <= hi) sp = make_short2((short)lo, (short)hi);
+      }
+      return sp;
+    };
+    // cache: the forward (vertex_rows) also stores each task's adjoint span
+    // (edge crossings only) at its list position first + dir * k
+    auto spans = [&](int buf, int nb, bool vertex_rows, short2* cache, uint32_t first, int dir) {
       for (int i = tid; i < TS * TS; i += NT) s.pmask[i] = 0u;
       for (int task = tid; task < nb * TS; task += NT) {
         const int k = task / TS, row = task - (task / TS) * TS;
         short2 sp = make_short2(0, -1);
+        short2* slot = nullptr;
+        if (cache) {
+          const uint32_t rel = first + (uint32_t)(dir * k) - rs;
+          if (rel < a.span_cache_tets) {
+            slot = cache + (size_t)rel * TS + row;
+            *slot = sp;  // overwritten below when the row has crossings
+          }
+        }
         const TetView& tv = s.view[buf][k];
         if (!((__float_as_uint(tv.gm.w) >> 4) & 1u) && row < valid_rows) {
           const float4 gx4 = tv.px, gy4 = tv.py;
@@ -334,6 +363,9 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
               xr = fmaxf(xr, x);
             }
           }
+          // the adjoint's span of this row: the same edge crossings, no
+          // vertex rows (empty when no edge crosses yc)
+          if (slot) *slot = span_of(xl, xr);
           if (vertex_rows) {
             const float blo = fs(yc, 0.5f), bhi = fa(yc, 0.5f);
 #pragma unroll
@@ -345,14 +377,16 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
               }
             }
           }
-          if (xl <= xr) {
-            const int32_t lo = max(__float2int_rz(ceilf(xl - 0.5f - 0.001f)), 0);
-            const int32_t hi = min(min(__float2int_rz(floorf(xr - 0.5f + 0.001f)), TS - 1), valid_cols - 1);
-            if (lo <= hi) sp = make_short2((short)lo, (short)hi);
-          }
+          sp = span_of(xl, xr);
         }
         s.span[k][row] = sp;
       }
+    };
+    // the adjoint's spans of list positions [lo, lo + nb) from the cache
+    auto cached_spans = [&](const short2* cache, uint32_t lo, int nb) {
+      for (int i = tid; i < TS * TS; i += NT) s.pmask[i] = 0u;
+      const short2* src = cache + (size_t)(lo - rs) * TS;
+      for (int task = tid; task < nb * TS; task += NT) (&s.span[0][0])[task] = src[task];
     };
     // per-tet row prefix sums and tet-major item offsets (after spans)
     auto prefixes = [&](int nb) {
@@ -464,6 +498,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
     };
 
     float Cr = 0.f, Cg = 0.f, Cb = 0.f, logT = 0.f;
+    uint32_t span_lo = re;  // the forward cached the adjoint spans of list positions [span_lo, re)
     float nd0 = 0.f, nd1 = 0.f, nd2 = 0.f, nd3 = 0.f, en0 = 0.f, en1 = 0.f, en2 = 0.f, en3 = 0.f;
 
     // =============== forward (front to back) ===============
@@ -499,7 +534,8 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
             const uint32_t h2 = next_hi - (uint32_t)nbn;
             if (h2 > rs) idx_next = load_idx(h2 - 1u, (int)min((uint32_t)kBatch, h2 - rs), -1);
           }
-          spans(buf, nb, true);
+          spans(buf, nb, true, scache, hi - 1u, -1);
+          span_lo = next_hi;  // the adjoint spans of [next_hi, hi) are cached
           __syncthreads();
           prefixes(nb);
           __syncthreads();
@@ -618,7 +654,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
             const uint32_t h2 = next_hi - (uint32_t)nbn;
             if (h2 > rs) idx_next = load_idx(h2 - 1u, (int)min((uint32_t)kBatch, h2 - rs), -1);
           }
-          spans(buf, nb, true);
+          spans(buf, nb, true, nullptr, 0u, 0);
           __syncthreads();
           prefixes(nb);
           __syncthreads();
@@ -805,7 +841,12 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
             const uint32_t l2 = next_lo + (uint32_t)nbn;
             if (l2 < re) idx_next = load_idx(l2, (int)min((uint32_t)kBatch, re - l2), +1);
           }
-          spans(buf, nb, false);  // adjoint: edge crossings only
+          // adjoint: edge crossings only, from the forward's cache when it
+          // covered the whole batch
+          if (scache && lo >= span_lo && lo + (uint32_t)nb - rs <= a.span_cache_tets)
+            cached_spans(scache, lo, nb);
+          else
+            spans(buf, nb, false, nullptr, 0u, 0);
           __syncthreads();
           prefixes(nb);
           __syncthreads();
