@@ -184,8 +184,22 @@ __device__ __forceinline__ float sh_direction(const TetRec& r, const float* cam,
 // softplus(SH(dir) + 0.5 + dot(g, v0 - centroid)), evaluated term by term in
 // the shader's order with explicitly rounded arithmetic.
 template <int DEG>
-__device__ __forceinline__ float4 sh_color(const TetRec& r, const float* __restrict__ q, const float* cam) {
+__device__ __forceinline__ float4 sh_color(const TetRec& r, const float* __restrict__ q_in, const float* cam) {
   constexpr int NC = (DEG + 1) * (DEG + 1);
+  // the tet's 3 x nc coefficients in registers; 16-byte loads when a tet's
+  // row (3 nc floats) keeps 16-byte alignment (degrees 1 and 3)
+  float q[3 * NC];
+  if ((3 * NC) % 4 == 0) {
+    const float4* q4 = reinterpret_cast<const float4*>(q_in);
+#pragma unroll
+    for (int i = 0; i < 3 * NC / 4; ++i) {
+      const float4 v = __ldg(q4 + i);
+      q[4 * i] = v.x; q[4 * i + 1] = v.y; q[4 * i + 2] = v.z; q[4 * i + 3] = v.w;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 3 * NC; ++i) q[i] = __ldg(q_in + i);
+  }
   float3 cen, dir;
   sh_direction(r, cam, cen, dir);
   const float x = dir.x, y = dir.y, z = dir.z;
@@ -259,7 +273,9 @@ struct ProjectArgs {
   Counters* counters;
 };
 
-__global__ void __launch_bounds__(256) project_kernel(ProjectArgs a) {
+// 3 resident blocks per SM: the register cap keeps the SH coefficients of
+// the 16-byte loads in registers without dropping to 2 blocks
+__global__ void __launch_bounds__(256, 3) project_kernel(ProjectArgs a) {
   __shared__ uint32_t s_blk;
   __shared__ uint32_t s_warp[8];
   __shared__ unsigned long long s_prefix;
