@@ -101,6 +101,7 @@ struct TileCfg {
 template <int TS, bool AUX>
 struct __align__(16) TileSmem {
   TetView view[2][kBatch];  // staged per-view tet records (double buffered)
+  short2 span_pf[kBatch][TS];  // adjoint: the next batch's cached spans (bulk copy)
   float mom[kBatch][kMom];  // adjoint moments per tet (phase 2)
   float4 pdir[TS * TS];     // pixel ray direction
   float4 pdl[TS * TS];      // pixel dL/dRGB (adjoint)
@@ -281,11 +282,15 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
       if (warp != 0 || lane >= nb) return 0u;
       return a.pair_val[dir < 0 ? first - (uint32_t)lane : first + (uint32_t)lane];
     };
-    auto issue = [&](int buf, int nb, uint32_t idx) {
+    // span_src (adjoint): the batch's cached spans, copied into span_pf on the
+    // same barrier
+    auto issue = [&](int buf, int nb, uint32_t idx, const short2* span_src) {
       if (warp == 0) {
         if (lane == 0) {
           fence_proxy_async_smem();
-          mbar_arrive_expect_tx(&s.bar[buf], (uint32_t)nb * (uint32_t)sizeof(TetView));
+          const uint32_t span_bytes = span_src ? (uint32_t)(nb * TS * (int)sizeof(short2)) : 0u;
+          mbar_arrive_expect_tx(&s.bar[buf], (uint32_t)nb * (uint32_t)sizeof(TetView) + span_bytes);
+          if (span_src) bulk_copy_g2s(&s.span_pf[0][0], span_src, span_bytes, &s.bar[buf]);
         }
         __syncwarp();
         if (lane < nb)
@@ -382,11 +387,10 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
         s.span[k][row] = sp;
       }
     };
-    // the adjoint's spans of list positions [lo, lo + nb) from the cache
-    auto cached_spans = [&](const short2* cache, uint32_t lo, int nb) {
+    // the adjoint's spans of a cached batch, already copied into span_pf
+    auto cached_spans = [&](int nb) {
       for (int i = tid; i < TS * TS; i += NT) s.pmask[i] = 0u;
-      const short2* src = cache + (size_t)(lo - rs) * TS;
-      for (int task = tid; task < nb * TS; task += NT) (&s.span[0][0])[task] = src[task];
+      for (int task = tid; task < nb * TS; task += NT) (&s.span[0][0])[task] = (&s.span_pf[0][0])[task];
     };
     // per-tet row prefix sums and tet-major item offsets (after spans)
     auto prefixes = [&](int nb) {
@@ -514,7 +518,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
       if (re > rs) {
         {
           const int nb0 = (int)min((uint32_t)kBatch, re - rs);
-          issue(0, nb0, load_idx(re - 1u, nb0, -1));
+          issue(0, nb0, load_idx(re - 1u, nb0, -1), nullptr);
         }
         uint32_t idx_next = 0u;  // record indices of the batch after the current one
         if (re - rs > (uint32_t)kBatch) {
@@ -530,7 +534,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
           if (failed) break;
           if (next_hi > rs) {
             const int nbn = (int)min((uint32_t)kBatch, next_hi - rs);
-            issue(buf ^ 1, nbn, idx_next);
+            issue(buf ^ 1, nbn, idx_next, nullptr);
             const uint32_t h2 = next_hi - (uint32_t)nbn;
             if (h2 > rs) idx_next = load_idx(h2 - 1u, (int)min((uint32_t)kBatch, h2 - rs), -1);
           }
@@ -634,7 +638,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
       if (re > rs) {
         {
           const int nb0 = (int)min((uint32_t)kBatch, re - rs);
-          issue(0, nb0, load_idx(re - 1u, nb0, -1));
+          issue(0, nb0, load_idx(re - 1u, nb0, -1), nullptr);
         }
         uint32_t idx_next = 0u;
         if (re - rs > (uint32_t)kBatch) {
@@ -650,7 +654,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
           if (failed) break;
           if (next_hi > rs) {
             const int nbn = (int)min((uint32_t)kBatch, next_hi - rs);
-            issue(buf ^ 1, nbn, idx_next);
+            issue(buf ^ 1, nbn, idx_next, nullptr);
             const uint32_t h2 = next_hi - (uint32_t)nbn;
             if (h2 > rs) idx_next = load_idx(h2 - 1u, (int)min((uint32_t)kBatch, h2 - rs), -1);
           }
@@ -817,11 +821,21 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
         dlr = dl.x; dlg = dl.y; dlb = dl.z;
       }
       if (in_tile) s.pdl[pl] = make_float4(dlr, dlg, dlb, 0.0f);
+      // a batch [lo, lo + nb) takes its spans from the forward's cache when
+      // the forward covered all of it
+      auto span_cached = [&](uint32_t lo, int nb) -> bool {
+        return scache && lo >= span_lo && lo + (uint32_t)nb - rs <= a.span_cache_tets;
+      };
+      auto span_src = [&](uint32_t lo, int nb) -> const short2* {
+        return span_cached(lo, nb) ? scache + (size_t)(lo - rs) * TS : nullptr;
+      };
       if (re > rs) {
+        // the forward's span-cache writes, before the bulk copies that read them
+        if (scache) fence_proxy_async_global();
         __syncthreads();
         {
           const int nb0 = (int)min((uint32_t)kBatch, re - rs);
-          issue(0, nb0, load_idx(rs, nb0, +1));
+          issue(0, nb0, load_idx(rs, nb0, +1), span_src(rs, nb0));
         }
         uint32_t idx_next = 0u;
         if (re - rs > (uint32_t)kBatch) {
@@ -835,19 +849,20 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
           const uint32_t next_lo = lo + (uint32_t)nb;
           wait_buf(buf);
           if (failed) break;
-          if (next_lo < re) {
-            const int nbn = (int)min((uint32_t)kBatch, re - next_lo);
-            issue(buf ^ 1, nbn, idx_next);
-            const uint32_t l2 = next_lo + (uint32_t)nbn;
-            if (l2 < re) idx_next = load_idx(l2, (int)min((uint32_t)kBatch, re - l2), +1);
-          }
           // adjoint: edge crossings only, from the forward's cache when it
           // covered the whole batch
-          if (scache && lo >= span_lo && lo + (uint32_t)nb - rs <= a.span_cache_tets)
-            cached_spans(scache, lo, nb);
+          if (span_cached(lo, nb))
+            cached_spans(nb);
           else
             spans(buf, nb, false, nullptr, 0u, 0);
           __syncthreads();
+          // the next batch's copies, after span_pf has been read
+          if (next_lo < re) {
+            const int nbn = (int)min((uint32_t)kBatch, re - next_lo);
+            issue(buf ^ 1, nbn, idx_next, span_src(next_lo, nbn));
+            const uint32_t l2 = next_lo + (uint32_t)nbn;
+            if (l2 < re) idx_next = load_idx(l2, (int)min((uint32_t)kBatch, re - l2), +1);
+          }
           prefixes(nb);
           __syncthreads();
           fill(nb);

@@ -3,7 +3,8 @@
 // Only the plain, CTA-local form of cp.async.bulk is used: global -> this
 // CTA's shared memory, completion counted on a local mbarrier.  No cluster
 // multicast anywhere.  Sources are 16-byte aligned and sizes are multiples
-// of 16 bytes (64-byte tet records, 16-byte colours).
+// of 16 bytes (144-byte per-view tet records, span-cache rows of 32/48/64
+// bytes per tet).
 #pragma once
 #include <stdint.h>
 
@@ -26,6 +27,12 @@ __device__ __forceinline__ void fence_mbar_init() {
 // subsequent async-proxy (bulk copy) accesses.
 __device__ __forceinline__ void fence_proxy_async_smem() {
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Order this thread's earlier generic-proxy global-memory writes before
+// later async-proxy (bulk copy) reads of them.
+__device__ __forceinline__ void fence_proxy_async_global() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
 }
 
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
