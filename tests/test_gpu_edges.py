@@ -104,3 +104,25 @@ def test_pair_buffer_overflow_grows_and_retries(oracle32):
         assert r.info().n_pairs_last == total
     assert r.info().pair_capacity >= total
     r.close()
+
+
+def test_long_tile_lists_past_the_span_cache(c2_scene):
+    """65k tets seen at 48x48 (16 tiles of 12x12): each tile's list holds
+    thousands of tets, more than the 2,048 entries of the per-CTA span cache,
+    so the batched adjoint reads cached spans for the head of each list and
+    recomputes the tail; losses and parameters equal the plain path's."""
+    from rmesh_b200.camera import orbit_cameras
+
+    cams = orbit_cameras(2, seed=21, radius=(2.8, 3.2), resolutions=((48, 48),))
+    rng = np.random.default_rng(22)
+    gts = [rng.uniform(0, 1, (48, 48, 3)).astype(np.float32) for _ in cams]
+    out = {}
+    for mode in ("plain", "batched"):
+        r = make_renderer(c2_scene, cams[0], sh=True)
+        losses = [r.train_step_views(cams, gts, 1e-4, 1e-2, 1e-3, 1, mode=mode, lr_sh=2.5e-3) for _ in range(2)]
+        out[mode] = (np.array(losses), r.get_params(), r.info().n_pairs_last)
+        r.close()
+    assert out["batched"][2] / (2 * 16) > 2048  # mean tile list longer than the cache
+    np.testing.assert_allclose(out["batched"][0], out["plain"][0], rtol=1e-4)
+    for k in out["plain"][1]:
+        assert rel_l2(out["batched"][1][k], out["plain"][1][k]) <= 1e-3, k

@@ -139,7 +139,10 @@ def test_train_step_matches_oracle(c1_scene):
         assert rel_l2(p[k], tr.scene[k]) <= 1e-3, k
 
 
-def test_views_modes_agree(c1_scene):
+@pytest.mark.parametrize("ts", [8, 12, 16])
+def test_views_modes_agree(c1_scene, ts):
+    """plain (one launch per view, no span cache) vs batched and graph
+    (persistent launches whose adjoint reads the forward's span cache)."""
     from rmesh_b200.camera import orbit_cameras
 
     cams = orbit_cameras(4, seed=3, radius=(2.5, 3.5), resolutions=((96, 96), (128, 80), (64, 64)))
@@ -147,7 +150,7 @@ def test_views_modes_agree(c1_scene):
     gts = [rng.uniform(0, 1, (c.height, c.width, 3)).astype(np.float32) for c in cams]
     out = {}
     for mode in ("plain", "batched", "graph"):
-        r = make_renderer(c1_scene, cams[0])
+        r = make_renderer(c1_scene, cams[0], tile_size=ts)
         losses = [r.train_step_views(cams, gts, 1e-4, 1e-2, 1e-3, 1, mode=mode) for _ in range(2)]
         out[mode] = (np.array(losses), r.get_params())
     for mode in ("batched", "graph"):
