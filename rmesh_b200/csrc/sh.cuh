@@ -76,8 +76,10 @@ struct ShBackwardArgs {
   float* grad_slot;          // [M][kGradSlot], colour gradient [4..6] and vertices [7..18] accumulated
 };
 
+// 4 resident blocks per SM (the register cap keeps the degree-3 coefficient
+// and gradient arrays in registers)
 template <int DEG>
-__global__ void __launch_bounds__(128) sh_backward_kernel(ShBackwardArgs a) {
+__global__ void __launch_bounds__(128, 4) sh_backward_kernel(ShBackwardArgs a) {
   constexpr int NC = (DEG + 1) * (DEG + 1);
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= a.M) return;
@@ -85,13 +87,23 @@ __global__ void __launch_bounds__(128) sh_backward_kernel(ShBackwardArgs a) {
   for (int v = 0; v < a.n_views && !any; ++v) any = a.vis_index[(size_t)v * a.M + t] != kSentinel;
   if (!any) return;
   const TetRec r = a.rec[t];
+  // a tet's 3 nc floats keep 16-byte alignment at degrees 1 and 3: vector
+  // loads and stores there
+  constexpr bool kVec = (3 * NC) % 4 == 0;
   float q[3 * NC], dq[3 * NC];
   const float* src = a.sh + (size_t)t * 3 * NC;
+  if (kVec) {
 #pragma unroll
-  for (int i = 0; i < 3 * NC; ++i) {
-    q[i] = sh_f16(src[i]);
-    dq[i] = 0.0f;
+    for (int i = 0; i < 3 * NC / 4; ++i) {
+      const float4 v = __ldg(reinterpret_cast<const float4*>(src) + i);
+      q[4 * i] = sh_f16(v.x); q[4 * i + 1] = sh_f16(v.y); q[4 * i + 2] = sh_f16(v.z); q[4 * i + 3] = sh_f16(v.w);
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 3 * NC; ++i) q[i] = sh_f16(src[i]);
   }
+#pragma unroll
+  for (int i = 0; i < 3 * NC; ++i) dq[i] = 0.0f;
   const float gx = r.b.w, gy = r.c.w, gz = r.d.w;
   float dg0 = 0.f, dg1 = 0.f, dg2 = 0.f;
   float dc0 = 0.f, dc1 = 0.f, dc2 = 0.f;  // d centroid
@@ -137,8 +149,18 @@ __global__ void __launch_bounds__(128) sh_backward_kernel(ShBackwardArgs a) {
     }
   }
   float* dst = a.d_sh + (size_t)t * 3 * NC;
+  if (kVec) {
 #pragma unroll
-  for (int i = 0; i < 3 * NC; ++i) dst[i] += dq[i];
+    for (int i = 0; i < 3 * NC / 4; ++i) {
+      float4* d4 = reinterpret_cast<float4*>(dst) + i;
+      float4 v = *d4;
+      v.x += dq[4 * i]; v.y += dq[4 * i + 1]; v.z += dq[4 * i + 2]; v.w += dq[4 * i + 3];
+      *d4 = v;
+    }
+  } else {
+#pragma unroll
+    for (int i = 0; i < 3 * NC; ++i) dst[i] += dq[i];
+  }
   float* sl = a.grad_slot + (size_t)t * kGradSlot;
   sl[4] += dg0; sl[5] += dg1; sl[6] += dg2;
   const float qx = 0.25f * dc0, qy = 0.25f * dc1, qz = 0.25f * dc2;
