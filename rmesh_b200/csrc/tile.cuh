@@ -147,10 +147,6 @@ __device__ __forceinline__ bool face_flipped(const TetView& tv, int f) {
 // (rasterize_compute.wgsl:355-390): |den| < 1e-20 is parallel (outside if
 // num > 0), entry = max t over den > 0 (strict), exit = min t over den < 0.
 // Exact arithmetic: t_max - t_min cancels for thin tets.
-// EXACT: correctly rounded products, sums and quotients (the forward, whose
-// image depends on t_max - t_min); otherwise contracted dot products and the
-// 2-ulp quotient (the adjoint's recomputation, held to the gradient bar).
-template <bool EXACT>
 __device__ __forceinline__ bool intersect4(const float4* nrm, const float* num_override, float dx, float dy, float dz,
                                            float& t_min, float& t_max, int& fmin, int& fmax) {
   t_min = -3.402823e38f;
@@ -162,13 +158,13 @@ __device__ __forceinline__ bool intersect4(const float4* nrm, const float* num_o
 #pragma unroll
   for (int f = 0; f < 4; ++f) {
     const float4 n = nrm[f];
-    const float den = EXACT ? dot3x(n.x, n.y, n.z, dx, dy, dz) : fmaf(n.x, dx, fmaf(n.y, dy, n.z * dz));
+    const float den = dot3x(n.x, n.y, n.z, dx, dy, dz);
     const float num = num_override ? num_override[f] : n.w;
     if (fabsf(den) < 1e-20f) {
       if (num > 0.0f) ok = false;
       continue;
     }
-    const float t = EXACT ? fdv(num, den) : __fdividef(num, den);
+    const float t = fdv(num, den);
     if (den > 0.0f) {
       if (t > t_min) { t_min = t; fmin = f; entry = f; }
     } else {
@@ -485,8 +481,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
         int fmin, fmax;
         float4 out = make_float4(0.f, 0.f, 0.f, -1.0f);  // od < 0: the ray misses
         float4 out2 = make_float4(0.f, 0.f, 0.f, 0.f);
-        const bool hit = fwd ? intersect4<true>(tv.nrm, nump, d.x, d.y, d.z, t_min, t_max, fmin, fmax)
-                             : intersect4<false>(tv.nrm, nump, d.x, d.y, d.z, t_min, t_max, fmin, fmax);
+        const bool hit = intersect4(tv.nrm, nump, d.x, d.y, d.z, t_min, t_max, fmin, fmax);
         if (hit) {
           float4 cb = tv.cb;
           if (fwd && has_min_t) cb = make_float4(bcr_o, bcg_o, bcb_o, cb.w);
