@@ -105,6 +105,7 @@ struct RmeshCtx {
   DevBuf pair_key, pair_val, pair_key_alt, pair_val_alt, ranges;
   DevBuf rgba, aux, dl, gt, out_a, out_b, out_c, out_d;
   DevBuf span_cache;  // per-CTA adjoint span cache of persistent train launches
+  DevBuf tile_order, order_hist;  // longest-first tile order of the run; bucket counts and cursors
   DevBuf err_in, err_out;  // per-pixel error inputs, per-tet error statistics
   uint64_t cap_pairs = 0;
   uint64_t generation = 0;  // bumped whenever a buffer is reallocated
@@ -321,6 +322,8 @@ int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t
   CKR(ensure_buf(c, c->sort_status, ((sort_items + kSortPart - 1) / kSortPart + 1) * 256 * 8));
   CKR(ensure_buf(c, c->scan_status, ((items + 255) / 256 + 2) * 8));
   CKR(ensure_buf(c, c->ranges, (uint64_t)std::max<uint32_t>(total_tiles, 1) * 8));
+  CKR(ensure_buf(c, c->tile_order, (uint64_t)std::max<uint32_t>(total_tiles, 1) * 4));
+  CKR(ensure_buf(c, c->order_hist, 2 * kOrderBuckets * 4));
   CKR(ensure_buf(c, c->rgba, std::max<uint64_t>(total_pixels, 1) * 16));
   return RMESH_OK;
 }
@@ -452,6 +455,15 @@ int run_bin(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t tota
     ranges_kernel<<<std::max(1, blocks), 256, 0, c->stream>>>(c->sorted_pair_key, &cnt->n_pairs, c->cap_pairs,
                                                                c->ranges.as<uint2>(), views_dev, n_views, cnt);
     CKL();
+    // longest-first order of the tiles for the persistent tile kernel
+    CK(cudaMemsetAsync(c->order_hist.p, 0, 2 * kOrderBuckets * 4, c->stream));
+    uint32_t* hist = c->order_hist.as<uint32_t>();
+    const int oblocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((total_tiles + 255) / 256, (uint64_t)c->num_sms * 2));
+    tile_order_hist_kernel<<<oblocks, 256, 0, c->stream>>>(c->ranges.as<uint2>(), total_tiles, hist);
+    CKL();
+    tile_order_scatter_kernel<<<oblocks, 256, 0, c->stream>>>(c->ranges.as<uint2>(), total_tiles, hist,
+                                                              hist + kOrderBuckets, c->tile_order.as<uint32_t>());
+    CKL();
   }
   return RMESH_OK;
 }
@@ -513,6 +525,7 @@ TileArgs base_tile_args(RmeshCtx* c, const ViewParams* views_dev, int n_views, u
   }
   ta.counters = cnt;
   ta.hp = c->hp_d.as<AdamParams>();
+  ta.tile_order = c->tile_order.as<uint32_t>();
   return ta;
 }
 

@@ -108,6 +108,48 @@ __global__ void __launch_bounds__(256) emit_kernel(EmitArgs a) {
   if (overflow) atomicOr(&a.counters->err, kErrPairOverflow);
 }
 
+// Longest-first tile order for the persistent tile kernel: a tile's cost
+// grows with its list length, and a long list taken last leaves the other
+// CTAs idle, so tiles are bucketed by floor(log2(length)) and the buckets are
+// handed out from the longest down (order within a bucket is arbitrary; every
+// tile's result is independent of the order).
+constexpr int kOrderBuckets = 33;  // 0: empty list; 1 + floor(log2(length)) otherwise
+__device__ __forceinline__ int order_bucket(uint2 r) {
+  const uint32_t len = r.y > r.x ? r.y - r.x : 0u;
+  return len ? 32 - __clz(len) : 0;
+}
+
+__global__ void __launch_bounds__(256) tile_order_hist_kernel(const uint2* __restrict__ ranges, uint32_t n_tiles,
+                                                              uint32_t* hist) {
+  __shared__ uint32_t sh[kOrderBuckets];
+  for (int i = threadIdx.x; i < kOrderBuckets; i += blockDim.x) sh[i] = 0u;
+  __syncthreads();
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n_tiles; t += gridDim.x * blockDim.x)
+    atomicAdd(&sh[order_bucket(ranges[t])], 1u);
+  __syncthreads();
+  for (int i = threadIdx.x; i < kOrderBuckets; i += blockDim.x)
+    if (sh[i]) atomicAdd(&hist[i], sh[i]);
+}
+
+// order[pos] = tile, bucket by bucket from the longest lists down
+__global__ void __launch_bounds__(256) tile_order_scatter_kernel(const uint2* __restrict__ ranges, uint32_t n_tiles,
+                                                                 const uint32_t* hist, uint32_t* cursor,
+                                                                 uint32_t* order) {
+  __shared__ uint32_t start[kOrderBuckets];
+  if (threadIdx.x == 0) {
+    uint32_t acc = 0u;
+    for (int b = kOrderBuckets - 1; b >= 0; --b) {
+      start[b] = acc;
+      acc += hist[b];
+    }
+  }
+  __syncthreads();
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n_tiles; t += gridDim.x * blockDim.x) {
+    const int b = order_bucket(ranges[t]);
+    order[start[b] + atomicAdd(&cursor[b], 1u)] = t;
+  }
+}
+
 // Per-tile [start, end) over the sorted pair keys.  Restates
 // tile_ranges_compute.wgsl:10-45 per view: the end of a view's last non-empty
 // tile is only written when the view had no sentinel slots (in the reference

@@ -87,6 +87,8 @@ struct TileArgs {
   // pass of the same tile; nullptr disables it
   short2* span_cache;
   uint32_t span_cache_tets;
+  // persistent launches: ticket -> tile (longest lists first); nullptr = identity
+  const uint32_t* tile_order;
 };
 
 template <int TS, bool AUX>
@@ -232,7 +234,15 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
                              : nullptr;
   const uint32_t first_tile = blockIdx.x;
   while (true) {
-    if (tid == 0) s.tile = a.persistent ? atomicAdd(&a.counters->tile_ticket, 1u) : first_tile;
+    if (tid == 0) {
+      uint32_t t = first_tile;
+      if (a.persistent) {
+        t = atomicAdd(&a.counters->tile_ticket, 1u);
+        if (a.tile_order && t < a.n_tiles) t = a.tile_order[t];
+        else if (t >= a.n_tiles) t = 0xFFFFFFFFu;
+      }
+      s.tile = t;
+    }
     __syncthreads();
     const uint32_t g = s.tile;
     if (g >= a.n_tiles || failed) break;
