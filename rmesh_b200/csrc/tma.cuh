@@ -1,8 +1,8 @@
 // mbarrier + TMA bulk-copy helpers (sm_90+ PTX, used on sm_100a).
 //
 // Only the plain, CTA-local form of cp.async.bulk is used: global -> this
-// CTA's shared memory, completion counted on a local mbarrier.  No cluster
-// multicast anywhere.  Sources are 16-byte aligned and sizes are multiples
+// CTA's shared memory, completion counted on a local mbarrier; every copy
+// reads this GPU's own memory.  Sources are 16-byte aligned and sizes are multiples
 // of 16 bytes (144-byte per-view tet records, span-cache rows of 32/48/64
 // bytes per tet).
 #pragma once
