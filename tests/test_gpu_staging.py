@@ -79,3 +79,32 @@ def test_staged_targets_train_like_device_targets():
     torch.cuda.synchronize()
     ra.close()
     rb.close()
+
+
+def test_graph_cache_evicts_and_recaptures(c1_scene):
+    """Ten device target buffers cycled through graph-mode steps: more
+    signatures than the cache keeps (eight), so graphs are evicted and captured
+    again; every step's losses and the final parameters equal batched mode's."""
+    import torch
+
+    from conftest import make_renderer, rel_l2
+
+    from rmesh_b200.camera import orbit_cameras
+
+    cams = orbit_cameras(2, seed=41, radius=(2.6, 3.4), resolutions=((96, 80), (64, 64)))
+    n = sum(3 * c.width * c.height for c in cams)
+    rng = np.random.default_rng(42)
+    bufs = [torch.from_numpy(rng.uniform(0, 1, n).astype(np.float32)).cuda() for _ in range(10)]
+    lr = dict(lr_verts=1e-4, lr_dens=1e-2, lr_grads=1e-3, loss_type=1)
+    rg = make_renderer(c1_scene, cams[0])
+    rb = make_renderer(c1_scene, cams[0])
+    for i in range(23):
+        gt = bufs[(3 * i) % 10]
+        lg = rg.train_step_views(cams, gt, mode="graph", **lr)
+        lb = rb.train_step_views(cams, gt, mode="batched", **lr)
+        np.testing.assert_allclose(lg, lb, rtol=1e-4, err_msg=str(i))
+    pg, pb = rg.get_params(), rb.get_params()
+    for k in pg:
+        assert rel_l2(pg[k], pb[k]) <= 1e-3, k
+    rg.close()
+    rb.close()
