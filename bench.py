@@ -541,7 +541,11 @@ def run_training(args):
                      "heldout_l1_before": fin(before), "heldout_l1_after": fin(after),
                      "e2e_trajectory_max_rel_diff_before_divergence":
                          fin(np.max(np.abs(losses_e2e[:n_ok] - losses[:n_ok]) / losses[:n_ok])),
-                     "loss_every_25": [fin(x) for x in losses[::25]]},
+                     "loss_every_25": [fin(x) for x in losses[::25]],
+                     "note": "at lr_verts 1e-4 the loop diverges in the reference algorithm itself: vertex steps "
+                             "flatten tets of the densest component, and a ray through a flat tet with no exit "
+                             "face keeps t_max = 3.4e38, so its colour runs to the 1e20 clip (the oracle gives "
+                             "the same pixels); --lr-verts 0 converges"},
     }
     if not args.no_cpu_baseline:
         trng = np.random.default_rng(args.seed + 3)
