@@ -393,6 +393,35 @@ def cpu_baseline(scene, cams, gts, args, budget_s=20.0):
             "mpix_per_s": round(px_done / dt / 1e6, 4)}
 
 
+def run_profile_step(args):
+    """For profiler captures (ncu --profile-from-start off): the default
+    workload's batched step, three times unprofiled, then once between
+    cudaProfilerStart and cudaProfilerStop.  Prints the step's counts."""
+    import torch
+
+    from rmesh_b200 import RMeshRenderer
+
+    torch.cuda.set_device(0)
+    scene, cams, gts = build_workload(args.points, args.seed, 0, args.views, args.res, args.sh_degree, args.cloud)
+    sh_kw = dict(sh_coeffs=scene["sh_coeffs"], sh_degree=args.sh_degree) if args.sh_degree >= 0 else {}
+    r = RMeshRenderer(scene["vertices"], scene["indices"], scene["base_colors"], scene["densities"],
+                      scene["color_grads"], scene["circumdata"], cams[0].width, cams[0].height,
+                      tile_size=args.tile_size, **sh_kw)
+    gt = torch.from_numpy(np.concatenate([g.ravel() for g in gts])).cuda()
+    lr_sh = LR_SH if args.sh_degree >= 0 else 0.0
+    for _ in range(3):
+        r.train_step_views(cams, gt, loss_type=1, mode="batched", lr_sh=lr_sh, **LR)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.start()
+    r.train_step_views(cams, gt, loss_type=1, mode="batched", lr_sh=lr_sh, **LR)
+    torch.cuda.synchronize()
+    torch.cuda.profiler.stop()
+    inf = r.info()
+    print(json.dumps({"n_visible": int(inf.n_visible_last), "n_pairs": int(inf.n_pairs_last), "n_tets": r.n_tets,
+                      "n_vertices": r.n_vertices, "pixels": sum(c.width * c.height for c in cams)}), flush=True)
+    r.close()
+
+
 def run_training(args):
     """The training loop: the teacher renders the targets on the GPU, then a
     fresh student renderer takes ``args.steps`` graph-replayed Adam steps of
@@ -617,6 +646,8 @@ def main():
                          "1080p; training: 250k-point teacher/student loop, 8 of 32 800^2 views per step, 500 steps")
     ap.add_argument("--targets", type=int, default=32, help="target views of the training loop")
     ap.add_argument("--lr-verts", type=float, default=None, help="training loop: vertex learning rate (1e-4)")
+    ap.add_argument("--profile-one-step", action="store_true",
+                    help="run one batched step of the workload between cudaProfilerStart/Stop (for ncu) and exit")
     ap.add_argument("--points", type=int, default=None)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--tile-size", type=int, default=12)
@@ -649,7 +680,9 @@ def main():
         args.cloud = "gmm"
     args.res = RES if args.res is None else tuple(tuple(int(v) for v in x.split("x")) for x in args.res.split(","))
     args.warmup = max(3, args.warmup)
-    if args.impl == "reference":
+    if args.profile_one_step:
+        run_profile_step(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.workload == "training":
         run_training(args)
