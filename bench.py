@@ -603,26 +603,29 @@ def run_reference(args):
 
     o = Oracle("f32")
     threads = o.max_threads
-    cam = min(cams, key=lambda c: c.width * c.height)
-    gt = gts[cams.index(cam)]
-
     shv, deg = _oracle_sh(o, scene, args)
 
-    def one():
+    def one(i):
+        """Forward, loss and adjoint of the step's i-th view (cycling); returns its pixels."""
+        cam, gt = cams[i % len(cams)], gts[i % len(cams)]
         fwd = o.forward_tiled(scene, cam, args.tile_size, sh=shv, sh_degree=deg)
         _, dl = o.loss(fwd["image"], gt, 1)
         o.backward(scene, cam, dl, fwd, args.tile_size, threads=threads, sh=shv, sh_degree=deg)
+        return cam.width * cam.height
 
+    smallest = min(range(len(cams)), key=lambda i: cams[i].width * cams[i].height)
     for _ in range(args.warmup):
-        one()
+        one(smallest)
+    # each timed step is one view of the step's views in turn, so the sample
+    # covers the resolution mix; the time scales by the pixels processed
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        one()
-    dt = (time.perf_counter() - t0) / args.steps
-    t_step = dt * n_pix / (cam.width * cam.height)
+    px = sum(one(i) for i in range(args.steps))
+    dt = time.perf_counter() - t0
+    t_step = dt * n_pix / px
     v = round(1.0 / t_step, 6)
-    sample = (f"one {cam.width}x{cam.height} view per step ({cam.width * cam.height} px), scaled by pixels to the "
-              f"{n_pix}-px {args.views}-view step; C port of the reference kernels, OpenMP {threads} threads")
+    sample = (f"{args.steps} views taken in turn from the step's {len(cams)} ({px} px in {dt:.1f} s), scaled by "
+              f"pixels to the {n_pix}-px {args.views}-view step; C port of the reference kernels, "
+              f"OpenMP {threads} threads")
     print(json.dumps({
         "impl": "reference", "metric": metric_name(args),
         "value": v, "unit": "train-steps/s", "n_gpus": int(os.environ.get("WORLD_SIZE", "1")), "steps": args.steps,
