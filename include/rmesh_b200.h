@@ -157,6 +157,15 @@ RMESH_API int rmesh_set_lr_sh(RmeshCtx* ctx, float lr_sh);
  * rgba_out [H][W][4]; aux_out [H][W][8 + aux_dim] or NULL (render_aux). */
 RMESH_API int rmesh_forward_tiled(RmeshCtx* ctx, const RmeshCamera* cam, float* rgba_out, float* aux_out);
 
+/* Batched forward (no reference counterpart; the forward half of
+ * rmesh_train_step_views): n_views cameras of any sizes rendered by one
+ * persistent launch.  rgba_out receives the views' [H][W][4] images back to
+ * back, aux_out (optional) their [H][W][8 + aux_dim] aux images back to back.
+ * Images equal rmesh_forward_tiled's per view.  rmesh_backward does not
+ * follow this call (it follows a single-view rmesh_forward_tiled). */
+RMESH_API int rmesh_forward_views(RmeshCtx* ctx, const RmeshCamera* cams, int32_t n_views, float* rgba_out,
+                                  float* aux_out);
+
 /* backward, lib.rs:1894-2031: must follow rmesh_forward_tiled on the same context;
  * reuses that call's sorted tile lists and image.  Outputs (any may be NULL):
  * d_vertices [3N], d_densities [M], d_base_colors [3M], d_color_grads [3M]. */

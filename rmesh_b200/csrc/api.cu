@@ -1063,6 +1063,52 @@ int rmesh_get_info(RmeshCtx* c, RmeshInfo* info) {
   return RMESH_OK;
 }
 
+int rmesh_forward_views(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views, float* rgba_out, float* aux_out) {
+  if (!c || !cams || !rgba_out) return RMESH_ERR_INVALID_ARG;
+  if (n_views <= 0 || n_views > kMaxViews) return fail(c, RMESH_ERR_INVALID_ARG, "n_views out of range");
+  uint64_t total_pix = 0;
+  uint32_t total_tiles = 0;
+  for (int v = 0; v < n_views; ++v) {
+    CKR(fill_view(c, cams[v], c->views_h[v], total_tiles, (uint32_t)total_pix));
+    total_tiles += (uint32_t)(c->views_h[v].tiles_x * c->views_h[v].tiles_y);
+    total_pix += (uint64_t)cams[v].width * cams[v].height;
+  }
+  const uint64_t aux_floats = total_pix * (8 + (uint64_t)c->aux_dim);
+  for (int attempt = 0; attempt < 4; ++attempt) {
+    CKR(ensure_run_buffers(c, n_views, total_pix, total_tiles));
+    if (aux_out) CKR(ensure_buf(c, c->aux, aux_floats * 4));
+    CKR(upload_views(c, n_views));
+    Counters* cnt = c->counters_d.as<Counters>();
+    CK(cudaMemsetAsync(cnt, 0, sizeof(Counters), c->stream));
+    CKR(run_records(c, false));
+    ViewParams* vd = c->views_d.as<ViewParams>();
+    CKR(run_bin(c, vd, n_views, total_tiles, cnt, false));
+    {
+      StageScope sc(c, kStComposite, false);
+      TileArgs ta = base_tile_args(c, vd, n_views, total_tiles, cnt);
+      ta.rgba = c->rgba.as<float>();
+      if (aux_out) {
+        ta.aux = c->aux.as<float>();
+        ta.aux_data = c->aux_data.as<float>();
+        ta.aux_dim = c->aux_dim;
+        CKR((launch_tile_m<kModeForward, true>(c, ta, total_tiles, true)));
+      } else {
+        CKR((launch_tile_m<kModeForward, false>(c, ta, total_tiles, true)));
+      }
+    }
+    CKR(sync_counters(c, 1));
+    if ((c->last_err_bits & kErrPairOverflow) && grow_pairs(c)) continue;
+    CKR(status_from_bits(c));
+    CK(cudaMemcpyAsync(rgba_out, c->rgba.p, total_pix * 16, cudaMemcpyDefault, c->stream));
+    if (aux_out) CK(cudaMemcpyAsync(aux_out, c->aux.p, aux_floats * 4, cudaMemcpyDefault, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_forward = false;
+    c->last_views = n_views;
+    return RMESH_OK;
+  }
+  return fail(c, RMESH_ERR_PAIR_OVERFLOW, "pair buffers could not be grown enough");
+}
+
 int rmesh_forward_tiled(RmeshCtx* c, const RmeshCamera* cam, float* rgba_out, float* aux_out) {
   if (!c || !cam || !rgba_out) return RMESH_ERR_INVALID_ARG;
   const uint64_t npix = (uint64_t)cam->width * cam->height;

@@ -402,6 +402,31 @@ class RMeshRenderer:
         o.mode = {"plain": _lib.MODE_PLAIN, "batched": _lib.MODE_BATCHED, "graph": _lib.MODE_GRAPH}[mode]
         return n, cams, obj, p, o
 
+    def forward_views(self, cameras: Sequence, render_aux: bool = False):
+        """Renders several cameras (``rmesh_b200.camera.Camera`` objects, any
+        sizes) in one batched launch.  Returns a list of [H, W, 4] images (and
+        a list of [H, W, 8 + aux_dim] aux images when ``render_aux``), each
+        equal to ``forward_tiled``'s for that camera."""
+        n = len(cameras)
+        cams = (_lib.Camera * n)()
+        sizes = []
+        for i, c in enumerate(cameras):
+            cams[i] = _camera_struct(c.cam_pos, c.vp, c.c2w_intrinsics, c.width, c.height)
+            sizes.append((int(c.height), int(c.width)))
+        total = sum(h * w for h, w in sizes)
+        na = 8 + self._aux_dim
+        rgba = np.empty(total * 4, np.float32)
+        aux = np.empty(total * na, np.float32) if render_aux else None
+        self._check(self._lib.rmesh_forward_views(self._ctx, cams, n, rgba.ctypes.data,
+                                                  aux.ctypes.data if render_aux else None))
+        imgs, auxs, o = [], [], 0
+        for h, w in sizes:
+            imgs.append(rgba[4 * o:4 * (o + h * w)].reshape(h, w, 4))
+            if render_aux:
+                auxs.append(aux[na * o:na * (o + h * w)].reshape(h, w, na))
+            o += h * w
+        return (imgs, auxs) if render_aux else imgs
+
     def train_step_views(self, cameras: Sequence, gt_images, lr_verts: float, lr_dens: float, lr_grads: float,
                          loss_type: int = 1, lr_base: float = 0.0, mode: str = "graph",
                          lr_sh: float = 0.0) -> np.ndarray:

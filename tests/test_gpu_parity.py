@@ -288,3 +288,22 @@ def test_l1_loss_steps_match_oracle(c1_scene):
         lg = rv.train_step_views(cams, gts, 1e-4, 1e-2, 1e-3, 0, mode="graph")
         lo = tv.train_step_views(cams, gts, 1e-4, 1e-2, 1e-3, 0)
         np.testing.assert_allclose(lg, lo, rtol=1e-4, err_msg=str(step))
+
+
+def test_forward_views_equals_single_view_forwards(c1_scene):
+    """rmesh_forward_views: three cameras of different sizes in one batched
+    launch give, bit for bit, the images (and aux images) of three
+    single-view forwards."""
+    from rmesh_b200.camera import orbit_cameras
+
+    cams = orbit_cameras(3, seed=51, radius=(2.6, 3.4), resolutions=((96, 96), (128, 80), (64, 72)))
+    r = make_renderer(c1_scene, cams[0])
+    imgs, auxs = r.forward_views(cams, render_aux=True)
+    for c, img, aux in zip(cams, imgs, auxs):
+        rc = make_renderer(c1_scene, c)
+        want, want_aux = rc.forward_tiled(c.cam_pos, c.vp, c.c2w_intrinsics, render_aux=True)
+        np.testing.assert_array_equal(img, want)
+        np.testing.assert_array_equal(aux, want_aux)
+        rc.close()
+    assert r.forward_views(cams[:1])[0].shape == (cams[0].height, cams[0].width, 4)
+    r.close()
