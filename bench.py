@@ -267,6 +267,27 @@ def run_gpu(args):
     ms_plain = timed("plain", gt_dev, max(1, args.steps // 2))
     r.stage_times()
 
+    # render only: the batched forward of the same views into a device buffer
+    # (rmesh_forward_views), device-timed
+    fwd_ms = None
+    if dist is None:
+        out_dev = torch.empty(n_pix * 4, dtype=torch.float32, device=f"cuda:{local}")
+
+        def fwd():
+            r.forward_views(cams, out=out_dev)
+
+        for _ in range(2):
+            fwd()
+        torch.cuda.synchronize()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(5):
+            fwd()
+        f1.record(stream)
+        f1.synchronize()
+        fwd_ms = f0.elapsed_time(f1) / 5
+
     # per-stage device times of the batched path (CUDA events on the library stream)
     r.set_profiling(True)
     for _ in range(max(1, args.steps // 2)):
@@ -299,6 +320,9 @@ def run_gpu(args):
         "mpix_per_s": round(world * n_pix / (ms_graph * 1e-3) / 1e6, 2),
         "plain": {"value": round(world * 1000.0 / ms_plain, 4), "unit": "train-steps/s", "ms_per_step": round(ms_plain, 4)},
         "batched_graph_vs_plain": round(ms_plain / ms_graph, 3),
+        "forward_only": None if fwd_ms is None else {
+            "ms_per_render": round(fwd_ms, 4), "mpix_per_s": round(n_pix / (fwd_ms * 1e-3) / 1e6, 2),
+            "what": "batched forward of the same views (rmesh_forward_views) into device memory"},
         "e2e": {"value": round(world * 1000.0 / ms_e2e, 4), "unit": "train-steps/s",
                 "h2d_bytes_per_step": int(n_pix * 12 + args.views * 160 + 48),
                 "d2h_bytes_per_step": int(_lib.COUNTERS_BYTES)},

@@ -402,11 +402,13 @@ class RMeshRenderer:
         o.mode = {"plain": _lib.MODE_PLAIN, "batched": _lib.MODE_BATCHED, "graph": _lib.MODE_GRAPH}[mode]
         return n, cams, obj, p, o
 
-    def forward_views(self, cameras: Sequence, render_aux: bool = False):
+    def forward_views(self, cameras: Sequence, render_aux: bool = False, out=None):
         """Renders several cameras (``rmesh_b200.camera.Camera`` objects, any
         sizes) in one batched launch.  Returns a list of [H, W, 4] images (and
         a list of [H, W, 8 + aux_dim] aux images when ``render_aux``), each
-        equal to ``forward_tiled``'s for that camera."""
+        equal to ``forward_tiled``'s for that camera.  With ``out`` (a float32
+        CUDA tensor of 4 x the cameras' total pixels) the images are written
+        there back to back, without a host copy, and ``out`` is returned."""
         n = len(cameras)
         cams = (_lib.Camera * n)()
         sizes = []
@@ -414,6 +416,14 @@ class RMeshRenderer:
             cams[i] = _camera_struct(c.cam_pos, c.vp, c.c2w_intrinsics, c.width, c.height)
             sizes.append((int(c.height), int(c.width)))
         total = sum(h * w for h, w in sizes)
+        if out is not None:
+            if render_aux:
+                raise ValueError("out= writes the RGBA images only")
+            if not (_is_torch(out) and out.is_cuda and out.dtype.is_floating_point and out.element_size() == 4
+                    and out.is_contiguous() and out.numel() == 4 * total):
+                raise ValueError(f"out must be a contiguous float32 CUDA tensor of {4 * total} values")
+            self._check(self._lib.rmesh_forward_views(self._ctx, cams, n, out.data_ptr(), None))
+            return out
         na = 8 + self._aux_dim
         rgba = np.empty(total * 4, np.float32)
         aux = np.empty(total * na, np.float32) if render_aux else None

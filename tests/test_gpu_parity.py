@@ -306,4 +306,9 @@ def test_forward_views_equals_single_view_forwards(c1_scene):
         np.testing.assert_array_equal(aux, want_aux)
         rc.close()
     assert r.forward_views(cams[:1])[0].shape == (cams[0].height, cams[0].width, 4)
+    import torch
+
+    out = torch.empty(4 * sum(c.width * c.height for c in cams), dtype=torch.float32, device="cuda")
+    r.forward_views(cams, out=out)
+    np.testing.assert_array_equal(out.cpu().numpy(), np.concatenate([i.ravel() for i in imgs]))
     r.close()
