@@ -100,7 +100,7 @@ typedef struct {
 
 #define RMESH_MODE_PLAIN 0    /* one launch sequence per view, one tile per CTA */
 #define RMESH_MODE_BATCHED 1  /* all views in one launch sequence, persistent (view,tile) queue */
-#define RMESH_MODE_GRAPH 2    /* BATCHED, captured once as a CUDA graph and replayed */
+#define RMESH_MODE_GRAPH 2    /* BATCHED, captured as a CUDA graph per step signature (up to 8 kept) and replayed */
 
 typedef struct {
   int64_t n_vertices, n_tets;
