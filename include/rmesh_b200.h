@@ -135,6 +135,19 @@ RMESH_API int rmesh_get_params(RmeshCtx* ctx, float* vertices, float* base_color
 /* getters step/width/height, lib.rs:2688-2705 */
 RMESH_API int rmesh_get_info(RmeshCtx* ctx, RmeshInfo* info);
 
+/* Optimiser state for checkpoints (no reference counterpart: the reference
+ * keeps its Adam moments private).  The state is the first and second Adam
+ * moments of every group back to back -- m and v of the vertices [3N], the
+ * densities [M], the colour gradients [3M], the base colours [3M] and, in SH
+ * contexts, the SH coefficients [3 nc M] -- plus the step count that drives
+ * the bias correction.  rmesh_adam_state_size gives the length in floats;
+ * state may be host or device memory.  With rmesh_get_params /
+ * rmesh_update_params (and rmesh_get_sh / rmesh_update_sh) a run restored
+ * from them continues as the saved one would. */
+RMESH_API int rmesh_adam_state_size(RmeshCtx* ctx, uint64_t* n_floats);
+RMESH_API int rmesh_get_adam_state(RmeshCtx* ctx, float* state, uint32_t* step);
+RMESH_API int rmesh_set_adam_state(RmeshCtx* ctx, const float* state, uint32_t step);
+
 /* set_aux_data / get_aux_data, lib.rs:892-921: the [M][aux_dim] custom
  * per-tet channels that forward_tiled's aux output composites after its eight
  * fixed channels (aux_out [H][W][8 + aux_dim]); zeros until set. */

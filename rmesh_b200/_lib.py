@@ -32,7 +32,8 @@ STAGE_NAMES = ("records", "project", "tet_sort", "emit", "pair_sort", "ranges", 
 EXPORTED = (
     "rmesh_create", "rmesh_destroy", "rmesh_last_error", "rmesh_abi_version", "rmesh_set_stream",
     "rmesh_set_min_t", "rmesh_set_tile_size", "rmesh_update_params", "rmesh_get_params", "rmesh_get_info",
-    "rmesh_forward_tiled", "rmesh_forward_views", "rmesh_backward", "rmesh_train_step", "rmesh_train_step_views",
+    "rmesh_forward_tiled", "rmesh_forward_views", "rmesh_backward",
+    "rmesh_adam_state_size", "rmesh_get_adam_state", "rmesh_set_adam_state", "rmesh_train_step", "rmesh_train_step_views",
     "rmesh_debug_tiles_touched", "rmesh_debug_pairs", "rmesh_debug_ranges", "rmesh_set_profiling",
     "rmesh_stage_times", "rmesh_accumulate_views", "rmesh_grad_slots", "rmesh_apply_adam",
     "rmesh_count_tiles_static", "rmesh_update_sh", "rmesh_get_sh", "rmesh_get_sh_grad", "rmesh_set_lr_sh",
@@ -115,6 +116,9 @@ def load() -> ctypes.CDLL:
         "rmesh_get_info": ([vp, P(Info)], ctypes.c_int),
         "rmesh_forward_tiled": ([vp, P(Camera), vp, vp], ctypes.c_int),
         "rmesh_forward_views": ([vp, P(Camera), i32, vp, vp], ctypes.c_int),
+        "rmesh_adam_state_size": ([vp, P(ctypes.c_uint64)], ctypes.c_int),
+        "rmesh_get_adam_state": ([vp, vp, P(ctypes.c_uint32)], ctypes.c_int),
+        "rmesh_set_adam_state": ([vp, vp, ctypes.c_uint32], ctypes.c_int),
         "rmesh_backward": ([vp, vp, vp, vp, vp, vp], ctypes.c_int),
         "rmesh_train_step": ([vp, P(Camera), vp, f32, f32, f32, i32, vp], ctypes.c_int),
         "rmesh_train_step_views": ([vp, P(Camera), i32, vp, P(TrainOpts), vp], ctypes.c_int),

@@ -1063,6 +1063,52 @@ int rmesh_get_info(RmeshCtx* c, RmeshInfo* info) {
   return RMESH_OK;
 }
 
+// the Adam moment buffers in checkpoint order, with their lengths in floats
+static std::vector<std::pair<DevBuf*, uint64_t>> adam_state_parts(RmeshCtx* c) {
+  const uint64_t N = (uint64_t)c->N, M = (uint64_t)c->M;
+  std::vector<std::pair<DevBuf*, uint64_t>> parts = {
+      {&c->m_verts, 3 * N}, {&c->v_verts, 3 * N}, {&c->m_dens, M},     {&c->v_dens, M},
+      {&c->m_cgrad, 3 * M}, {&c->v_cgrad, 3 * M}, {&c->m_base, 3 * M}, {&c->v_base, 3 * M}};
+  if (c->sh_degree >= 0) {
+    const uint64_t n_sh = 3 * (uint64_t)c->sh_nc * M;
+    parts.push_back({&c->m_sh, n_sh});
+    parts.push_back({&c->v_sh, n_sh});
+  }
+  return parts;
+}
+
+int rmesh_adam_state_size(RmeshCtx* c, uint64_t* n_floats) {
+  if (!c || !n_floats) return RMESH_ERR_INVALID_ARG;
+  uint64_t n = 0;
+  for (auto& p : adam_state_parts(c)) n += p.second;
+  *n_floats = n;
+  return RMESH_OK;
+}
+
+int rmesh_get_adam_state(RmeshCtx* c, float* state, uint32_t* step) {
+  if (!c || !state) return RMESH_ERR_INVALID_ARG;
+  uint64_t off = 0;
+  for (auto& p : adam_state_parts(c)) {
+    CK(cudaMemcpyAsync(state + off, p.first->p, p.second * 4, cudaMemcpyDefault, c->stream));
+    off += p.second;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  if (step) *step = c->step;
+  return RMESH_OK;
+}
+
+int rmesh_set_adam_state(RmeshCtx* c, const float* state, uint32_t step) {
+  if (!c || !state) return RMESH_ERR_INVALID_ARG;
+  uint64_t off = 0;
+  for (auto& p : adam_state_parts(c)) {
+    CK(cudaMemcpyAsync(p.first->p, state + off, p.second * 4, cudaMemcpyDefault, c->stream));
+    off += p.second;
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  c->step = step;
+  return RMESH_OK;
+}
+
 int rmesh_forward_views(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views, float* rgba_out, float* aux_out) {
   if (!c || !cams || !rgba_out) return RMESH_ERR_INVALID_ARG;
   if (n_views <= 0 || n_views > kMaxViews) return fail(c, RMESH_ERR_INVALID_ARG, "n_views out of range");

@@ -282,6 +282,30 @@ class RMeshRenderer:
             self._check(self._lib.rmesh_get_sh(self._ctx, out["sh_coeffs"].ctypes.data))
         return out
 
+    def state_dict(self) -> dict:
+        """Checkpoint: parameters (as ``get_params``), the Adam moments of
+        every group (one float32 array, see ``rmesh_get_adam_state``) and the
+        step count.  No reference counterpart (its Adam state is private)."""
+        n = ctypes.c_uint64()
+        self._check(self._lib.rmesh_adam_state_size(self._ctx, ctypes.byref(n)))
+        adam = np.empty(int(n.value), np.float32)
+        step = ctypes.c_uint32()
+        self._check(self._lib.rmesh_get_adam_state(self._ctx, adam.ctypes.data, ctypes.byref(step)))
+        return {"params": self.get_params(), "adam": adam, "step": int(step.value)}
+
+    def load_state_dict(self, state: dict):
+        """Restores a ``state_dict`` of a renderer over the same mesh; training
+        then continues as it would have from the saved state."""
+        p = state["params"]
+        self.update_params(p["vertices"], p["base_colors"], p["densities"], p["color_grads"],
+                           sh_coeffs=p.get("sh_coeffs"))
+        n = ctypes.c_uint64()
+        self._check(self._lib.rmesh_adam_state_size(self._ctx, ctypes.byref(n)))
+        adam = np.ascontiguousarray(state["adam"], dtype=np.float32)
+        if adam.size != int(n.value):
+            raise ValueError(f"adam state must hold {int(n.value)} floats, got {adam.size}")
+        self._check(self._lib.rmesh_set_adam_state(self._ctx, adam.ctypes.data, int(state["step"])))
+
     def sh_grad_into(self, out):
         """Coefficient gradient of the last backward / training call into ``out``."""
         _, p = _as_array(out, np.float32, "out")
