@@ -11,6 +11,7 @@
 // device bit, Adam is skipped on the device, and the host grows the buffers to
 // the exact count and repeats the call.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <mutex>
@@ -68,6 +69,11 @@ struct DevBuf {
 };
 
 enum Stage { kStRecords = 0, kStProject, kStTetSort, kStEmit, kStPairSort, kStRanges, kStComposite, kStAdam, kStShAdjoint };
+// NVTX range names of the stages (profilers can select kernels by them, e.g.
+// ncu --nvtx --nvtx-include "rmesh/composite/")
+const char* const kStageRange[] = {"rmesh/records",   "rmesh/project", "rmesh/tet_sort",
+                                   "rmesh/emit",      "rmesh/pair_sort", "rmesh/ranges",
+                                   "rmesh/composite", "rmesh/adam",    "rmesh/sh_adjoint"};
 
 struct EventPair {
   int stage;
@@ -193,7 +199,12 @@ struct StageScope {
   RmeshCtx* c;
   int stage;
   cudaEvent_t a = nullptr;
+  bool ranged = false;
   StageScope(RmeshCtx* c_, int s, bool capturing) : c(c_), stage(s) {
+    if (!capturing) {  // host-side range around the stage's launches
+      nvtxRangePushA(kStageRange[s]);
+      ranged = true;
+    }
     if (c->profiling && !capturing) {
       a = take_event(c);
       cudaEventRecord(a, c->stream);
@@ -205,6 +216,7 @@ struct StageScope {
       cudaEventRecord(b, c->stream);
       c->events.push_back({stage, a, b});
     }
+    if (ranged) nvtxRangePop();
   }
 };
 
