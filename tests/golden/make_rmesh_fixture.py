@@ -1,4 +1,4 @@
-"""Writes tests/golden/small_deg3.rmesh with the reference's own .rmesh writer.
+"""Writes tests/golden/small_deg{1,2,3}.rmesh with the reference's own .rmesh writer.
 
 Run from the repository root with the reference checkout available:
 ``python tests/golden/make_rmesh_fixture.py /path/to/rmeshvk``.
@@ -9,10 +9,12 @@ compresses the SH coefficients (k = 12), log-encodes densities to u8 and
 stores colour gradients as f16.  Its two third-party imports (tinyplypy,
 pyquaternion) are not installed here; they are replaced by stand-ins that hand
 the writer an in-memory PLY dictionary built from a seeded synthetic scene.
-The fixture also keeps the writer's inputs and its PCA factors
-(small_deg3_inputs.npz: geometry, densities, colour gradients and the PCA
+Each fixture also keeps the writer's inputs and its PCA factors
+(small_deg<d>_inputs.npz: geometry, densities, colour gradients and the PCA
 factors) so the tests can check the decoded scene against what went into the
-file.
+file.  Degree 0 is not written: the writer's fixed k = 12 PCA components
+exceed degree 0's 3 coefficients per tet, and the header it writes then
+disagrees with the basis it stores.
 """
 import gzip
 import os
@@ -47,7 +49,7 @@ def synthetic_ply(seed=21, points=120, degree=3):
     return {"vertex": vert, "tetrahedron": tet}
 
 
-def main(reference_root):
+def main(reference_root, degree=3):
     ply = synthetic_ply()
     stub = types.ModuleType("tinyplypy")
     stub.read_ply = lambda path: ply
@@ -59,25 +61,25 @@ def main(reference_root):
     import convert  # the reference's writer
 
     cam = np.array([0.5, -2.5, 0.8, 0.0, 0.0, 0.0, 1.0, 0.0], np.float32)
-    degree = 3
     buf, mask = convert._process_ply_to_rmesh_buffer("in-memory.ply", cam, degree)
     raw = buf.getvalue()
-    with open(os.path.join(HERE, "small_deg3.rmesh"), "wb") as f:
+    with open(os.path.join(HERE, f"small_deg{degree}.rmesh"), "wb") as f:
         f.write(gzip.compress(raw, compresslevel=9, mtime=0))
     tet = ply["tetrahedron"]
     keep = ~mask
     nc = (degree + 1) ** 2
     sh = np.stack([np.stack([tet[f"sh_{i}_{ch}"] for ch in "rgb"], axis=1) for i in range(nc)], axis=1)
-    sh = np.transpose(sh, (0, 2, 1))[keep]  # [M, 3, nc], as the writer lays it out
+    sh = np.transpose(sh, (0, 2, 1))[keep]  # [M, 3, nc] of the written degree, as the writer lays it out
     w16, b16, m16 = convert.compress_matrix(sh, k=12)  # the factors the writer stored
     v = ply["vertex"]
-    np.savez_compressed(os.path.join(HERE, "small_deg3_inputs.npz"),
+    np.savez_compressed(os.path.join(HERE, f"small_deg{degree}_inputs.npz"),
                         vertices=np.stack([v["x"], v["y"], v["z"]], axis=1).astype(np.float32),
                         indices=tet["indices"][keep].astype(np.uint32), densities=tet["s"][keep],
                         color_grads=np.stack([tet["grd_x"], tet["grd_y"], tet["grd_z"]], axis=1)[keep],
                         pca_weights=w16, pca_basis=b16, pca_mean=m16, start_pose=cam)
-    print("wrote", len(raw), "bytes raw;", int(keep.sum()), "tets kept of", keep.size)
+    print(f"degree {degree}: wrote", len(raw), "bytes raw;", int(keep.sum()), "tets kept of", keep.size)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(os.sep, "root", "reference"))
+    for d in (1, 2, 3):
+        main(sys.argv[1] if len(sys.argv) > 1 else os.path.join(os.sep, "root", "reference"), d)

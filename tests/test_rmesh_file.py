@@ -1,9 +1,10 @@
 """.rmesh scene files: the oracle's decode pinned to the reference's writer,
 the host section parser, and the device decode (bit-exact vs the oracle).
 
-tests/golden/small_deg3.rmesh was written by the reference's own writer
+tests/golden/small_deg{1,2,3}.rmesh were written by the reference's own writer
 (convert.py:213-290, see tests/golden/make_rmesh_fixture.py) from a seeded
-615-tet degree-3 scene; small_deg3_inputs.npz holds what went into it.
+615-tet scene at SH degrees 1, 2 and 3; small_deg<d>_inputs.npz hold what went
+into them.
 """
 from __future__ import annotations
 
@@ -14,26 +15,38 @@ import pytest
 
 from conftest import ROOT, c1_camera
 
-FIX = os.path.join(ROOT, "tests", "golden", "small_deg3.rmesh")
-INP = os.path.join(ROOT, "tests", "golden", "small_deg3_inputs.npz")
+DEGREES = (1, 2, 3)
 
 
-def _raw():
+def _fix(deg):
+    return os.path.join(ROOT, "tests", "golden", f"small_deg{deg}.rmesh")
+
+
+def _inp(deg):
+    return os.path.join(ROOT, "tests", "golden", f"small_deg{deg}_inputs.npz")
+
+
+FIX = _fix(3)
+
+
+def _raw(deg=3):
     from rmesh_b200.rmesh_file import read_rmesh_bytes
 
-    return read_rmesh_bytes(FIX)
+    return read_rmesh_bytes(_fix(deg))
 
 
-def test_oracle_decode_matches_reference_writer(oracle32):
+@pytest.mark.parametrize("deg", DEGREES)
+def test_oracle_decode_matches_reference_writer(oracle32, deg):
     """Decoding (crates/rmesh-data/src/lib.rs:247-393) returns what the writer
     stored: exact geometry, densities within the u8 log code's step
     (exp(1/20) = 5.1 %), colour gradients within f16, SH equal to the PCA
     reconstruction of the writer's factors, circumspheres as computed here."""
     from rmesh_b200.scenes import circumspheres
 
-    d = oracle32.rmesh_decode(_raw())
-    g = np.load(INP)
-    assert d["sh_degree"] == 3
+    d = oracle32.rmesh_decode(_raw(deg))
+    g = np.load(_inp(deg))
+    assert d["sh_degree"] == deg
+    assert d["sh_coeffs"].size == 615 * 3 * (deg + 1) ** 2
     np.testing.assert_array_equal(d["vertices"], g["vertices"].ravel())
     np.testing.assert_array_equal(d["indices"], g["indices"].ravel())
     np.testing.assert_array_equal(d["start_pose"], g["start_pose"][:7])
@@ -46,17 +59,18 @@ def test_oracle_decode_matches_reference_writer(oracle32):
     np.testing.assert_array_equal(d["circumdata"], circumspheres(d["vertices"], d["indices"]))
 
 
-def test_host_sections(oracle32):
+@pytest.mark.parametrize("deg", DEGREES)
+def test_host_sections(oracle32, deg):
     from rmesh_b200.rmesh_file import parse_rmesh_sections
 
-    raw = _raw()
+    raw = _raw(deg)
     sec = parse_rmesh_sections(raw)
     d = oracle32.rmesh_decode(raw)
-    assert (sec["n_vertices"], sec["n_tets"], sec["sh_degree"], sec["k_components"]) == (120, 615, 3, 12)
+    assert (sec["n_vertices"], sec["n_tets"], sec["sh_degree"], sec["k_components"]) == (120, 615, deg, 12)
     np.testing.assert_array_equal(sec["vertices"], d["vertices"])
     np.testing.assert_array_equal(sec["indices"], d["indices"])
     np.testing.assert_array_equal(sec["color_grads_f16"].view(np.float16).astype(np.float32), d["color_grads"])
-    assert sec["sh_weights"].size == 615 * 12 and sec["sh_basis"].size == 12 * 48
+    assert sec["sh_weights"].size == 615 * 12 and sec["sh_basis"].size == 12 * 3 * (deg + 1) ** 2
 
 
 def test_truncated_and_tagged_files(oracle32):
@@ -80,30 +94,32 @@ def test_truncated_and_tagged_files(oracle32):
 
 
 @pytest.mark.gpu
-def test_device_decode_matches_oracle(oracle32):
+@pytest.mark.parametrize("deg", DEGREES)
+def test_device_decode_matches_oracle(oracle32, deg):
     from rmesh_b200.rmesh_file import load_rmesh
 
-    d = oracle32.rmesh_decode(_raw())
-    s = load_rmesh(FIX)
+    d = oracle32.rmesh_decode(_raw(deg))
+    s = load_rmesh(_fix(deg))
     for k in ("vertices", "densities", "color_grads", "circumdata", "sh_coeffs"):
         np.testing.assert_array_equal(s[k].cpu().numpy(), d[k], err_msg=k)
     np.testing.assert_array_equal(s["indices"].cpu().numpy().view(np.uint32), d["indices"])
 
 
 @pytest.mark.gpu
-def test_loaded_scene_renders_like_oracle(oracle32):
+@pytest.mark.parametrize("deg", DEGREES)
+def test_loaded_scene_renders_like_oracle(oracle32, deg):
     """A renderer built straight from the device tensors of load_rmesh."""
     from rmesh_b200 import RMeshRenderer
     from rmesh_b200.rmesh_file import load_rmesh
 
-    s = load_rmesh(FIX)
+    s = load_rmesh(_fix(deg))
     cam = c1_camera(160, 128)
     r = RMeshRenderer(s["vertices"], s["indices"], s["base_colors"], s["densities"], s["color_grads"],
                       s["circumdata"], cam.width, cam.height, sh_coeffs=s["sh_coeffs"], sh_degree=s["sh_degree"])
     img = r.forward_tiled(cam.cam_pos, cam.vp, cam.c2w_intrinsics)
-    d = oracle32.rmesh_decode(_raw())
+    d = oracle32.rmesh_decode(_raw(deg))
     scene = {k: d[k] for k in ("vertices", "indices", "densities", "color_grads", "circumdata")}
     scene["base_colors"] = s["base_colors"].cpu().numpy()
-    ref = oracle32.forward_tiled(scene, cam, sh=oracle32.sh_values(d["sh_coeffs"]), sh_degree=3)
+    ref = oracle32.forward_tiled(scene, cam, sh=oracle32.sh_values(d["sh_coeffs"]), sh_degree=deg)
     assert ref["image"][..., 3].max() > 0.1
     assert np.abs(img - ref["image"]).max() <= 1e-4
