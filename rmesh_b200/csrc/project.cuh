@@ -251,7 +251,9 @@ struct ProjectArgs {
   const ViewParams* views;
   const TetRec* rec;
   const float4* circ;
-  // compaction outputs (index j in (view, tet) order of tile-touching tets)
+  // compaction outputs, index j over the tile-touching (tet, view) items in
+  // tet-major order (within one view: ascending tet id, which is the tie
+  // order of the stable (view, depth) sort)
   unsigned long long* vis_key;  // (view << 32) | ~bits(depth)
   uint32_t* vis_val;            // j (sort payload)
   uint32_t* vis_tet;
@@ -262,12 +264,12 @@ struct ProjectArgs {
   uint32_t color_view_stride;
   // SH colours (sh != nullptr): coefficients [M][3][nc]; the colour of each
   // tile-touching entry goes to vis_color[j], and vis_index maps every item
-  // (view * M + tet) to its entry j (0xFFFFFFFF when it touches no tile)
+  // (tet * n_views + view) to its entry j (0xFFFFFFFF when it touches no tile)
   const float* sh;
   int sh_degree;
   float4* vis_color;
   uint32_t* vis_index;
-  uint32_t* tiles_touched;      // optional [n_views*M], indexed by (view, tet id)
+  uint32_t* tiles_touched;      // optional [M * n_views], indexed by tet * n_views + view
   unsigned long long* status;   // chained-scan status, one word per block (zeroed)
   uint32_t* ticket;             // block ticket (zeroed)
   Counters* counters;
@@ -289,8 +291,10 @@ __global__ void __launch_bounds__(256, 3) project_kernel(ProjectArgs a) {
   uint32_t count = 0, inv_depth = 0, view = 0, tet = 0;
   float qx[4], qy[4];
   if (i < total_items) {
-    view = (uint32_t)(i / (unsigned long long)a.M);
-    tet = (uint32_t)(i - (unsigned long long)view * a.M);
+    // items tet-major: a tet's views are neighbouring threads, so its record
+    // and SH coefficients are read once for all views
+    tet = (uint32_t)(i / (unsigned long long)a.n_views);
+    view = (uint32_t)(i - (unsigned long long)tet * a.n_views);
     const ViewParams& V = a.views[view];
     const TetRec r = a.rec[tet];
     const float vx[4] = {r.a.x, r.b.x, r.c.x, r.d.x};
