@@ -14,7 +14,6 @@ import socket
 import sys
 
 import numpy as np
-import pytest
 
 from conftest import ROOT
 
