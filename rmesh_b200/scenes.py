@@ -94,6 +94,46 @@ def make_scene(points: np.ndarray, rng: np.random.Generator, sh_degree: int = 0)
     }
 
 
+def grid_scene(grid_size: int, rng: np.random.Generator, jitter: float = 0.1) -> dict:
+    """Regular-grid tet mesh (the structure of the reference's grid_tet_scene,
+    crates/rmesh-util/src/test_util.rs:231-324): grid_size^3 vertices on the
+    unit cube, each jittered by U(-0.5, 0.5) x jitter x the cell step, and every
+    cube cell cut into the reference's five tets (A B D F, A D C G, A E F G,
+    D F G H and the central A F D G, with A..H the corners 000, 100, 010, 110,
+    001, 101, 011, 111; the renderer orients faces by the opposite vertex, so
+    vertex order does not matter); densities U(0.5, 3.5), colour gradients
+    U(-0.1, 0.1), base colours U(0.2, 0.8).  The random numbers come from
+    ``rng`` (the reference draws them from a ChaCha8 stream), so the layout
+    is the reference's and the values are seeded here.  jitter = 0 leaves
+    the faces exactly axis-aligned and coplanar across cells."""
+    n = int(grid_size)
+    step = 1.0 / (n - 1)
+    iz, iy, ix = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    base = np.stack([ix, iy, iz], axis=-1).reshape(-1, 3).astype(np.float64) * step
+    pts = base + (rng.random(base.shape) - 0.5) * (jitter * step)
+    vid = lambda x, y, z: x + y * n + z * n * n
+    cells = []
+    for z in range(n - 1):
+        for y in range(n - 1):
+            for x in range(n - 1):
+                A, B, C, D = vid(x, y, z), vid(x + 1, y, z), vid(x, y + 1, z), vid(x + 1, y + 1, z)
+                E, F, G, H = vid(x, y, z + 1), vid(x + 1, y, z + 1), vid(x, y + 1, z + 1), vid(x + 1, y + 1, z + 1)
+                cells += [A, B, D, F, A, D, C, G, A, E, F, G, D, F, G, H, A, F, D, G]
+    indices = np.asarray(cells, dtype=np.uint32)
+    m = indices.size // 4
+    vertices = np.ascontiguousarray(pts.astype(np.float32).ravel())
+    return {
+        "vertices": vertices,
+        "indices": indices,
+        "base_colors": rng.uniform(0.2, 0.8, 3 * m).astype(np.float32),
+        "densities": (rng.random(m) * 3.0 + 0.5).astype(np.float32),
+        "color_grads": ((rng.random(3 * m) - 0.5) * 0.2).astype(np.float32),
+        "circumdata": circumspheres(vertices, indices),
+        "sh_coeffs": np.zeros(3 * m, np.float32),
+        "sh_degree": 0,
+    }
+
+
 # The five benchmark configurations (point counts, cloud recipe, views).
 CONFIGS = {
     "c1": dict(points=2_000, cloud="uniform", sh_degree=0, views=1, res=((512, 512),), seed=0),

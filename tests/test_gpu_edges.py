@@ -126,3 +126,35 @@ def test_long_tile_lists_past_the_span_cache(c2_scene):
     np.testing.assert_allclose(out["batched"][0], out["plain"][0], rtol=1e-4)
     for k in out["plain"][1]:
         assert rel_l2(out["batched"][1][k], out["plain"][1][k]) <= 1e-3, k
+
+
+@pytest.mark.parametrize("jitter", [0.1, 0.0])
+def test_grid_scene_parity(oracle32, jitter):
+    """The reference's regular-grid mesh (test_util.rs:231-324; 8^3 vertices,
+    5 tets per cell).  With jitter 0 the faces are exactly coplanar across
+    cells and the axis-aligned camera's rays run exactly parallel to faces
+    (the |n.d| < 1e-20 rule) and through shared edges.  Images within 1e-4,
+    tile counts and sorted (tile, tet) lists bit-exact, gradients within 1e-3
+    relative L2, from an axis-aligned and an oblique camera."""
+    from rmesh_b200.camera import make_camera
+    from rmesh_b200.scenes import grid_scene
+
+    sc = grid_scene(8, np.random.default_rng(5), jitter=jitter)
+    for eye in ((0.5, -1.6, 0.5), (1.9, -1.2, 1.4)):
+        cam = make_camera(eye, (0.5, 0.5, 0.5), 50.0, 96, 96)
+        r = make_renderer(sc, cam)
+        img = r.forward_tiled(cam.cam_pos, cam.vp, cam.c2w_intrinsics)
+        ref = oracle32.forward_tiled(sc, cam)
+        assert ref["P"] > 0
+        np.testing.assert_array_equal(r.debug_tiles_touched(), np.where(ref["visible"] > 0, ref["tiles_touched"], 0))
+        tiles, tets = r.debug_pairs()
+        np.testing.assert_array_equal(tiles, ref["key_hi"])
+        np.testing.assert_array_equal(tets, ref["vals"])
+        assert np.abs(img - ref["image"]).max() <= 1e-4
+        gt = np.random.default_rng(6).uniform(0, 1, (96, 96, 3)).astype(np.float32)
+        _, dl = oracle32.loss(ref["image"], gt, 1)
+        g = r.backward(dl)
+        go = oracle32.backward(sc, cam, dl, ref)
+        for k in go:
+            assert rel_l2(g[k], go[k]) <= 1e-3, (eye, k)
+        r.close()

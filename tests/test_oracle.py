@@ -518,3 +518,21 @@ def test_c2_fd_gradients_200_per_group(oracle64):
         err = np.abs(ana - num)
         ok = (err <= tol * np.maximum(np.abs(ana), np.abs(num))) | (err <= 1e-8)
         assert idx.size >= 100 and ok.mean() >= min_pass, (key, ok.mean(), float(np.median(err / np.abs(num))))
+
+
+def test_grid_scene_structure():
+    """grid_scene restates the reference's grid layout: n^3 vertices, five
+    tets per cell over the cell's eight corners, every tet non-degenerate."""
+    from rmesh_b200.scenes import grid_scene
+
+    sc = grid_scene(4, np.random.default_rng(1), jitter=0.0)
+    v = sc["vertices"].reshape(-1, 3).astype(np.float64)
+    idx = sc["indices"].reshape(-1, 4)
+    assert v.shape == (64, 3) and idx.shape == (27 * 5, 4)
+    assert sc["circumdata"].size == 4 * idx.shape[0]
+    a, b, c, d = (v[idx[:, k]] for k in range(4))
+    vol = np.abs(np.einsum("ij,ij->i", np.cross(b - a, c - a), d - a)) / 6.0
+    step = 1.0 / 3.0
+    # four corner tets of volume step^3/6 and the central one of step^3/3 per cell
+    np.testing.assert_allclose(np.sort(vol.reshape(27, 5), axis=1),
+                               np.tile([step ** 3 / 6] * 4 + [step ** 3 / 3], (27, 1)), rtol=1e-5)
