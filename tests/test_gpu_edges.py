@@ -158,3 +158,28 @@ def test_grid_scene_parity(oracle32, jitter):
         for k in go:
             assert rel_l2(g[k], go[k]) <= 1e-3, (eye, k)
         r.close()
+
+
+@pytest.mark.parametrize("eye,target", [((3.0, 1.5, 0.0), (0.0, 1.5, 0.0)),     # tet at the frame's edge
+                                        ((50.0, 0.0, 0.0), (0.0, 0.0, 0.0)),    # sub-pixel tet
+                                        ((3.0, 0.0, 0.0), (10.0, 0.0, 0.0)),    # tet behind the camera
+                                        ((3.0, 0.0, 0.0), (0.0, 0.0, 0.0))])    # centred
+def test_known_tet_cross_renderer_cameras(oracle32, eye, target):
+    """The camera setups of cross_renderer_test.rs:766-981 (64x64, 90 degrees)
+    on the known tet: the CUDA image within 1e-4 of the oracle's, tile counts
+    and (tile, tet) lists bit-exact."""
+    from conftest import known_tet_scene
+
+    from rmesh_b200.camera import make_camera
+
+    sc = known_tet_scene()
+    cam = make_camera(eye, target, 90.0, 64, 64)
+    r = make_renderer(sc, cam)
+    img = r.forward_tiled(cam.cam_pos, cam.vp, cam.c2w_intrinsics)
+    ref = oracle32.forward_tiled(sc, cam)
+    assert np.abs(img - ref["image"]).max() <= 1e-4
+    np.testing.assert_array_equal(r.debug_tiles_touched(), np.where(ref["visible"] > 0, ref["tiles_touched"], 0))
+    tiles, tets = r.debug_pairs()
+    np.testing.assert_array_equal(tiles, ref["key_hi"])
+    np.testing.assert_array_equal(tets, ref["vals"])
+    r.close()

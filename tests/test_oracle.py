@@ -231,6 +231,50 @@ def test_four_tet_multi_angle(oracle32, eye):
     assert mean < 0.02, mean
 
 
+def test_tet_at_boundary(oracle32):
+    """cross_renderer_test.rs:766-810: the known tet at the edge of the frame;
+    tiled vs the CPU renderer max-abs < 0.002, mean-abs < 0.02."""
+    sc = known_tet_scene()
+    cam = _cam((3.0, 1.5, 0.0), (0.0, 1.5, 0.0))
+    img = oracle32.forward_tiled(sc, cam)["image"]
+    mx, mean = compare_images(img, cpu_render_scene(sc, cam))
+    assert img[..., 3].max() > 0.01
+    assert mx < 0.002 and mean < 0.02, (mx, mean)
+
+
+def test_tet_behind_camera(oracle32):
+    """cross_renderer_test.rs:812-850: camera looking away from the tet: the
+    alpha sum stays below 0.01 (here exactly zero: nothing is binned)."""
+    sc = known_tet_scene()
+    cam = _cam((3.0, 0.0, 0.0), (10.0, 0.0, 0.0))
+    f = oracle32.forward_tiled(sc, cam)
+    assert f["P"] == 0 and f["image"][..., 3].sum() < 0.01
+    assert cpu_render_scene(sc, cam)[..., 3].sum() < 0.01
+
+
+def test_distant_tet(oracle32):
+    """cross_renderer_test.rs:853-888: at distance 50 the tet covers a pixel
+    or less; tiled vs the CPU renderer mean-abs < 0.01."""
+    sc = known_tet_scene()
+    cam = _cam((50.0, 0.0, 0.0), (0.0, 0.0, 0.0))
+    img = oracle32.forward_tiled(sc, cam)["image"]
+    _, mean = compare_images(img, cpu_render_scene(sc, cam))
+    assert mean < 0.01, mean
+
+
+def test_center_pixel(oracle32):
+    """cross_renderer_test.rs:893-981: the centre pixel of the known tet seen
+    from (3, 0, 0) has alpha > 0.01, non-negative premultiplied colour, and
+    matches the CPU renderer within 0.01 per channel."""
+    sc = known_tet_scene()
+    cam = _cam((3.0, 0.0, 0.0), (0.0, 0.0, 0.0))
+    img = oracle32.forward_tiled(sc, cam)["image"]
+    ref = cpu_render_scene(sc, cam)
+    px, want = img[H // 2, W // 2], ref[H // 2, W // 2]
+    assert want[3] > 0.01 and np.all(want[:3] >= -1e-6)
+    assert np.all(np.abs(px - want) < 0.01), (px, want)
+
+
 def test_tiled_forward_multi_scene_finite(oracle32, c1_scene):
     """kernel_tests.rs:549-718: a many-tet tiled forward is finite and non-zero."""
     from conftest import c1_camera
