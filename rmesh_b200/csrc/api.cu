@@ -266,8 +266,9 @@ int radix_sort(RmeshCtx* c, K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals
   CKL();
   sort_scan_kernel<<<1, 256, 0, c->stream>>>(passes, st);
   CKL();
-  const size_t smem = sizeof(K) * kSortPart + sizeof(uint32_t) * kSortPart + sizeof(uint32_t) * (kSortWarps * 256 + 512);
-  const unsigned grid = (unsigned)std::max<uint64_t>(1, (cap + kSortPart - 1) / kSortPart);
+  constexpr int part = SortCfg<K>::PART;
+  const size_t smem = sizeof(K) * part + sizeof(uint32_t) * part + sizeof(uint32_t) * (kSortWarps * 256 + 512);
+  const unsigned grid = (unsigned)std::max<uint64_t>(1, (cap + part - 1) / part);
   K* kin = keys;
   uint32_t* vin = vals;
   K* kout = keys_alt;
@@ -289,8 +290,9 @@ int radix_sort(RmeshCtx* c, K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals
 int setup_sort_attrs() {
   static bool done = false;
   if (done) return 0;
-  const int s64 = (int)(sizeof(uint64_t) * kSortPart + sizeof(uint32_t) * kSortPart + sizeof(uint32_t) * (kSortWarps * 256 + 512));
-  const int s32 = (int)(sizeof(uint32_t) * kSortPart + sizeof(uint32_t) * kSortPart + sizeof(uint32_t) * (kSortWarps * 256 + 512));
+  constexpr int p64 = SortCfg<uint64_t>::PART, p32 = SortCfg<uint32_t>::PART;
+  const int s64 = (int)(sizeof(uint64_t) * p64 + sizeof(uint32_t) * p64 + sizeof(uint32_t) * (kSortWarps * 256 + 512));
+  const int s32 = (int)(sizeof(uint32_t) * p32 + sizeof(uint32_t) * p32 + sizeof(uint32_t) * (kSortWarps * 256 + 512));
   if (cudaFuncSetAttribute(onesweep_kernel<unsigned long long>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64) != cudaSuccess) return 1;
   if (cudaFuncSetAttribute(onesweep_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32) != cudaSuccess) return 1;
   done = true;

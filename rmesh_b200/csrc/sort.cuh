@@ -21,7 +21,15 @@ namespace rm {
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortKPT = 16;
-constexpr int kSortPart = kSortThreads * kSortKPT;  // 4096 keys per partition
+constexpr int kSortPart = kSortThreads * kSortKPT;  // 4096 keys: the smallest partition (buffer sizing)
+// Keys per thread by key width: 32-bit keys take 24 (6144-key partitions, a
+// third fewer look-back steps per pass); 64-bit keys stay at 16, where 24
+// would push the kernel past its register budget for two blocks per SM.
+template <typename K>
+struct SortCfg {
+  static constexpr int KPT = sizeof(K) == 4 ? 24 : 16;
+  static constexpr int PART = kSortThreads * KPT;
+};
 constexpr int kMaxPasses = 8;
 
 struct SortState {
@@ -94,8 +102,8 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(const K* __restr
                                                                 uint32_t* err) {
   extern __shared__ __align__(16) unsigned char smem[];
   K* s_keys = reinterpret_cast<K*>(smem);
-  uint32_t* s_vals = reinterpret_cast<uint32_t*>(smem + sizeof(K) * kSortPart);
-  uint32_t* s_whist = s_vals + kSortPart;            // [kSortWarps][256]
+  uint32_t* s_vals = reinterpret_cast<uint32_t*>(smem + sizeof(K) * SortCfg<K>::PART);
+  uint32_t* s_whist = s_vals + SortCfg<K>::PART;            // [kSortWarps][256]
   uint32_t* s_dstart = s_whist + kSortWarps * 256;   // [256] digit start inside the partition
   uint32_t* s_gbase = s_dstart + 256;                // [256] global base per digit
   __shared__ uint32_t s_part;
@@ -106,16 +114,16 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(const K* __restr
   const uint32_t part = s_part;
   unsigned long long n = n_is_u64 ? *(const unsigned long long*)n_ptr : *(const uint32_t*)n_ptr;
   if (n > cap) n = cap;
-  const unsigned long long base = (unsigned long long)part * kSortPart;
+  const unsigned long long base = (unsigned long long)part * SortCfg<K>::PART;
   if (base >= n) return;
   const uint32_t epoch = st->epoch * (uint32_t)kMaxPasses + (uint32_t)pass;  // unique per (sort, pass)
 
   // warp-striped load: warp w owns keys [w*32*KPT, (w+1)*32*KPT), lane-minor
-  K k[kSortKPT];
-  uint32_t v[kSortKPT];
-  const unsigned long long wbase = base + (unsigned long long)warp * 32 * kSortKPT;
+  K k[SortCfg<K>::KPT];
+  uint32_t v[SortCfg<K>::KPT];
+  const unsigned long long wbase = base + (unsigned long long)warp * 32 * SortCfg<K>::KPT;
 #pragma unroll
-  for (int i = 0; i < kSortKPT; ++i) {
+  for (int i = 0; i < SortCfg<K>::KPT; ++i) {
     const unsigned long long idx = wbase + (unsigned long long)i * 32 + lane;
     if (idx < n) {
       k[i] = keys_in[idx];
@@ -129,10 +137,10 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(const K* __restr
   __syncwarp();
 
   // warp multi-split: rank of each key among equal digits of this warp, in order
-  uint32_t rank[kSortKPT];
+  uint32_t rank[SortCfg<K>::KPT];
   const unsigned lt_mask = (1u << lane) - 1u;
 #pragma unroll
-  for (int i = 0; i < kSortKPT; ++i) {
+  for (int i = 0; i < SortCfg<K>::KPT; ++i) {
     const uint32_t d = digit_of(k[i], shift);
     const unsigned peers = __match_any_sync(0xffffffffu, d);
     const int leader = __ffs(peers) - 1;
@@ -201,7 +209,7 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(const K* __restr
 
   // scatter into shared memory in sorted order
 #pragma unroll
-  for (int i = 0; i < kSortKPT; ++i) {
+  for (int i = 0; i < SortCfg<K>::KPT; ++i) {
     const uint32_t dg = digit_of(k[i], shift);
     const uint32_t pos = s_dstart[dg] + s_whist[warp * 256 + dg] + rank[i];
     s_keys[pos] = k[i];
@@ -210,7 +218,7 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(const K* __restr
   __syncthreads();
 
   // write out; consecutive threads write consecutive slots of one digit run
-  for (int j = tid; j < kSortPart; j += kSortThreads) {
+  for (int j = tid; j < SortCfg<K>::PART; j += kSortThreads) {
     const K kk = s_keys[j];
     const uint32_t dg = digit_of(kk, shift);
     const unsigned long long out = (unsigned long long)s_gbase[dg] + (unsigned long long)(j - s_dstart[dg]);
