@@ -931,6 +931,19 @@ int rmesh_create(const RmeshSceneDesc* d, RmeshCtx** out) {
     CK(cudaMemsetAsync(c->sort_state.p, 0, sizeof(SortState), c->stream));
     CKR(copy_in(c, c->verts, d->vertices, 3 * N * 4));
     CKR(copy_in(c, c->idx, d->indices, 4 * M * 4));
+    {
+      // every index must name a vertex before any kernel gathers through it
+      uint32_t* bad = c->counters_d.as<uint32_t>();  // scratch word; the counters are cleared per run
+      CK(cudaMemsetAsync(bad, 0, 4, c->stream));
+      const int blocks = (int)std::min<uint64_t>((4 * M + 255) / 256, (uint64_t)c->num_sms * 8);
+      index_range_kernel<<<std::max(1, blocks), 256, 0, c->stream>>>(c->idx.as<uint32_t>(), 4 * (uint64_t)M,
+                                                                     (uint32_t)N, bad);
+      CKL();
+      uint32_t bad_h = 0;
+      CK(cudaMemcpyAsync(&bad_h, bad, 4, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      if (bad_h) return fail(c, RMESH_ERR_INVALID_ARG, "a tet index is not below the vertex count");
+    }
     CKR(copy_in(c, c->dens, d->densities, M * 4));
     CKR(copy_in(c, c->cgrad, d->color_grads, 3 * M * 4));
     CKR(copy_in(c, c->base, d->base_colors, 3 * M * 4));

@@ -108,6 +108,16 @@ __global__ void __launch_bounds__(256) emit_kernel(EmitArgs a) {
   if (overflow) atomicOr(&a.counters->err, kErrPairOverflow);
 }
 
+// Sets *bad when an index is not below n_verts (reads only the index array):
+// rmesh_create runs it before any kernel gathers through the indices.
+__global__ void __launch_bounds__(256) index_range_kernel(const uint32_t* __restrict__ idx, uint64_t n,
+                                                          uint32_t n_verts, uint32_t* bad) {
+  bool any = false;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    any = any || idx[i] >= n_verts;
+  if (__any_sync(0xffffffffu, any) && (threadIdx.x & 31) == 0) atomicOr(bad, 1u);
+}
+
 // Longest-first tile order for the persistent tile kernel: a tile's cost
 // grows with its list length, and a long list taken last leaves the other
 // CTAs idle, so tiles are bucketed by floor(log2(length)) and the buckets are

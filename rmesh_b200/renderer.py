@@ -119,6 +119,9 @@ class RMeshRenderer:
         if n_v % 3 or n_i % 4 or n_i == 0:
             raise ValueError("vertices must hold 3N floats and indices 4M (M > 0) integers")
         self._N, self._M = n_v // 3, n_i // 4
+        idx_obj = ptrs["indices"][0]
+        if isinstance(idx_obj, np.ndarray) and int(idx_obj.max()) >= self._N:
+            raise ValueError(f"indices must be below the vertex count {self._N}")  # device arrays: checked in C
         for name, per in (("base_colors", 3), ("densities", 1), ("color_grads", 3), ("circumdata", 4)):
             if _numel(ptrs[name][0]) != per * self._M:
                 raise ValueError(f"{name} must hold {per}*M = {per * self._M} values")
@@ -148,7 +151,8 @@ class RMeshRenderer:
         ctx = ctypes.c_void_p()
         rc = self._lib.rmesh_create(ctypes.byref(d), ctypes.byref(ctx))
         if rc != 0:
-            raise RMeshError(rc, "rmesh_create failed (no CUDA device, bad sizes or out of memory)")
+            raise RMeshError(rc, "rmesh_create failed (no CUDA device, bad sizes, an index not below the vertex "
+                                 "count, or out of memory)")
         self._ctx = ctx
         self._width, self._height = int(width), int(height)
         self._tile_size = int(tile_size)

@@ -188,3 +188,25 @@ def test_forward_and_binning_are_deterministic(c1_scene):
             np.testing.assert_array_equal(a, b)
     r1.close()
     r2.close()
+
+
+def test_out_of_range_index_rejected_on_the_device(c1_scene):
+    """Indices passed as a CUDA tensor with one index equal to the vertex
+    count: rmesh_create's range check (it reads only the index array) rejects
+    them before any kernel gathers through them, and the device keeps
+    rendering correctly."""
+    import torch
+
+    from rmesh_b200 import RMeshError, RMeshRenderer
+
+    sc = c1_scene
+    idx = torch.from_numpy(sc["indices"].astype(np.int32)).cuda()
+    idx[7] = sc["vertices"].size // 3
+    with pytest.raises(RMeshError):
+        RMeshRenderer(sc["vertices"], idx, sc["base_colors"], sc["densities"], sc["color_grads"],
+                      sc["circumdata"], 64, 64)
+    cam = c1_camera(64, 64)
+    r = make_renderer(sc, cam)
+    img = r.forward_tiled(cam.cam_pos, cam.vp, cam.c2w_intrinsics)
+    assert np.isfinite(img).all() and img[..., 3].max() > 0
+    r.close()
