@@ -489,6 +489,9 @@ int launch_tile_t(RmeshCtx* c, TileArgs& ta, uint32_t n_tiles, bool persistent) 
   static bool attr_done = false;  // per instantiation
   if (!attr_done) {
     CK(cudaFuncSetAttribute(tile_kernel<TS, MODE, AUX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    // the whole unified L1 as shared memory: resident CTAs are limited by it
+    CK(cudaFuncSetAttribute(tile_kernel<TS, MODE, AUX>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                            (int)cudaSharedmemCarveoutMaxShared));
     attr_done = true;
   }
   unsigned grid = n_tiles;

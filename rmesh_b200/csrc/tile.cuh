@@ -95,9 +95,11 @@ template <int TS, bool AUX>
 struct TileCfg {
   static constexpr int NT = ((TS * TS + 31) / 32) * 32;
   static constexpr int NW = NT / 32;
-  static constexpr int CAP = 512;  // items per sub-batch
+  // items per sub-batch; 448 for 12x12 tiles keeps the shared memory of a CTA
+  // under a fifth of the SM's 228 KB, for five resident CTAs
+  static constexpr int CAP = TS == 12 ? 448 : 512;
   // resident CTAs per SM the register budget is sized for
-  static constexpr int MINB = TS == 16 ? 2 : (TS == 12 ? 4 : 8);
+  static constexpr int MINB = TS == 16 ? 2 : (TS == 12 ? 5 : 8);
 };
 
 template <int TS, bool AUX>
@@ -114,7 +116,7 @@ struct __align__(16) TileSmem {
   uint32_t pmask[TS * TS];
   short2 span[kBatch][TS];
   uint16_t rowpref[kBatch][TS + 1];
-  uint16_t ipix[kBatch * TS * TS];  // (tet slot << 8) | pixel of each item of the batch (tet-major)
+  uint16_t ipix[TileCfg<TS, AUX>::CAP];  // (tet slot << 8) | pixel of each item of the sub-batch (tet-major)
   uint64_t bar[2];
   float lsum[16];
   uint32_t tile;
@@ -427,20 +429,24 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
         if (lane == 0) s.toff[0] = 0u;
       }
     };
-    // item pixel ids (tet-major) and per-pixel coverage masks
-    auto fill = [&](int nb) {
-      for (int task = tid; task < nb * TS; task += NT) {
+    // item pixel ids of tets [k0, k1), numbered from the sub-batch's first
+    // item, and their per-pixel coverage bits.  Only phase 0 reads the ids, so
+    // the next sub-batch's are written in the tail of the current one (before
+    // its closing barrier); the coverage bits of later tets are masked off there.
+    auto fill = [&](int k0, int k1) {
+      const uint32_t base0 = s.toff[k0];
+      for (int task = tid + k0 * TS; task < k1 * TS; task += NT) {
         const int k = task / TS, row = task - (task / TS) * TS;
         const short2 sp = s.span[k][row];
         if (sp.x > sp.y) continue;
-        const uint32_t base = s.toff[k] + s.rowpref[k][row];
+        const uint32_t base = s.toff[k] - base0 + s.rowpref[k][row];
         for (int c = sp.x; c <= sp.y; ++c) {
           s.ipix[base + (uint32_t)(c - sp.x)] = (uint16_t)((k << 8) | (row * TS + c));
           atomicOr(&s.pmask[row * TS + c], 1u << k);
         }
       }
     };
-    // tet-major item gi -> (tet k, pixel index in tile)
+    // item gi of the sub-batch -> (tet k, pixel index in tile)
     auto decode = [&](uint32_t gi, int& k, int& p) {
       const uint32_t e = s.ipix[gi];
       k = (int)(e >> 8);
@@ -463,7 +469,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
       const uint32_t n_items = s.toff[k1] - base;
       for (uint32_t i = tid; i < n_items; i += NT) {
         int k, p;
-        decode(base + i, k, p);
+        decode(i, k, p);
         const float4 d = s.pdir[p];
         float numo[4];
         const float* nump = nullptr;
@@ -553,10 +559,10 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
           __syncthreads();
           prefixes(nb);
           __syncthreads();
-          fill(nb);
+          int k1 = sub_end(0, nb);
+          fill(0, k1);
           __syncthreads();
           for (int k0 = 0; k0 < nb;) {
-            const int k1 = sub_end(k0, nb);
             phase0(buf, k0, k1, true);
             __syncthreads();
             // phase 1: composite this pixel's items nearest first
@@ -608,8 +614,11 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
                 }
               }
             }
+            const int k2 = k1 < nb ? sub_end(k1, nb) : nb;
+            if (k1 < nb) fill(k1, k2);
             __syncthreads();
             k0 = k1;
+            k1 = k2;
           }
           hi = next_hi;
           ++b;
@@ -672,10 +681,10 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
           __syncthreads();
           prefixes(nb);
           __syncthreads();
-          fill(nb);
+          int k1 = sub_end(0, nb);
+          fill(0, k1);
           __syncthreads();
           for (int k0 = 0; k0 < nb;) {
-            const int k1 = sub_end(k0, nb);
             const uint32_t base = s.toff[k0];
             const uint32_t n_items = s.toff[k1] - base;
             phase0(buf, k0, k1, true);
@@ -756,8 +765,11 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
               }
               __syncwarp();
             }
+            const int k2 = k1 < nb ? sub_end(k1, nb) : nb;
+            if (k1 < nb) fill(k1, k2);
             __syncthreads();
             k0 = k1;
+            k1 = k2;
           }
           // flush the batch's per-tet sums
           if (tid < nb) {
@@ -875,10 +887,10 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
           }
           prefixes(nb);
           __syncthreads();
-          fill(nb);
+          int k1 = sub_end(0, nb);
+          fill(0, k1);
           __syncthreads();
           for (int k0 = 0; k0 < nb;) {
-            const int k1 = sub_end(k0, nb);
             const uint32_t base = s.toff[k0];
             const uint32_t n_items = s.toff[k1] - base;
             phase0(buf, k0, k1, false);
@@ -1044,8 +1056,11 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
                 __syncwarp();
               }
             }
+            const int k2 = k1 < nb ? sub_end(k1, nb) : nb;
+            if (k1 < nb) fill(k1, k2);
             __syncthreads();
             k0 = k1;
+            k1 = k2;
           }
           // flush: rebuild each tet's 19 gradients from its moments, four threads
           // per tet (thread f takes face f's vertex terms, thread 0 also the
