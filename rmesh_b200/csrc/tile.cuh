@@ -457,10 +457,17 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
     auto item_of = [&](int k, uint32_t base) -> uint32_t {
       return s.toff[k] - base + s.rowpref[k][prow] + (uint32_t)(pcol - s.span[k][prow].x);
     };
-    // greedy sub-batch end: largest k1 with toff[k1] - toff[k0] <= CAP (>= k0+1)
+    // sub-batch end (>= k0 + 1): the batch's remaining items split into the
+    // fewest sub-batches of at most CAP items, of about equal size, so that
+    // no short remainder leaves most threads of a phase idle
     auto sub_end = [&](int k0, int nb) -> int {
+      const uint32_t base = s.toff[k0];
+      const uint32_t rem = s.toff[nb] - base;
+      if (rem <= (uint32_t)CAP) return nb;
+      const uint32_t parts = (rem + (uint32_t)CAP - 1u) / (uint32_t)CAP;
+      const uint32_t target = (rem + parts - 1u) / parts;
       int k1 = k0 + 1;
-      while (k1 < nb && s.toff[k1 + 1] - s.toff[k0] <= (uint32_t)CAP) ++k1;
+      while (k1 < nb && s.toff[k1] - base < target && s.toff[k1 + 1] - base <= (uint32_t)CAP) ++k1;
       return k1;
     };
     // phase 0: item-parallel intersection + integral.  clip_lo: 0 for the
