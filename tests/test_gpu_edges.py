@@ -1,6 +1,9 @@
 """Edge cases of the CUDA path vs the oracle (needs a B200): a view that sees
 nothing, a camera inside the mesh (negative depth keys, vertices behind the
-camera), and a multi-view step whose tiles exceed 2^16 in total."""
+camera), a multi-view step whose tiles exceed 2^16 in total, pair-buffer
+overflow, tile lists longer than the span cache, the reference's grid mesh,
+its cross-renderer cameras, and tets large enough that a batch's covered
+pixels exceed the kernel's sub-batch capacity."""
 from __future__ import annotations
 
 import numpy as np
@@ -183,3 +186,106 @@ def test_known_tet_cross_renderer_cameras(oracle32, eye, target):
     np.testing.assert_array_equal(tiles, ref["key_hi"])
     np.testing.assert_array_equal(tets, ref["vals"])
     r.close()
+
+
+def _max_batch_items(sc, cam, ref, ts):
+    """Largest number of covered (pixel, tet) items in one 32-tet batch of a
+    tile's sorted list: pixel centres inside each listed tet's projected
+    silhouette (convex hull of its four projected vertices), batches taken
+    from the front of the list as the forward pass takes them."""
+    from scipy.spatial import ConvexHull
+
+    vp = np.asarray(cam.vp, np.float64).reshape(4, 4).T  # column-major
+    v = np.asarray(sc["vertices"], np.float64).reshape(-1, 3)
+    clip = np.c_[v, np.ones(len(v))] @ vp.T
+    xy = clip[:, :2] / clip[:, 3:4]
+    px = np.c_[(xy[:, 0] + 1) * 0.5 * cam.width, (1 - xy[:, 1]) * 0.5 * cam.height]
+    idx = np.asarray(sc["indices"]).reshape(-1, 4)
+    tiles_x = (cam.width + ts - 1) // ts
+    real = ref["key_hi"] != 0xFFFFFFFF
+    keys, vals = ref["key_hi"][real], ref["vals"][real]
+    starts = np.r_[0, np.nonzero(np.diff(keys))[0] + 1, len(keys)]
+    best = 0
+    for a, b in zip(starts[:-1], starts[1:]):
+        ty, tx = divmod(int(keys[a]), tiles_x)
+        ys, xs = np.mgrid[ty * ts:(ty + 1) * ts, tx * ts:(tx + 1) * ts]
+        centres = np.c_[xs.ravel() + 0.5, ys.ravel() + 0.5]
+        counts = []
+        for tet in vals[a:b]:
+            q = px[idx[tet]]
+            try:
+                poly = q[ConvexHull(q).vertices]  # counter-clockwise
+            except Exception:  # degenerate silhouette
+                counts.append(0)
+                continue
+            inside = np.ones(len(centres), bool)
+            for i in range(len(poly)):
+                p0, p1 = poly[i], poly[(i + 1) % len(poly)]
+                inside &= (p1[0] - p0[0]) * (centres[:, 1] - p0[1]) - (p1[1] - p0[1]) * (centres[:, 0] - p0[0]) >= 0
+            counts.append(int(inside.sum()))
+        counts = np.array(counts)[::-1]  # front to back
+        for s0 in range(0, len(counts), 32):
+            best = max(best, int(counts[s0:s0 + 32].sum()))
+    return best
+
+
+@pytest.mark.parametrize("ts", [8, 12, 16])
+def test_large_tets_many_sub_batches(oracle32, ts):
+    """60 points -> 287 tets, most covering more than a tile at 128x96: a
+    tile's 32-tet batch then holds more covered pixels than the kernel's
+    per-sub-batch item capacity (512; 768 for 12-pixel tiles), so batches
+    split into sub-batches, whose item maps are written in the previous
+    sub-batch's tail.  Forward image, tile
+    lists, adjoint gradients, error statistics and a batched / graph-mode
+    training step against the oracle."""
+    from oracle import OracleTrainer
+    from rmesh_b200.camera import make_camera
+    from rmesh_b200.scenes import make_scene, uniform_cloud
+
+    rng = np.random.default_rng(31)
+    sc = make_scene(uniform_cloud(60, rng), rng)
+    sc["densities"] = (sc["densities"] * 0.1).astype(np.float32)  # few pixels saturate
+    cam = make_camera((2.2, -1.6, 1.0), (0.0, 0.0, 0.0), 60.0, 128, 96)
+
+    r = make_renderer(sc, cam, tile_size=ts)
+    img = r.forward_tiled(cam.cam_pos, cam.vp, cam.c2w_intrinsics)
+    ref = oracle32.forward_tiled(sc, cam, tile_size=ts)
+    # some batches exceed the kernel's sub-batch capacity (953, 1,660 and 2,497
+    # items at tiles of 8, 12 and 16)
+    assert _max_batch_items(sc, cam, ref, ts) > (768 if ts == 12 else 512)
+    tiles, tets = r.debug_pairs()
+    np.testing.assert_array_equal(tiles, ref["key_hi"])
+    np.testing.assert_array_equal(tets, ref["vals"])
+    assert np.abs(img - ref["image"]).max() <= 1e-4
+
+    gt = np.random.default_rng(32).uniform(0, 1, (96, 128, 3)).astype(np.float32)
+    _, dl = oracle32.loss(ref["image"], gt, 1)
+    g = r.backward(dl)
+    go = oracle32.backward(sc, cam, dl, ref, tile_size=ts)
+    for k in go:
+        assert rel_l2(g[k], go[k]) <= 1e-3, k
+
+    r.forward_tiled(cam.cam_pos, cam.vp, cam.c2w_intrinsics)
+    n = cam.width * cam.height
+    pe = np.random.default_rng(33).uniform(0, 1, n).astype(np.float32)
+    se = np.random.default_rng(34).uniform(0, 1, n).astype(np.float32)
+    err, cnt = r.forward_error(pe, se)
+    e_ref, c_ref = oracle32.error_stats(sc, cam, ref, pe, se, tile_size=ts)
+    for k in (0, 1, 2, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15):
+        assert rel_l2(err[:, k], e_ref[:, k]) <= 1e-4, k
+    assert np.abs(cnt[:, 0] - c_ref[:, 0]).sum() <= max(2, c_ref[:, 0].sum() // 10000)
+    r.close()
+
+    cams = [cam, make_camera((-1.8, -2.0, 0.6), (0.0, 0.0, 0.0), 60.0, 128, 96)]
+    gts = [gt, np.random.default_rng(35).uniform(0, 1, (96, 128, 3)).astype(np.float32)]
+    for mode in ("batched", "graph"):
+        r = make_renderer(sc, cam, tile_size=ts)
+        tr = OracleTrainer(sc, tile_size=ts)
+        for step in range(2):
+            losses = r.train_step_views(cams, gts, 1e-4, 1e-2, 1e-3, 1, mode=mode)
+            want = tr.train_step_views(cams, gts, 1e-4, 1e-2, 1e-3, 1)
+            np.testing.assert_allclose(losses, want, rtol=1e-4, err_msg=f"{mode} step {step}")
+        p = r.get_params()
+        for k in ("vertices", "densities", "color_grads"):
+            assert rel_l2(p[k], tr.scene[k]) <= 1e-3, (mode, k)
+        r.close()
