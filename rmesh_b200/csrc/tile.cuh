@@ -95,10 +95,10 @@ template <int TS, bool AUX>
 struct TileCfg {
   static constexpr int NT = ((TS * TS + 31) / 32) * 32;
   static constexpr int NW = NT / 32;
-  // items per sub-batch; 768 for 12x12 tiles fills a quarter of the SM's
+  // items per sub-batch; 800 for 12x12 tiles fills a quarter of the SM's
   // 228 KB of shared memory (four resident CTAs, the register limit at 96
   // registers per thread): fewer sub-batches, fewer block barriers
-  static constexpr int CAP = TS == 12 ? 768 : 512;
+  static constexpr int CAP = TS == 12 ? 800 : 512;
   // resident CTAs per SM the register budget is sized for
   static constexpr int MINB = TS == 16 ? 2 : (TS == 12 ? 4 : 8);
 };

@@ -233,7 +233,7 @@ def _max_batch_items(sc, cam, ref, ts):
 def test_large_tets_many_sub_batches(oracle32, ts):
     """60 points -> 287 tets, most covering more than a tile at 128x96: a
     tile's 32-tet batch then holds more covered pixels than the kernel's
-    per-sub-batch item capacity (512; 768 for 12-pixel tiles), so batches
+    per-sub-batch item capacity (512; 800 for 12-pixel tiles), so batches
     split into sub-batches, whose item maps are written in the previous
     sub-batch's tail.  Forward image, tile
     lists, adjoint gradients, error statistics and a batched / graph-mode
@@ -252,7 +252,7 @@ def test_large_tets_many_sub_batches(oracle32, ts):
     ref = oracle32.forward_tiled(sc, cam, tile_size=ts)
     # some batches exceed the kernel's sub-batch capacity (953, 1,660 and 2,497
     # items at tiles of 8, 12 and 16)
-    assert _max_batch_items(sc, cam, ref, ts) > (768 if ts == 12 else 512)
+    assert _max_batch_items(sc, cam, ref, ts) > (800 if ts == 12 else 512)
     tiles, tets = r.debug_pairs()
     np.testing.assert_array_equal(tiles, ref["key_hi"])
     np.testing.assert_array_equal(tets, ref["vals"])
