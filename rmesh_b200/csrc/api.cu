@@ -184,6 +184,46 @@ float* sh_grad(const RmeshCtx* c) {
     c->kernel_launches++;                                                                         \
   } while (0)
 
+// One-time per-device settings.  cudaFuncSetAttribute applies to the current
+// device only, so "already set" is recorded per device ordinal (under a mutex:
+// contexts on different devices may be driven from different threads).
+constexpr int kMaxDeviceOrdinals = 64;
+struct PerDeviceOnce {
+  std::mutex mu;
+  bool done[kMaxDeviceOrdinals] = {};
+  template <typename F>
+  cudaError_t run(F f) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDeviceOrdinals) return f();
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[dev]) return cudaSuccess;
+    e = f();
+    if (e == cudaSuccess) done[dev] = true;
+    return e;
+  }
+};
+
+// Makes the context's device current for the duration of an API call and
+// restores the caller's device afterwards (contexts on several devices can be
+// driven from one thread).
+struct DevGuard {
+  int prev = -1;
+  explicit DevGuard(const RmeshCtx* c) {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      cudaGetLastError();
+      prev = -1;
+      return;
+    }
+    if (prev != c->device && cudaSetDevice(c->device) != cudaSuccess) cudaGetLastError();
+  }
+  ~DevGuard() {
+    int now = -1;
+    if (prev >= 0 && cudaGetDevice(&now) == cudaSuccess && now != prev) cudaSetDevice(prev);
+  }
+};
+
 cudaEvent_t take_event(RmeshCtx* c) {
   if (!c->event_pool.empty()) {
     cudaEvent_t e = c->event_pool.back();
@@ -288,14 +328,19 @@ int radix_sort(RmeshCtx* c, K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals
 }
 
 int setup_sort_attrs() {
-  static bool done = false;
-  if (done) return 0;
-  constexpr int p64 = SortCfg<uint64_t>::PART, p32 = SortCfg<uint32_t>::PART;
-  const int s64 = (int)(sizeof(uint64_t) * p64 + sizeof(uint32_t) * p64 + sizeof(uint32_t) * (kSortWarps * 256 + 512));
-  const int s32 = (int)(sizeof(uint32_t) * p32 + sizeof(uint32_t) * p32 + sizeof(uint32_t) * (kSortWarps * 256 + 512));
-  if (cudaFuncSetAttribute(onesweep_kernel<unsigned long long>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64) != cudaSuccess) return 1;
-  if (cudaFuncSetAttribute(onesweep_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32) != cudaSuccess) return 1;
-  done = true;
+  static PerDeviceOnce once;
+  const cudaError_t e = once.run([]() -> cudaError_t {
+    constexpr int p64 = SortCfg<uint64_t>::PART, p32 = SortCfg<uint32_t>::PART;
+    const int s64 = (int)(sizeof(uint64_t) * p64 + sizeof(uint32_t) * p64 + sizeof(uint32_t) * (kSortWarps * 256 + 512));
+    const int s32 = (int)(sizeof(uint32_t) * p32 + sizeof(uint32_t) * p32 + sizeof(uint32_t) * (kSortWarps * 256 + 512));
+    cudaError_t r = cudaFuncSetAttribute(onesweep_kernel<unsigned long long>, cudaFuncAttributeMaxDynamicSharedMemorySize, s64);
+    if (r != cudaSuccess) return r;
+    return cudaFuncSetAttribute(onesweep_kernel<uint32_t>, cudaFuncAttributeMaxDynamicSharedMemorySize, s32);
+  });
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return 1;
+  }
   return 0;
 }
 
@@ -486,14 +531,14 @@ template <int TS, int MODE, bool AUX>
 int launch_tile_t(RmeshCtx* c, TileArgs& ta, uint32_t n_tiles, bool persistent) {
   constexpr int NT = TileCfg<TS, AUX>::NT;
   constexpr size_t smem = sizeof(TileSmem<TS, AUX>);
-  static bool attr_done = false;  // per instantiation
-  if (!attr_done) {
-    CK(cudaFuncSetAttribute(tile_kernel<TS, MODE, AUX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  static PerDeviceOnce attrs;  // per instantiation and device
+  CK(attrs.run([]() -> cudaError_t {
+    cudaError_t e = cudaFuncSetAttribute(tile_kernel<TS, MODE, AUX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
     // the whole unified L1 as shared memory: resident CTAs are limited by it
-    CK(cudaFuncSetAttribute(tile_kernel<TS, MODE, AUX>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                            (int)cudaSharedmemCarveoutMaxShared));
-    attr_done = true;
-  }
+    return cudaFuncSetAttribute(tile_kernel<TS, MODE, AUX>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                (int)cudaSharedmemCarveoutMaxShared);
+  }));
   unsigned grid = n_tiles;
   if (persistent) {
     int occ = 0;
@@ -965,6 +1010,7 @@ int rmesh_create(const RmeshSceneDesc* d, RmeshCtx** out) {
 
 int rmesh_destroy(RmeshCtx* c) {
   if (!c) return RMESH_OK;
+  DevGuard dg__(c);
   if (c->stream) cudaStreamSynchronize(c->stream);
   c->drop_graphs();
   for (auto& e : c->events) {
@@ -982,6 +1028,7 @@ int rmesh_destroy(RmeshCtx* c) {
 
 int rmesh_set_stream(RmeshCtx* c, void* s) {
   if (!c) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   CK(cudaStreamSynchronize(c->stream));
   if (c->own_stream) cudaStreamDestroy(c->stream);
   c->own_stream = false;
@@ -992,12 +1039,14 @@ int rmesh_set_stream(RmeshCtx* c, void* s) {
 
 int rmesh_set_min_t(RmeshCtx* c, float t) {
   if (!c) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   c->min_t = t;
   return RMESH_OK;
 }
 
 int rmesh_set_tile_size(RmeshCtx* c, int32_t ts) {
   if (!c) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   if (ts != 8 && ts != 12 && ts != 16) return fail(c, RMESH_ERR_INVALID_ARG, "tile size must be 8, 12 or 16");
   c->tile_size = ts;
   c->have_forward = false;
@@ -1006,6 +1055,7 @@ int rmesh_set_tile_size(RmeshCtx* c, int32_t ts) {
 
 int rmesh_update_params(RmeshCtx* c, const float* v, const float* b, const float* d, const float* g) {
   if (!c) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   CKR(copy_in(c, c->verts, v, 3 * (size_t)c->N * 4));
   CKR(copy_in(c, c->base, b, 3 * (size_t)c->M * 4));
   CKR(copy_in(c, c->dens, d, (size_t)c->M * 4));
@@ -1015,6 +1065,7 @@ int rmesh_update_params(RmeshCtx* c, const float* v, const float* b, const float
 
 int rmesh_get_params(RmeshCtx* c, float* v, float* b, float* d, float* g) {
   if (!c) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   if (v) CK(cudaMemcpyAsync(v, c->verts.p, 3 * (size_t)c->N * 4, cudaMemcpyDefault, c->stream));
   if (b) CK(cudaMemcpyAsync(b, c->base.p, 3 * (size_t)c->M * 4, cudaMemcpyDefault, c->stream));
   if (d) CK(cudaMemcpyAsync(d, c->dens.p, (size_t)c->M * 4, cudaMemcpyDefault, c->stream));
@@ -1025,6 +1076,7 @@ int rmesh_get_params(RmeshCtx* c, float* v, float* b, float* d, float* g) {
 
 int rmesh_set_aux_data(RmeshCtx* c, const float* aux_data) {
   if (!c || !aux_data) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   if (c->aux_dim == 0) return fail(c, RMESH_ERR_INVALID_ARG, "aux_dim is 0; create the context with aux_dim > 0");
   CKR(copy_in(c, c->aux_data, aux_data, (size_t)c->M * c->aux_dim * 4));
   return RMESH_OK;
@@ -1032,6 +1084,7 @@ int rmesh_set_aux_data(RmeshCtx* c, const float* aux_data) {
 
 int rmesh_get_aux_data(RmeshCtx* c, float* aux_data) {
   if (!c || !aux_data) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   if (c->aux_dim == 0) return fail(c, RMESH_ERR_INVALID_ARG, "aux_dim is 0; no aux data");
   CK(cudaMemcpyAsync(aux_data, c->aux_data.p, (size_t)c->M * c->aux_dim * 4, cudaMemcpyDefault, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -1040,12 +1093,14 @@ int rmesh_get_aux_data(RmeshCtx* c, float* aux_data) {
 
 int rmesh_set_lr_sh(RmeshCtx* c, float lr) {
   if (!c) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   c->lr_sh = lr;
   return RMESH_OK;
 }
 
 int rmesh_update_sh(RmeshCtx* c, const float* sh) {
   if (!c || !sh) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   if (c->sh_degree < 0) return fail(c, RMESH_ERR_STATE, "the context has no SH coefficients");
   CKR(copy_in(c, c->sh, sh, (size_t)c->M * 3 * c->sh_nc * 4));
   return RMESH_OK;
@@ -1053,6 +1108,7 @@ int rmesh_update_sh(RmeshCtx* c, const float* sh) {
 
 int rmesh_get_sh(RmeshCtx* c, float* sh) {
   if (!c || !sh) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   if (c->sh_degree < 0) return fail(c, RMESH_ERR_STATE, "the context has no SH coefficients");
   CK(cudaMemcpyAsync(sh, c->sh.p, (size_t)c->M * 3 * c->sh_nc * 4, cudaMemcpyDefault, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -1061,6 +1117,7 @@ int rmesh_get_sh(RmeshCtx* c, float* sh) {
 
 int rmesh_get_sh_grad(RmeshCtx* c, float* d_sh) {
   if (!c || !d_sh) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   if (c->sh_degree < 0) return fail(c, RMESH_ERR_STATE, "the context has no SH coefficients");
   CK(cudaMemcpyAsync(d_sh, sh_grad(c), (size_t)c->M * 3 * c->sh_nc * 4, cudaMemcpyDefault, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -1069,6 +1126,7 @@ int rmesh_get_sh_grad(RmeshCtx* c, float* d_sh) {
 
 int rmesh_get_info(RmeshCtx* c, RmeshInfo* info) {
   if (!c || !info) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   memset(info, 0, sizeof(*info));
   info->n_vertices = c->N;
   info->n_tets = c->M;
@@ -1109,6 +1167,7 @@ static std::vector<std::pair<DevBuf*, uint64_t>> adam_state_parts(RmeshCtx* c) {
 
 int rmesh_adam_state_size(RmeshCtx* c, uint64_t* n_floats) {
   if (!c || !n_floats) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   uint64_t n = 0;
   for (auto& p : adam_state_parts(c)) n += p.second;
   *n_floats = n;
@@ -1117,6 +1176,7 @@ int rmesh_adam_state_size(RmeshCtx* c, uint64_t* n_floats) {
 
 int rmesh_get_adam_state(RmeshCtx* c, float* state, uint32_t* step) {
   if (!c || !state) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   uint64_t off = 0;
   for (auto& p : adam_state_parts(c)) {
     CK(cudaMemcpyAsync(state + off, p.first->p, p.second * 4, cudaMemcpyDefault, c->stream));
@@ -1129,6 +1189,7 @@ int rmesh_get_adam_state(RmeshCtx* c, float* state, uint32_t* step) {
 
 int rmesh_set_adam_state(RmeshCtx* c, const float* state, uint32_t step) {
   if (!c || !state) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   uint64_t off = 0;
   for (auto& p : adam_state_parts(c)) {
     CK(cudaMemcpyAsync(p.first->p, state + off, p.second * 4, cudaMemcpyDefault, c->stream));
@@ -1141,6 +1202,7 @@ int rmesh_set_adam_state(RmeshCtx* c, const float* state, uint32_t step) {
 
 int rmesh_forward_views(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views, float* rgba_out, float* aux_out) {
   if (!c || !cams || !rgba_out) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   if (n_views <= 0 || n_views > kMaxViews) return fail(c, RMESH_ERR_INVALID_ARG, "n_views out of range");
   uint64_t total_pix = 0;
   uint32_t total_tiles = 0;
@@ -1187,6 +1249,7 @@ int rmesh_forward_views(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views, f
 
 int rmesh_forward_tiled(RmeshCtx* c, const RmeshCamera* cam, float* rgba_out, float* aux_out) {
   if (!c || !cam || !rgba_out) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   const uint64_t npix = (uint64_t)cam->width * cam->height;
   for (int attempt = 0; attempt < 4; ++attempt) {
     CKR(fill_view(c, *cam, c->views_h[0], 0, 0));
@@ -1228,6 +1291,7 @@ int rmesh_forward_tiled(RmeshCtx* c, const RmeshCamera* cam, float* rgba_out, fl
 
 int rmesh_backward(RmeshCtx* c, const float* dl, float* d_verts, float* d_dens, float* d_base, float* d_cgrad) {
   if (!c || !dl) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   if (!c->have_forward) return fail(c, RMESH_ERR_STATE, "backward() must follow forward_tiled()");
   const ViewParams& v = c->views_h[0];
   const uint64_t npix = (uint64_t)v.W * v.H;
@@ -1267,6 +1331,7 @@ int rmesh_backward(RmeshCtx* c, const float* dl, float* d_verts, float* d_dens, 
 int rmesh_forward_error(RmeshCtx* c, const float* pixel_err, const float* ssim_err, float* tet_err,
                         int32_t* tet_count) {
   if (!c || !pixel_err || !ssim_err || !tet_err || !tet_count) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   if (!c->have_forward) return fail(c, RMESH_ERR_STATE, "forward_error() must follow forward_tiled()");
   const ViewParams& v = c->views_h[0];
   const uint64_t npix = (uint64_t)v.W * v.H;
@@ -1298,6 +1363,7 @@ int rmesh_forward_error(RmeshCtx* c, const float* pixel_err, const float* ssim_e
 int rmesh_train_step(RmeshCtx* c, const RmeshCamera* cam, const float* gt, float lr_verts, float lr_dens,
                      float lr_grads, int32_t loss_type, float* loss_out) {
   if (!c) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   RmeshTrainOpts o;
   memset(&o, 0, sizeof(o));
   o.lr_verts = lr_verts;
@@ -1313,6 +1379,7 @@ int rmesh_train_step(RmeshCtx* c, const RmeshCamera* cam, const float* gt, float
 int rmesh_train_step_views(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views, const float* gt,
                            const RmeshTrainOpts* opts, float* loss_out) {
   if (!c) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   if (!opts || opts->mode < 0 || opts->mode > 2) return fail(c, RMESH_ERR_INVALID_ARG, "bad mode");
   return train_views(c, cams, n_views, gt, opts, loss_out);
 }
@@ -1320,6 +1387,7 @@ int rmesh_train_step_views(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views
 int rmesh_accumulate_views(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views, const float* gt,
                            const RmeshTrainOpts* opts, float* loss_out) {
   if (!c) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   if (!opts || opts->mode < 0 || opts->mode > 2) return fail(c, RMESH_ERR_INVALID_ARG, "bad mode");
   return train_views(c, cams, n_views, gt, opts, loss_out, false);
 }
@@ -1327,6 +1395,7 @@ int rmesh_accumulate_views(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views
 int rmesh_autotune_tile_size(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views, const float* gt,
                              const RmeshTrainOpts* opts, int32_t* tile_size_out, float* ms_out) {
   if (!c || !opts || !tile_size_out) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   RmeshTrainOpts o = *opts;
   o.mode = RMESH_MODE_BATCHED;
   const int sizes[3] = {8, 12, 16};
@@ -1369,6 +1438,7 @@ int rmesh_autotune_tile_size(RmeshCtx* c, const RmeshCamera* cams, int32_t n_vie
 
 int rmesh_grad_slots(RmeshCtx* c, float** ptr, uint64_t* n_floats) {
   if (!c || !ptr || !n_floats) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   *ptr = c->grad_slot.as<float>();
   *n_floats = grad_floats(c);
   return RMESH_OK;
@@ -1376,6 +1446,7 @@ int rmesh_grad_slots(RmeshCtx* c, float** ptr, uint64_t* n_floats) {
 
 int rmesh_apply_adam(RmeshCtx* c, const RmeshTrainOpts* o) {
   if (!c || !o) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   AdamParams& hp = *c->hp_h;
   hp.step = c->step + 1;
   hp.lr_verts = o->lr_verts;
@@ -1396,6 +1467,7 @@ int rmesh_apply_adam(RmeshCtx* c, const RmeshTrainOpts* o) {
 
 int rmesh_debug_tiles_touched(RmeshCtx* c, uint32_t* out) {
   if (!c || !out) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   if (!c->have_forward) return fail(c, RMESH_ERR_STATE, "no forward yet");
   CK(cudaMemcpyAsync(out, c->tiles_touched.p, (size_t)c->M * 4, cudaMemcpyDefault, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -1404,6 +1476,7 @@ int rmesh_debug_tiles_touched(RmeshCtx* c, uint32_t* out) {
 
 int rmesh_debug_pairs(RmeshCtx* c, uint32_t* tiles, uint32_t* tets, uint64_t cap, uint64_t* n) {
   if (!c || !n) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   if (!c->have_forward) return fail(c, RMESH_ERR_STATE, "no forward yet");
   *n = c->last_n_pairs;
   const uint64_t k = std::min<uint64_t>(cap, c->last_n_pairs);
@@ -1425,6 +1498,7 @@ int rmesh_debug_pairs(RmeshCtx* c, uint32_t* tiles, uint32_t* tets, uint64_t cap
 
 int rmesh_debug_ranges(RmeshCtx* c, uint32_t* ranges, uint64_t n_tiles) {
   if (!c || !ranges) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   if (!c->have_forward) return fail(c, RMESH_ERR_STATE, "no forward yet");
   const uint64_t k = std::min<uint64_t>(n_tiles, c->last_tiles);
   CK(cudaMemcpyAsync(ranges, c->ranges.p, k * 8, cudaMemcpyDefault, c->stream));
@@ -1456,12 +1530,14 @@ int rmesh_debug_timeouts(uint32_t* bits_out) {
 
 int rmesh_set_profiling(RmeshCtx* c, int32_t on) {
   if (!c) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   c->profiling = on != 0;
   return RMESH_OK;
 }
 
 int rmesh_stage_times(RmeshCtx* c, float* ms_out, int32_t* launches_out) {
   if (!c) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
   CK(cudaStreamSynchronize(c->stream));
   for (auto& e : c->events) {
     float ms = 0.f;
@@ -1626,7 +1702,7 @@ __global__ void __launch_bounds__(256) count_tiles_static_kernel(const float* __
 
 namespace {
 
-// Device address of g_count_scratch per device ordinal, looked up on the first
+// Device address of g_count_scratch per device ordinal, looked up by every
 // call made with that device current.
 constexpr int kStaticMaxDevices = 64;
 std::mutex g_scratch_mu;
@@ -1647,16 +1723,16 @@ bool device_range_ok(const void* p, size_t bytes, int dev) {
   } else if (at.type != cudaMemoryTypeManaged) {
     return false;
   }
-  static MemRangeFn range_fn = nullptr;
-  static bool looked_up = false;
-  if (!looked_up) {
+  // looked up once; a function-local static initialiser is thread-safe
+  static const MemRangeFn range_fn = []() -> MemRangeFn {
     void* fn = nullptr;
     cudaDriverEntryPointQueryResult q;
     if (cudaGetDriverEntryPointByVersion("cuMemGetAddressRange", &fn, 12000, cudaEnableDefault, &q) == cudaSuccess &&
         q == cudaDriverEntryPointSuccess)
-      range_fn = reinterpret_cast<MemRangeFn>(fn);
-    looked_up = true;
-  }
+      return reinterpret_cast<MemRangeFn>(fn);
+    cudaGetLastError();
+    return nullptr;
+  }();
   if (range_fn) {
     unsigned long long base = 0;
     size_t size = 0;
@@ -1691,17 +1767,18 @@ extern "C" int rmesh_count_tiles_static(const float* vertices, uint64_t n_vertic
   if (dev < 0 || dev >= kStaticMaxDevices) return RMESH_ERR_INVALID_ARG;
   unsigned char* scratch = nullptr;
   {
-    // first call on this device: look up the scratch array's device address
-    // (this may load the module on the device, so make it before any capture)
+    // The scratch array's device address on this device.  The first call on a
+    // device may load the module there, so make it before any stream capture.
+    // The address is looked up again on every call (cheap once the module is
+    // loaded), so a device reset between calls cannot leave a stale pointer;
+    // the cached copy only records that the first lookup happened.
     std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (!g_scratch_ptr[dev]) {
-      void* p = nullptr;
-      if (cudaGetSymbolAddress(&p, g_count_scratch) != cudaSuccess || !p) {
-        cudaGetLastError();
-        return RMESH_ERR_CUDA;
-      }
-      g_scratch_ptr[dev] = static_cast<unsigned char*>(p);
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_count_scratch) != cudaSuccess || !p) {
+      cudaGetLastError();
+      return RMESH_ERR_CUDA;
     }
+    g_scratch_ptr[dev] = static_cast<unsigned char*>(p);
     scratch = g_scratch_ptr[dev];
   }
 

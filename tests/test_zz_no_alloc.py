@@ -99,3 +99,56 @@ def test_static_count_rejects_host_memory(c1_scene):
                                       sc["indices"].ctypes.data, sc["densities"].ctypes.data, M, ctypes.byref(cs),
                                       12, host_out.ctypes.data, host_out.ctypes.data, counts.data_ptr(), None)
     assert rc == _lib.RMESH_ERR_INVALID_ARG
+
+
+@pytest.mark.gpu
+def test_static_count_bad_index_empty_mesh_and_no_allocation(c1_scene):
+    """A tet with a vertex index past the vertex count is skipped and flagged
+    (counts[1] bit 4) while every other tet keeps its count; an empty mesh
+    returns counts (0, 0); and a warm call leaves the device's free memory
+    unchanged (the call allocates nothing)."""
+    import torch
+
+    from rmesh_b200 import _lib
+
+    lib = _lib.load()
+    sc = c1_scene
+    M = sc["densities"].size
+    N = sc["vertices"].size // 3
+    cam = c1_camera(256, 256)
+    vert = torch.from_numpy(sc["vertices"]).cuda()
+    dens = torch.from_numpy(sc["densities"]).cuda()
+    good = torch.from_numpy(sc["indices"].view(np.int32)).cuda()
+    out = (torch.full((M,), -1, dtype=torch.int32, device="cuda"),
+           torch.full((M,), -1, dtype=torch.int32, device="cuda"),
+           torch.full((2,), -1, dtype=torch.int32, device="cuda"))
+    assert _call(lib, (vert, good, dens), cam, 12, out) == _lib.RMESH_OK
+    torch.cuda.synchronize()
+    want = out[0].cpu().numpy().view(np.uint32).copy()
+    hit = int(np.nonzero(want)[0][0])  # a tile-touching tet, made invalid below
+
+    bad_idx = sc["indices"].copy()
+    bad_idx[4 * hit + 2] = N  # one past the last vertex
+    bad = torch.from_numpy(bad_idx.view(np.int32)).cuda()
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    assert _call(lib, (vert, bad, dens), cam, 12, out) == _lib.RMESH_OK
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
+    assert free1 == free0
+    tiles = out[0].cpu().numpy().view(np.uint32)
+    n_vis, err = (int(x) for x in out[2].cpu().numpy().view(np.uint32))
+    assert err & 4
+    assert tiles[hit] == 0
+    rest = np.ones(M, bool)
+    rest[hit] = False
+    np.testing.assert_array_equal(tiles[rest], want[rest])
+    assert n_vis == int(np.count_nonzero(want)) - 1
+
+    # empty mesh: counts cleared to (0, 0), nothing else touched
+    counts = torch.full((2,), -1, dtype=torch.int32, device="cuda")
+    cs = _cam_struct(cam)
+    assert lib.rmesh_count_tiles_static(None, 0, None, None, 0, ctypes.byref(cs), 12, None, None,
+                                        counts.data_ptr(), None) == _lib.RMESH_OK
+    torch.cuda.synchronize()
+    assert counts.cpu().tolist() == [0, 0]
