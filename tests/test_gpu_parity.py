@@ -91,14 +91,14 @@ def test_custom_aux_channels(c1_scene, oracle32):
 
 
 def test_c1_backward_parity(c1_scene, oracle32):
-    cam = c1_camera(256, 256)
+    cam = c1_camera(512, 512)  # the configuration's stated resolution
     r = make_renderer(c1_scene, cam)
     img = r.forward_tiled(cam.cam_pos, cam.vp, cam.c2w_intrinsics)
     gt = np.random.default_rng(0).uniform(0, 1, (cam.height, cam.width, 3)).astype(np.float32)
     ref = oracle32.forward_tiled(c1_scene, cam)
     _, dl = oracle32.loss(ref["image"], gt, 1)
     g = r.backward(dl)
-    go = oracle32.backward(c1_scene, cam, dl, ref)
+    go = oracle32.backward(c1_scene, cam, dl, ref, threads=oracle32.max_threads)
     for k in ("d_vertices", "d_densities", "d_color_grads", "d_base_colors"):
         e = rel_l2(g[k], go[k])
         assert e <= GRAD_TOL, (k, e)

@@ -42,7 +42,7 @@ def test_sh_forward_parity(c2_scene, oracle32, res):
 
 
 def test_sh_backward_parity(c2_scene, oracle32):
-    cam = c1_camera(256, 256)
+    cam = c1_camera(512, 512)  # the configuration's stated resolution
     r = make_renderer(c2_scene, cam, sh=True)
     r.forward_tiled(cam.cam_pos, cam.vp, cam.c2w_intrinsics)
     shv, deg = _oracle_sh(oracle32, c2_scene)
@@ -50,7 +50,7 @@ def test_sh_backward_parity(c2_scene, oracle32):
     gt = np.random.default_rng(0).uniform(0, 1, (cam.height, cam.width, 3)).astype(np.float32)
     _, dl = oracle32.loss(ref["image"], gt, 1)
     g = r.backward(dl)
-    go = oracle32.backward(c2_scene, cam, dl, ref, sh=shv, sh_degree=deg)
+    go = oracle32.backward(c2_scene, cam, dl, ref, threads=oracle32.max_threads, sh=shv, sh_degree=deg)
     assert np.abs(g["d_base_colors"]).max() == 0.0
     for k, ko in (("d_vertices", "d_vertices"), ("d_densities", "d_densities"), ("d_color_grads", "d_color_grads"),
                   ("d_sh_coeffs", "d_sh")):
