@@ -116,7 +116,9 @@ struct __align__(16) TileSmem {
   uint32_t toff[kBatch + 1];   // tet-major item offsets
   uint32_t pmask[TS * TS];
   short2 span[kBatch][TS];
-  uint16_t rowpref[kBatch][TS + 1];
+  // per (tet, row): item index of the row's column 0 -- relative to the tet's
+  // first item after the prefixes, to the sub-batch's first item after fill
+  int16_t rowoff[kBatch][TS];
   uint16_t ipix[TileCfg<TS, AUX>::CAP];  // (tet slot << 8) | pixel of each item of the sub-batch (tet-major)
   uint64_t bar[2];
   float lsum[16];
@@ -411,11 +413,10 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
       if (tid < nb) {
         const int k = tid;
         uint32_t acc = 0;
-        s.rowpref[k][0] = 0;
         for (int r = 0; r < TS; ++r) {
           const short2 sp = s.span[k][r];
+          s.rowoff[k][r] = (int16_t)((int)acc - (int)sp.x);
           acc += (uint32_t)max(sp.y - sp.x + 1, 0);
-          s.rowpref[k][r + 1] = (uint16_t)acc;
         }
         cnt = acc;
       }
@@ -440,7 +441,10 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
         const int k = task / TS, row = task - (task / TS) * TS;
         const short2 sp = s.span[k][row];
         if (sp.x > sp.y) continue;
-        const uint32_t base = s.toff[k] - base0 + s.rowpref[k][row];
+        // rebase the row's offset onto the sub-batch (read by item_of)
+        const int ro = (int)s.rowoff[k][row] + (int)(s.toff[k] - base0);
+        s.rowoff[k][row] = (int16_t)ro;
+        const uint32_t base = (uint32_t)(ro + sp.x);
         for (int c = sp.x; c <= sp.y; ++c) {
           s.ipix[base + (uint32_t)(c - sp.x)] = (uint16_t)((k << 8) | (row * TS + c));
           atomicOr(&s.pmask[row * TS + c], 1u << k);
@@ -454,9 +458,8 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
       p = (int)(e & 255u);
     };
     // item index of (tet k, this thread's pixel) inside the current sub-batch
-    auto item_of = [&](int k, uint32_t base) -> uint32_t {
-      return s.toff[k] - base + s.rowpref[k][prow] + (uint32_t)(pcol - s.span[k][prow].x);
-    };
+    // (one shared load: fill rebased the row offsets onto the sub-batch)
+    auto item_of = [&](int k, uint32_t) -> uint32_t { return (uint32_t)((int)s.rowoff[k][prow] + pcol); };
     // sub-batch end (>= k0 + 1): the batch's remaining items split into the
     // fewest sub-batches of at most CAP items, of about equal size, so that
     // no short remainder leaves most threads of a phase idle
@@ -936,132 +939,152 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
             // rebuilt from them once per tet at flush time.  Moments per item:
             //  [0] density  [1..3] base colour  [4] sum(sb)  [5..7] d * d(dc/dt)
             //  [8 + 4f] S_f  [9 + 4f .. 11 + 4f] P_f   (f = face 0..3)
-            float(*red)[kMomHalf + 1] = s.red[warp];
-            const uint32_t n_valid = n_items;
-            for (uint32_t chunk = (uint32_t)warp * 32u; chunk < n_items; chunk += (uint32_t)NT) {
-              const uint32_t i = chunk + (uint32_t)lane;
-              float m[8];  // density, base colour, sum(sb), d * d(dc/dt)
+            // Each tet's items are cut into runs of at most R consecutive items
+            // (its pixels along its rows), R chosen so that the sub-batch has at
+            // most one run per thread; thread t takes run t and sums its items'
+            // moments in registers (the 8 tet moments and (S, P) of each of the
+            // 4 faces).  The runs' sums (lanes in run order, so a tet's lanes are
+            // adjacent) are then combined per warp by a transpose through shared
+            // memory, half of the moments at a time: lane (h, q) with q < kMomHalf
+            // walks column q over rows [16h, 16h + 16) and adds a partial sum to
+            // the tet's moment at every tet boundary and at the end of its rows.
+            {
+              const int nsub = k1 - k0;
+              const uint32_t R = max(1u, (n_items + (uint32_t)(NT - nsub) - 1u) / (uint32_t)(NT - nsub));
+              float(*red)[kMomHalf + 1] = s.red[warp];
+              // cumulative run counts of the sub-batch's tets (each warp its own copy)
+              int* crun = reinterpret_cast<int*>(&red[0][0]);
+              {
+                int cnt = 0;
+                if (lane < nsub) cnt = (int)((s.toff[k0 + lane + 1] - s.toff[k0 + lane] + R - 1u) / R);
+                int x = cnt;
 #pragma unroll
-              for (int q = 0; q < 8; ++q) m[q] = 0.0f;
-              // the two faces the ray crosses: (face, s, s t d) for entry and exit
-              int fs0 = 0, fs1 = 0;
-              float sv0 = 0.f, px0 = 0.f, py0 = 0.f, pz0 = 0.f, sv1 = 0.f, px1 = 0.f, py1 = 0.f, pz1 = 0.f;
+                for (int o = 1; o < 32; o <<= 1) {
+                  const int y = __shfl_up_sync(0xffffffffu, x, o);
+                  if (lane >= o) x += y;
+                }
+                crun[lane + 1] = x;
+                if (lane == 0) crun[0] = 0;
+                __syncwarp();
+              }
               int k = -1;
-              if (i < n_valid) {
+              uint32_t i0 = 0, i1 = 0;
+              if (tid < crun[nsub]) {
+                int lo = 0, hi = nsub;  // crun[lo] <= tid < crun[hi]
+                while (hi - lo > 1) {
+                  const int mid = (lo + hi) >> 1;
+                  if (crun[mid] <= tid) lo = mid; else hi = mid;
+                }
+                k = k0 + lo;
+                i0 = s.toff[k] - base + (uint32_t)(tid - crun[lo]) * R;
+                i1 = min(i0 + R, s.toff[k + 1] - base);
+              }
+              __syncwarp();  // crun is overwritten by the transpose below
+              float acc[8], fac[16];
+#pragma unroll
+              for (int q = 0; q < 8; ++q) acc[q] = 0.0f;
+#pragma unroll
+              for (int q = 0; q < 16; ++q) fac[q] = 0.0f;
+              for (uint32_t i = i0; i < i1; ++i) {
                 const float4 st = s.item[i];
+                if (!(st.w >= 0.0f && st.z > 0.5f)) continue;  // ray miss or no gradient
                 const float4 ix = s.itemx[i];
                 const uint32_t pk = __float_as_uint(ix.z);
-                k = (int)((pk >> 5) & 31u);
-                if (st.w >= 0.0f && st.z > 0.5f) {
-                  const int p = (int)(pk >> 10);
-                  int fmin = (int)(pk & 7u);
-                  const int fmax = (int)((pk >> 3) & 3u);
-                  if (fmin == 4) fmin = 0;  // reference keeps min_face = 0 when no face enters
-                  const float t_min = ix.x, t_max = ix.y;
-                  const float t_prev = st.x, d_od_state = st.y;
-                  const float4 d = s.pdir[p];
-                  const float4 dlv = s.pdl[p];
-                  const TetView& tv = s.view[buf][k];
-                  const float4 cb = tv.cb;
-                  const float4 gg = tv.gm;
-                  const float dcdt = dot3x(gg.x, gg.y, gg.z, d.x, d.y, d.z);
-                  Integral I;
-                  integrate(cb, dcdt, t_min, t_max, I, ix.w);
-                  const float dcpr = clipf(dlv.x * t_prev, kMinVal, kMaxVal);
-                  const float dcpg = clipf(dlv.y * t_prev, kMinVal, kMaxVal);
-                  const float dcpb = clipf(dlv.z * t_prev, kMinVal, kMaxVal);
-                  float dph;
-                  if (fabsf(I.od) < 0.02f)
-                    dph = -0.5f + I.od * (1.0f / 3.0f + I.od * (-1.0f / 8.0f + I.od * (1.0f / 30.0f)));
-                  else
-                    dph = clipf(__fdividef(I.alpha_t * (I.od + 1.0f) - 1.0f, I.od * I.od), kMinVal, kMaxVal);
-                  const float dw0 = dph + I.alpha_t, dw1 = -dph;
-                  const float d_od_int = dcpr * (I.cer * dw0 + I.csr * dw1) + dcpg * (I.ceg * dw0 + I.csg * dw1) +
-                                         dcpb * (I.ceb * dw0 + I.csb * dw1);
-                  const float d_od = clipf(d_od_state + d_od_int, kMinVal, kMaxVal);
-                  const bool active = (I.od_raw >= 1e-8f) && (I.od_raw <= 88.0f);
-                  const float d_od_raw = active ? d_od : 0.0f;
-                  const float d_dist = clipf(d_od_raw * cb.w, kMinVal, kMaxVal);
-                  float d_tmin = -d_dist, d_tmax = d_dist;
-                  const float dsr = I.csr_r > 0.f ? dcpr * I.w1 : 0.f, dsg = I.csg_r > 0.f ? dcpg * I.w1 : 0.f,
-                              dsb = I.csb_r > 0.f ? dcpb * I.w1 : 0.f;
-                  const float der = I.cer_r > 0.f ? dcpr * I.w0 : 0.f, deg = I.ceg_r > 0.f ? dcpg * I.w0 : 0.f,
-                              deb = I.ceb_r > 0.f ? dcpb * I.w0 : 0.f;
-                  const float dbr = dsr + der, dbg = dsg + deg, dbb = dsb + deb;
-                  const float ss = dsr + dsg + dsb, se = der + deg + deb;
-                  const float d_dcdt = ss * t_min + se * t_max;
-                  d_tmin += ss * dcdt;
-                  d_tmax += se * dcdt;
-                  m[0] = clipf(d_od_raw * I.dist, kMinVal, kMaxVal);
-                  m[1] = clipf(dbr, kMinVal, kMaxVal);
-                  m[2] = clipf(dbg, kMinVal, kMaxVal);
-                  m[3] = clipf(dbb, kMinVal, kMaxVal);
-                  m[4] = dbr + dbg + dbb;
-                  m[5] = d.x * d_dcdt;
-                  m[6] = d.y * d_dcdt;
-                  m[7] = d.z * d_dcdt;
+                const int p = (int)(pk >> 10);
+                int fmin = (int)(pk & 7u);
+                const int fmax = (int)((pk >> 3) & 3u);
+                if (fmin == 4) fmin = 0;  // reference keeps min_face = 0 when no face enters
+                const float t_min = ix.x, t_max = ix.y;
+                const float t_prev = st.x, d_od_state = st.y;
+                const float4 d = s.pdir[p];
+                const float4 dlv = s.pdl[p];
+                const TetView& tv = s.view[buf][k];
+                const float4 cb = tv.cb;
+                const float4 gg = tv.gm;
+                const float dcdt = dot3x(gg.x, gg.y, gg.z, d.x, d.y, d.z);
+                Integral I;
+                integrate(cb, dcdt, t_min, t_max, I, ix.w);
+                const float dcpr = clipf(dlv.x * t_prev, kMinVal, kMaxVal);
+                const float dcpg = clipf(dlv.y * t_prev, kMinVal, kMaxVal);
+                const float dcpb = clipf(dlv.z * t_prev, kMinVal, kMaxVal);
+                float dph;
+                if (fabsf(I.od) < 0.02f)
+                  dph = -0.5f + I.od * (1.0f / 3.0f + I.od * (-1.0f / 8.0f + I.od * (1.0f / 30.0f)));
+                else
+                  dph = clipf(__fdividef(I.alpha_t * (I.od + 1.0f) - 1.0f, I.od * I.od), kMinVal, kMaxVal);
+                const float dw0 = dph + I.alpha_t, dw1 = -dph;
+                const float d_od_int = dcpr * (I.cer * dw0 + I.csr * dw1) + dcpg * (I.ceg * dw0 + I.csg * dw1) +
+                                       dcpb * (I.ceb * dw0 + I.csb * dw1);
+                const float d_od = clipf(d_od_state + d_od_int, kMinVal, kMaxVal);
+                const bool active = (I.od_raw >= 1e-8f) && (I.od_raw <= 88.0f);
+                const float d_od_raw = active ? d_od : 0.0f;
+                const float d_dist = clipf(d_od_raw * cb.w, kMinVal, kMaxVal);
+                float d_tmin = -d_dist, d_tmax = d_dist;
+                const float dsr = I.csr_r > 0.f ? dcpr * I.w1 : 0.f, dsg = I.csg_r > 0.f ? dcpg * I.w1 : 0.f,
+                            dsb = I.csb_r > 0.f ? dcpb * I.w1 : 0.f;
+                const float der = I.cer_r > 0.f ? dcpr * I.w0 : 0.f, deg = I.ceg_r > 0.f ? dcpg * I.w0 : 0.f,
+                            deb = I.ceb_r > 0.f ? dcpb * I.w0 : 0.f;
+                const float dbr = dsr + der, dbg = dsg + deg, dbb = dsb + deb;
+                const float ss = dsr + dsg + dsb, se = der + deg + deb;
+                const float d_dcdt = ss * t_min + se * t_max;
+                d_tmin += ss * dcdt;
+                d_tmax += se * dcdt;
+                acc[0] += clipf(d_od_raw * I.dist, kMinVal, kMaxVal);
+                acc[1] += clipf(dbr, kMinVal, kMaxVal);
+                acc[2] += clipf(dbg, kMinVal, kMaxVal);
+                acc[3] += clipf(dbb, kMinVal, kMaxVal);
+                acc[4] += dbr + dbg + dbb;
+                acc[5] += d.x * d_dcdt;
+                acc[6] += d.y * d_dcdt;
+                acc[7] += d.z * d_dcdt;
 #pragma unroll
-                  for (int side = 0; side < 2; ++side) {
-                    const int f = side == 0 ? fmin : fmax;
-                    const float dt = side == 0 ? d_tmin : d_tmax;
-                    const float tt = side == 0 ? t_min : t_max;
-                    const float4 nf = tv.nrm[f];
-                    const float den = (face_flipped(tv, f) ? -1.0f : 1.0f) * (nf.x * d.x + nf.y * d.y + nf.z * d.z);
-                    const float inv_den = fabsf(den) < kTiny ? clipf(1.0f / kTiny, kMinVal, kMaxVal)
-                                                             : clipf(__fdividef(1.0f, den), kMinVal, kMaxVal);
-                    const float sv = dt * inv_den, st_ = sv * tt;
-                    if (side == 0) { fs0 = f; sv0 = sv; px0 = st_ * d.x; py0 = st_ * d.y; pz0 = st_ * d.z; }
-                    else { fs1 = f; sv1 = sv; px1 = st_ * d.x; py1 = st_ * d.y; pz1 = st_ * d.z; }
+                for (int side = 0; side < 2; ++side) {
+                  const int f = side == 0 ? fmin : fmax;
+                  const float dt = side == 0 ? d_tmin : d_tmax;
+                  const float tt = side == 0 ? t_min : t_max;
+                  const float4 nf = tv.nrm[f];
+                  const float den = (face_flipped(tv, f) ? -1.0f : 1.0f) * (nf.x * d.x + nf.y * d.y + nf.z * d.z);
+                  const float inv_den = fabsf(den) < kTiny ? clipf(1.0f / kTiny, kMinVal, kMaxVal)
+                                                           : clipf(__fdividef(1.0f, den), kMinVal, kMaxVal);
+                  const float sv = dt * inv_den, st_ = sv * tt;
+#pragma unroll
+                  for (int ff = 0; ff < 4; ++ff) {
+                    if (f == ff) {
+                      fac[4 * ff] += sv;
+                      fac[4 * ff + 1] += st_ * d.x;
+                      fac[4 * ff + 2] += st_ * d.y;
+                      fac[4 * ff + 3] += st_ * d.z;
+                    }
                   }
                 }
               }
-              // transpose through shared memory, half of the moments at a time;
-              // lane (h, q) with q < kMomHalf then walks column q over rows
-              // [16h, 16h + 16) of the chunk, adding a partial sum to the tet's
-              // moment at every tet boundary and at the end of its rows
+              // warp combine of the runs' sums (lanes without a run come last)
               const int kp = __shfl_up_sync(0xffffffffu, k, 1);
               const unsigned heads = __ballot_sync(0xffffffffu, k >= 0 && (lane == 0 || kp != k));
-              const int n_rows = __popc(__ballot_sync(0xffffffffu, k >= 0));  // valid rows come first
-              const int wq = lane & 15, wr0 = (lane >> 4) * 16;
-              const int wr1 = min(wr0 + 16, n_rows);
+              const int n_rows = __popc(__ballot_sync(0xffffffffu, k >= 0));
+              if (n_rows > 0) {
+                const int wq = lane & 15, wr0 = (lane >> 4) * 16;
+                const int wr1 = min(wr0 + 16, n_rows);
 #pragma unroll
-              for (int hm = 0; hm < 2; ++hm) {
-                // row layout: half 0 = m[0..7] + face 0's (S, P); half 1 = faces 1..3,
-                // the two crossed faces placed by index (they differ unless both are
-                // face 0, which half 0 sums)
-                if (hm == 0) {
+                for (int hm = 0; hm < 2; ++hm) {
+                  // row layout: half 0 = the 8 tet moments + face 0's (S, P); half 1 = faces 1..3
 #pragma unroll
-                  for (int q = 0; q < 8; ++q) red[lane][q] = m[q];
-                  red[lane][8] = (fs0 == 0 ? sv0 : 0.f) + (fs1 == 0 ? sv1 : 0.f);
-                  red[lane][9] = (fs0 == 0 ? px0 : 0.f) + (fs1 == 0 ? px1 : 0.f);
-                  red[lane][10] = (fs0 == 0 ? py0 : 0.f) + (fs1 == 0 ? py1 : 0.f);
-                  red[lane][11] = (fs0 == 0 ? pz0 : 0.f) + (fs1 == 0 ? pz1 : 0.f);
-                } else {
-#pragma unroll
-                  for (int q = 0; q < kMomHalf; ++q) red[lane][q] = 0.0f;
-                  if (fs0 > 0) {
-                    float* r4 = &red[lane][4 * (fs0 - 1)];
-                    r4[0] = sv0; r4[1] = px0; r4[2] = py0; r4[3] = pz0;
+                  for (int q = 0; q < kMomHalf; ++q) red[lane][q] = hm == 0 ? (q < 8 ? acc[q] : fac[q - 8]) : fac[4 + q];
+                  red[lane][kMomHalf] = __int_as_float(k);
+                  __syncwarp();
+                  if (wq < kMomHalf && wr0 < wr1) {
+                    const int col = hm * kMomHalf + wq;
+                    for (int r0 = wr0; r0 < wr1;) {  // one tet segment [r0, r1) at a time
+                      const unsigned later = heads & ~((2u << r0) - 1u);
+                      const int r1 = later ? min(__ffs(later) - 1, wr1) : wr1;
+                      float sum = 0.0f;
+                      for (int row = r0; row < r1; ++row) sum += red[row][wq];
+                      if (sum != 0.0f) atomicAdd(&s.mom[__float_as_int(red[r0][kMomHalf])][col], sum);
+                      r0 = r1;
+                    }
                   }
-                  if (fs1 > 0) {
-                    float* r4 = &red[lane][4 * (fs1 - 1)];
-                    r4[0] = sv1; r4[1] = px1; r4[2] = py1; r4[3] = pz1;
-                  }
+                  __syncwarp();
                 }
-                red[lane][kMomHalf] = __int_as_float(k);
-                __syncwarp();
-                if (wq < kMomHalf && wr0 < wr1) {
-                  const int col = hm * kMomHalf + wq;
-                  for (int r0 = wr0; r0 < wr1;) {  // one tet segment [r0, r1) at a time
-                    const unsigned later = heads & ~((2u << r0) - 1u);
-                    const int r1 = later ? min(__ffs(later) - 1, wr1) : wr1;
-                    float sum = 0.0f;
-                    for (int row = r0; row < r1; ++row) sum += red[row][wq];
-                    if (sum != 0.0f) atomicAdd(&s.mom[__float_as_int(red[r0][kMomHalf])][col], sum);
-                    r0 = r1;
-                  }
-                }
-                __syncwarp();
               }
             }
             const int k2 = k1 < nb ? sub_end(k1, nb) : nb;
