@@ -340,12 +340,65 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
       }
       return sp;
     };
+    // Row table of the batch, kept in registers by every warp: lane l < nb holds
+    // tet l's first row and row count under the forward's reach rule (a row is
+    // reached when an edge crosses its centre or a vertex lies in it; the
+    // adjoint's rows, edge crossings only, are a subset) clipped to the image,
+    // and the inclusive prefix of the counts.  Span, prefix and fill tasks are
+    // (tet, reachable row) pairs numbered through this prefix, so no thread
+    // works on a row the tet cannot touch.
+    int rr_lo = 0, rr_n = 0, rr_pre = 0, rr_total = 0;
+    auto row_ranges = [&](int buf, int nb) {
+      int lo = 0, n = 0;
+      if (lane < nb) {
+        const TetView& tv = s.view[buf][lane];
+        if (!((__float_as_uint(tv.gm.w) >> 4) & 1u)) {
+          const float4 gy4 = tv.py;
+          // min/max of the tile-local y (subtracting the tile origin is monotonic)
+          const float ylo = fs(fminf(fminf(gy4.x, gy4.y), fminf(gy4.z, gy4.w)), tile_oy);
+          const float yhi = fs(fmaxf(fmaxf(gy4.x, gy4.y), fmaxf(gy4.z, gy4.w)), tile_oy);
+          // row r is reached iff yhi >= r and ylo < r + 1, i.e. floor(ylo) <= r <= floor(yhi)
+          const float flo = fmaxf(floorf(ylo), 0.0f);
+          const float fhi = fminf(floorf(yhi), (float)(valid_rows - 1));
+          if (flo <= fhi) {
+            lo = (int)flo;
+            n = (int)fhi - lo + 1;
+          }
+        }
+      }
+      int x = n;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+      }
+      rr_lo = lo;
+      rr_n = n;
+      rr_pre = x;
+      rr_total = __shfl_sync(0xffffffffu, x, 31);
+    };
+    // tet of task t: the first tet whose inclusive prefix exceeds t (all lanes call)
+    auto task_tet = [&](int t) -> int {
+      int k = 0;
+#pragma unroll
+      for (int st = 16; st > 0; st >>= 1) {
+        const int pv = __shfl_sync(0xffffffffu, rr_pre, k + st - 1);
+        if (pv <= t) k += st;
+      }
+      return k;
+    };
+    // row of task t of tet k (all lanes call)
+    auto task_row = [&](int t, int k) -> int { return __shfl_sync(0xffffffffu, rr_lo - (rr_pre - rr_n), k) + t; };
     // cache: the forward (vertex_rows) also stores each task's adjoint span
     // (edge crossings only) at its list position first + dir * k
     auto spans = [&](int buf, int nb, bool vertex_rows, short2* cache, uint32_t first, int dir) {
+      row_ranges(buf, nb);
       for (int i = tid; i < TS * TS; i += NT) s.pmask[i] = 0u;
-      for (int task = tid; task < nb * TS; task += NT) {
-        const int k = task / TS, row = task - (task / TS) * TS;
+      for (int t0 = warp * 32; t0 < rr_total; t0 += NT) {  // warp-uniform trip count
+        const int t = t0 + lane;
+        const int k = task_tet(t);
+        const int row = task_row(t, k);
+        if (t >= rr_total) continue;
         short2 sp = make_short2(0, -1);
         short2* slot = nullptr;
         if (cache) {
@@ -356,7 +409,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
           }
         }
         const TetView& tv = s.view[buf][k];
-        if (!((__float_as_uint(tv.gm.w) >> 4) & 1u) && row < valid_rows) {
+        {
           const float4 gx4 = tv.px, gy4 = tv.py;
           const float vpx[4] = {gx4.x - tile_ox, gx4.y - tile_ox, gx4.z - tile_ox, gx4.w - tile_ox};
           const float vpy[4] = {gy4.x - tile_oy, gy4.y - tile_oy, gy4.z - tile_oy, gy4.w - tile_oy};
@@ -402,26 +455,29 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
         s.span[k][row] = sp;
       }
     };
-    // the adjoint's spans of a cached batch, already copied into span_pf
-    auto cached_spans = [&](int nb) {
+    // the adjoint's spans of a cached batch, already copied into span_pf (the
+    // forward wrote every row of the table above for each cached tet)
+    auto cached_spans = [&](int buf, int nb) {
+      row_ranges(buf, nb);
       for (int i = tid; i < TS * TS; i += NT) s.pmask[i] = 0u;
       for (int task = tid; task < nb * TS; task += NT) (&s.span[0][0])[task] = (&s.span_pf[0][0])[task];
     };
-    // per-tet row prefix sums and tet-major item offsets (after spans)
+    // per-tet row prefix sums over the tet's reachable rows and tet-major item
+    // offsets (after spans; warp 0, lane = tet)
     auto prefixes = [&](int nb) {
-      uint32_t cnt = 0;
-      if (tid < nb) {
-        const int k = tid;
-        uint32_t acc = 0;
-        for (int r = 0; r < TS; ++r) {
-          const short2 sp = s.span[k][r];
-          s.rowoff[k][r] = (int16_t)((int)acc - (int)sp.x);
-          acc += (uint32_t)max(sp.y - sp.x + 1, 0);
+      if (warp == 0) {
+        uint32_t cnt = 0;
+        if (lane < nb) {
+          const int k = lane;
+          uint32_t acc = 0;
+          for (int r = rr_lo; r < rr_lo + rr_n; ++r) {
+            const short2 sp = s.span[k][r];
+            s.rowoff[k][r] = (int16_t)((int)acc - (int)sp.x);
+            acc += (uint32_t)max(sp.y - sp.x + 1, 0);
+          }
+          cnt = acc;
         }
-        cnt = acc;
-      }
-      if (warp == 0) {  // exclusive scan over the batch's tets (nb <= 32)
-        uint32_t x = cnt;
+        uint32_t x = cnt;  // exclusive scan over the batch's tets (nb <= 32)
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
           const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
@@ -437,8 +493,14 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
     // its closing barrier); the coverage bits of later tets are masked off there.
     auto fill = [&](int k0, int k1) {
       const uint32_t base0 = s.toff[k0];
-      for (int task = tid + k0 * TS; task < k1 * TS; task += NT) {
-        const int k = task / TS, row = task - (task / TS) * TS;
+      // tasks of tets [k0, k1) in the row table
+      const int tb = __shfl_sync(0xffffffffu, rr_pre - rr_n, k0);
+      const int te = k1 >= 32 ? rr_total : __shfl_sync(0xffffffffu, rr_pre - rr_n, k1);
+      for (int t0 = tb + warp * 32; t0 < te; t0 += NT) {  // warp-uniform trip count
+        const int t = t0 + lane;
+        const int k = task_tet(t);
+        const int row = task_row(t, k);
+        if (t >= te) continue;
         const short2 sp = s.span[k][row];
         if (sp.x > sp.y) continue;
         // rebase the row's offset onto the sub-batch (read by item_of)
@@ -885,7 +947,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
           // adjoint: edge crossings only, from the forward's cache when it
           // covered the whole batch
           if (span_cached(lo, nb))
-            cached_spans(nb);
+            cached_spans(buf, nb);
           else
             spans(buf, nb, false, nullptr, 0u, 0);
           __syncthreads();
