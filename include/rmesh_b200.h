@@ -185,6 +185,21 @@ RMESH_API int rmesh_forward_views(RmeshCtx* ctx, const RmeshCamera* cams, int32_
 RMESH_API int rmesh_backward(RmeshCtx* ctx, const float* dl_d_image, float* d_vertices, float* d_densities,
                    float* d_base_colors, float* d_color_grads);
 
+/* backward with the custom aux channels' gradient: the dl_d_aux argument and
+ * d_aux_data output of the reference's backward (lib.rs:2043-2090, buffers
+ * :702-704, 745-763).  dl_d_aux [H][W][aux_dim] (NULL: zero) is the loss
+ * gradient of the aux image's custom channels (those after the eight fixed
+ * ones of rmesh_forward_tiled's aux_out); d_aux_data [M][aux_dim] receives the
+ * gradient of the per-tet aux data, and the other outputs also carry the aux
+ * channels' optical-depth terms.  The aux channels composite as
+ * aux += T * alpha * a[tet] (rasterize_compute.wgsl:458-462); the adjoint is
+ * the exact derivative of that sum (its d_aux_data term is the reference's
+ * backward_interval_tiled.wgsl:637-649).  Same rules as rmesh_backward;
+ * a context with aux_dim 0 gives rmesh_backward's results. */
+RMESH_API int rmesh_backward_aux(RmeshCtx* ctx, const float* dl_d_image, const float* dl_d_aux, float* d_vertices,
+                                 float* d_densities, float* d_base_colors, float* d_color_grads,
+                                 float* d_aux_data);
+
 /* forward_error, lib.rs:1621-1710 (the kernel: crates/rmesh-error/src/wgsl/
  * error_tiled_compute.wgsl): per-tet error statistics over the tile lists of
  * the last rmesh_forward_tiled.  pixel_err, ssim_err [H*W]; outputs

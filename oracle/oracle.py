@@ -69,6 +69,7 @@ class Oracle:
         self._loss = getattr(L, "orc_loss" + s)
         self._loss.restype = ctypes.c_double
         self._backward = getattr(L, "orc_backward" + s)
+        self._backward_aux = getattr(L, "orc_backward_aux" + s)
         self._adam = getattr(L, "orc_adam" + s)
         self._sh_backward = getattr(L, "orc_sh_backward" + s)
         rt = ctypes.c_float if dtype == "f32" else ctypes.c_double
@@ -186,7 +187,10 @@ class Oracle:
                          _ptr(self._r(gt), self.rp), _ptr(dl, self.rp))
         return float(val), dl.reshape(H, W, 4)
 
-    def backward_raw(self, scene, cam, colors, vals, ranges, dl, rendered, tile_size=12, threads=1):
+    def backward_raw(self, scene, cam, colors, vals, ranges, dl, rendered, tile_size=12, threads=1,
+                     aux_data=None, dl_aux=None):
+        """With aux_data [M*aux_dim] and dl_aux [H*W*aux_dim] also returns
+        d_aux_data (the custom aux channels' adjoint, see orc_backward_aux)."""
         vp, c2w, intr, cp, W, H = self._cam(cam)
         n = scene["vertices"].size
         m = scene["indices"].size // 4
@@ -194,14 +198,21 @@ class Oracle:
         dd = np.zeros(m, dtype=self.np)
         dg = np.zeros(3 * m, dtype=self.np)
         db = np.zeros(3 * m, dtype=self.np)
-        self._backward(_ptr(self._r(scene["vertices"]), self.rp), _ptr(self._u(scene["indices"]), _u32p),
-                       _ptr(self._r(colors), self.rp), _ptr(self._r(scene["densities"]), self.rp),
-                       _ptr(self._r(scene["color_grads"]), self.rp), _ptr(self._u(vals), _u32p),
-                       _ptr(self._u(ranges), _u32p), _ptr(vp, self.rp), _ptr(c2w, self.rp), _ptr(intr, self.rp),
-                       _ptr(cp, self.rp), ctypes.c_int(W), ctypes.c_int(H), ctypes.c_int(tile_size),
-                       _ptr(self._r(dl), self.rp), _ptr(self._r(rendered), self.rp), _ptr(dv, self.rp),
-                       _ptr(dd, self.rp), _ptr(dg, self.rp), _ptr(db, self.rp), ctypes.c_int(threads))
-        return {"d_vertices": dv, "d_densities": dd, "d_color_grads": dg, "d_base_colors": db}
+        aux_dim = 0 if aux_data is None or dl_aux is None else int(np.asarray(aux_data).size // m)
+        da = np.zeros(max(aux_dim, 1) * m, dtype=self.np)
+        self._backward_aux(_ptr(self._r(scene["vertices"]), self.rp), _ptr(self._u(scene["indices"]), _u32p),
+                           _ptr(self._r(colors), self.rp), _ptr(self._r(scene["densities"]), self.rp),
+                           _ptr(self._r(scene["color_grads"]), self.rp), _ptr(self._u(vals), _u32p),
+                           _ptr(self._u(ranges), _u32p), _ptr(vp, self.rp), _ptr(c2w, self.rp), _ptr(intr, self.rp),
+                           _ptr(cp, self.rp), ctypes.c_int(W), ctypes.c_int(H), ctypes.c_int(tile_size),
+                           _ptr(self._r(dl), self.rp), _ptr(self._r(rendered), self.rp), _ptr(dv, self.rp),
+                           _ptr(dd, self.rp), _ptr(dg, self.rp), _ptr(db, self.rp), ctypes.c_int(threads),
+                           _ptr(self._r(aux_data) if aux_dim else None, self.rp), ctypes.c_int(aux_dim),
+                           _ptr(self._r(dl_aux) if aux_dim else None, self.rp), _ptr(da, self.rp))
+        out = {"d_vertices": dv, "d_densities": dd, "d_color_grads": dg, "d_base_colors": db}
+        if aux_dim:
+            out["d_aux_data"] = da
+        return out
 
     def error_stats(self, scene, cam, fwd, pixel_err, ssim_err, tile_size=12, min_t=0.0):
         """Per-tet error statistics (error_tiled_compute.wgsl:90-373) over the
@@ -267,13 +278,15 @@ class Oracle:
                    unsorted=(lo, hi, vals))
         return out
 
-    def backward(self, scene, cam, dl_d_image, fwd, tile_size=12, threads=1, sh=None, sh_degree=0):
+    def backward(self, scene, cam, dl_d_image, fwd, tile_size=12, threads=1, sh=None, sh_degree=0,
+                 aux_data=None, dl_aux=None):
         """lib.rs:1894-2031 (the sort it redoes equals the forward's).  With sh
         (the coefficient values of the forward), the colour gradient continues
         through the SH colour: d_sh is added, d_vertices and d_color_grads gain
         the colour's dependence on them, and d_base_colors is zero."""
         g = self.backward_raw(scene, cam, fwd["colors"], fwd["vals"], fwd["ranges"],
-                              np.asarray(dl_d_image).reshape(-1), fwd["image"].reshape(-1), tile_size, threads)
+                              np.asarray(dl_d_image).reshape(-1), fwd["image"].reshape(-1), tile_size, threads,
+                              aux_data=aux_data, dl_aux=None if dl_aux is None else np.asarray(dl_aux).reshape(-1))
         if sh is not None:
             g["d_sh"] = self.sh_backward(scene, cam, sh, sh_degree, fwd["visible"], g["d_base_colors"],
                                          g["d_vertices"], g["d_color_grads"])

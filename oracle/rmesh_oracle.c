@@ -851,10 +851,22 @@ EXPORT double SFX(orc_loss)(int W, int H, int loss_type, const R* rendered, cons
 /* accumulated (+=) into d_verts[3N], d_dens[M], d_cgrad[3M], d_base[3M].  */
 /* threads <= 1 runs tiles in order (deterministic sums).                  */
 /* ======================================================================== */
+/* Custom aux channels (aux_dim > 0, dl_aux != NULL): the forward composites   */
+/* aux[p][ai] += T alpha a[t][ai] (rasterize_compute.wgsl:458-462), i.e. each  */
+/* item adds the "colour" alpha a[t] with weight T.  Its adjoint follows the    */
+/* colour chain of this kernel: with s = sum_ai dl_aux[p][ai] a[t][ai], the     */
+/* running d(log T) gains alpha s T_prev, the item's optical depth gains        */
+/* T_prev alpha_t s (d alpha / d od = alpha_t), and d_aux[t][ai] gains          */
+/* dl_aux[p][ai] T_prev alpha.  (The reference's only aux adjoint is in its     */
+/* interval-tiled render mode, backward_interval_tiled.wgsl:637-649, whose d_aux */
+/* term is the same and whose optical-depth term is an approximation; the tiled */
+/* path has none.)                                                              */
 static void backward_tile(const Cam* cm, int64_t tile, const R* verts, const uint32_t* idx, const R* colors,
                           const R* dens, const R* cgrad, const uint32_t* vals, const uint32_t* ranges,
                           const R* dl, const R* rendered, R* d_verts, R* d_dens, R* d_cgrad, R* d_base,
-                          int use_atomics) {
+                          int use_atomics, const R* aux_data, int aux_dim, const R* dl_aux, R* d_aux) {
+    if (!dl_aux || !aux_data) aux_dim = 0;
+    R acc_aux[64];
     int W = cm->W, H = cm->H, TS = cm->TS;
     uint32_t tiles_x = (uint32_t)((W + TS - 1) / TS);
     uint32_t tile_x = (uint32_t)(tile % tiles_x), tile_y = (uint32_t)(tile / tiles_x);
@@ -890,6 +902,7 @@ static void backward_tile(const Cam* cm, int64_t tile, const R* verts, const uin
         V3 n[4];
         face_normals(v, n);
         R acc_d = 0;
+        for (int ai = 0; ai < aux_dim; ++ai) acc_aux[ai] = 0;
         V3 acc_v[4] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
         V3 acc_g = {0, 0, 0}, acc_b = {0, 0, 0};
         for (int r = 0; r < TS; ++r) {
@@ -925,12 +938,17 @@ static void backward_tile(const Cam* cm, int64_t tile, const R* verts, const uin
                 V3 dcol = v3(dl[4 * p], dl[4 * p + 1], dl[4 * p + 2]);
                 V3 dcp = vclip(vscale(dcol, t_prev), MIN_VAL, MAX_VAL);
                 R d_od_state = -d_log_t;
-                R d_old = clipr(d_log_t + vdot(dcol, cp) * t_prev, MIN_VAL, MAX_VAL);
+                R aux_s = 0;  /* sum_ai dl_aux[p][ai] a[t][ai] */
+                for (int ai = 0; ai < aux_dim; ++ai)
+                    aux_s += dl_aux[(size_t)p * aux_dim + ai] * aux_data[(size_t)t * aux_dim + ai];
+                R alpha = (R)1 - alpha_t;
+                R d_old = clipr(d_log_t + (vdot(dcol, cp) + alpha * aux_s) * t_prev, MIN_VAL, MAX_VAL);
                 dlt[pl] = d_old;
                 R dph = dphi_dx(od);
                 R dw0 = dph + alpha_t, dw1 = -dph;
                 V3 dce_i = vscale(dcp, w0), dcs_i = vscale(dcp, w1);
-                R d_od_int = vdot(dcp, vadd(vscale(ce, dw0), vscale(cs, dw1)));
+                R d_od_int = vdot(dcp, vadd(vscale(ce, dw0), vscale(cs, dw1))) + t_prev * alpha_t * aux_s;
+                for (int ai = 0; ai < aux_dim; ++ai) acc_aux[ai] += dl_aux[(size_t)p * aux_dim + ai] * t_prev * alpha;
                 R d_od = clipr(d_od_state + d_od_int, MIN_VAL, MAX_VAL);
                 R od_raw = density * dist;
                 int active = (od_raw >= (R)1e-8) && (od_raw <= (R)88.0);
@@ -973,6 +991,14 @@ static void backward_tile(const Cam* cm, int64_t tile, const R* verts, const uin
                 acc_g = vadd(acc_g, vclip(dgl, MIN_VAL, MAX_VAL));
             }
         }
+        for (int ai = 0; ai < aux_dim; ++ai) {
+            if (use_atomics) {
+#pragma omp atomic
+                d_aux[(size_t)t * aux_dim + ai] += acc_aux[ai];
+            } else {
+                d_aux[(size_t)t * aux_dim + ai] += acc_aux[ai];
+            }
+        }
         if (use_atomics) {
 #pragma omp atomic
             d_dens[t] += acc_d;
@@ -1009,23 +1035,36 @@ static void backward_tile(const Cam* cm, int64_t tile, const R* verts, const uin
     }
 }
 
-EXPORT void SFX(orc_backward)(const R* verts, const uint32_t* idx, const R* colors, const R* dens, const R* cgrad,
-                              const uint32_t* vals, const uint32_t* ranges, const R* vp, const R* c2w,
-                              const R* intr, const R* cam3, int W, int H, int TS, const R* dl, const R* rendered,
-                              R* d_verts, R* d_dens, R* d_cgrad, R* d_base, int threads) {
+/* orc_backward_aux -- orc_backward plus the custom aux channels' adjoint     */
+/* (see backward_tile): aux_data [M][aux_dim], dl_aux [H*W][aux_dim]; d_aux   */
+/* [M][aux_dim] is accumulated (+=).  aux_dim <= 64.                          */
+EXPORT void SFX(orc_backward_aux)(const R* verts, const uint32_t* idx, const R* colors, const R* dens,
+                                  const R* cgrad, const uint32_t* vals, const uint32_t* ranges, const R* vp,
+                                  const R* c2w, const R* intr, const R* cam3, int W, int H, int TS, const R* dl,
+                                  const R* rendered, R* d_verts, R* d_dens, R* d_cgrad, R* d_base, int threads,
+                                  const R* aux_data, int aux_dim, const R* dl_aux, R* d_aux) {
     Cam cm = {vp, c2w, intr, cam3, W, H, TS, (R)0};
     uint32_t tiles_x = (uint32_t)((W + TS - 1) / TS), tiles_y = (uint32_t)((H + TS - 1) / TS);
     int64_t ntiles = (int64_t)tiles_x * tiles_y;
+    if (aux_dim > 64) aux_dim = 64;
     if (threads <= 1) {
         for (int64_t tile = 0; tile < ntiles; ++tile)
             backward_tile(&cm, tile, verts, idx, colors, dens, cgrad, vals, ranges, dl, rendered, d_verts, d_dens,
-                          d_cgrad, d_base, 0);
+                          d_cgrad, d_base, 0, aux_data, aux_dim, dl_aux, d_aux);
     } else {
 #pragma omp parallel for schedule(dynamic, 4) num_threads(threads)
         for (int64_t tile = 0; tile < ntiles; ++tile)
             backward_tile(&cm, tile, verts, idx, colors, dens, cgrad, vals, ranges, dl, rendered, d_verts, d_dens,
-                          d_cgrad, d_base, 1);
+                          d_cgrad, d_base, 1, aux_data, aux_dim, dl_aux, d_aux);
     }
+}
+
+EXPORT void SFX(orc_backward)(const R* verts, const uint32_t* idx, const R* colors, const R* dens, const R* cgrad,
+                              const uint32_t* vals, const uint32_t* ranges, const R* vp, const R* c2w,
+                              const R* intr, const R* cam3, int W, int H, int TS, const R* dl, const R* rendered,
+                              R* d_verts, R* d_dens, R* d_cgrad, R* d_base, int threads) {
+    SFX(orc_backward_aux)(verts, idx, colors, dens, cgrad, vals, ranges, vp, c2w, intr, cam3, W, H, TS, dl, rendered,
+                          d_verts, d_dens, d_cgrad, d_base, threads, NULL, 0, NULL, NULL);
 }
 
 /* ======================================================================== */

@@ -32,7 +32,7 @@ STAGE_NAMES = ("records", "project", "tet_sort", "emit", "pair_sort", "ranges", 
 EXPORTED = (
     "rmesh_create", "rmesh_destroy", "rmesh_last_error", "rmesh_abi_version", "rmesh_set_stream",
     "rmesh_set_min_t", "rmesh_set_tile_size", "rmesh_update_params", "rmesh_get_params", "rmesh_get_info",
-    "rmesh_forward_tiled", "rmesh_forward_views", "rmesh_backward",
+    "rmesh_forward_tiled", "rmesh_forward_views", "rmesh_backward", "rmesh_backward_aux",
     "rmesh_adam_state_size", "rmesh_get_adam_state", "rmesh_set_adam_state", "rmesh_train_step", "rmesh_train_step_views",
     "rmesh_debug_tiles_touched", "rmesh_debug_pairs", "rmesh_debug_ranges", "rmesh_set_profiling",
     "rmesh_stage_times", "rmesh_accumulate_views", "rmesh_grad_slots", "rmesh_apply_adam",
@@ -120,6 +120,7 @@ def load() -> ctypes.CDLL:
         "rmesh_get_adam_state": ([vp, vp, P(ctypes.c_uint32)], ctypes.c_int),
         "rmesh_set_adam_state": ([vp, vp, ctypes.c_uint32], ctypes.c_int),
         "rmesh_backward": ([vp, vp, vp, vp, vp, vp], ctypes.c_int),
+        "rmesh_backward_aux": ([vp, vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
         "rmesh_train_step": ([vp, P(Camera), vp, f32, f32, f32, i32, vp], ctypes.c_int),
         "rmesh_train_step_views": ([vp, P(Camera), i32, vp, P(TrainOpts), vp], ctypes.c_int),
         "rmesh_debug_tiles_touched": ([vp, vp], ctypes.c_int),

@@ -103,6 +103,7 @@ struct RmeshCtx {
   DevBuf rec, color4, grad_slot, csr_off, csr_ref;
   DevBuf sh, m_sh, v_sh;  // SH coefficients [M][3][nc] and their Adam moments
   DevBuf aux_data;        // [M][aux_dim] custom aux channels
+  DevBuf dl_aux, d_aux;   // backward: [pixels][aux_dim] loss gradient, [M][aux_dim] data gradient
 
   // per-run
   DevBuf views_d, counters_d, hp_d, sort_state, sort_status, scan_status;
@@ -1289,15 +1290,25 @@ int rmesh_forward_tiled(RmeshCtx* c, const RmeshCamera* cam, float* rgba_out, fl
   return fail(c, RMESH_ERR_PAIR_OVERFLOW, "pair buffers could not be grown enough");
 }
 
-int rmesh_backward(RmeshCtx* c, const float* dl, float* d_verts, float* d_dens, float* d_base, float* d_cgrad) {
-  if (!c || !dl) return RMESH_ERR_INVALID_ARG;
-  DevGuard dg__(c);
+// rmesh_backward and rmesh_backward_aux: dl_aux / d_aux only with aux channels
+static int backward_impl(RmeshCtx* c, const float* dl, const float* dl_aux, float* d_verts, float* d_dens,
+                         float* d_base, float* d_cgrad, float* d_aux) {
   if (!c->have_forward) return fail(c, RMESH_ERR_STATE, "backward() must follow forward_tiled()");
   const ViewParams& v = c->views_h[0];
   const uint64_t npix = (uint64_t)v.W * v.H;
+  const bool with_aux = c->aux_dim > 0 && (dl_aux || d_aux);
   CKR(ensure_buf(c, c->dl, npix * 16));
   CK(cudaMemcpyAsync(c->dl.p, dl, npix * 16, cudaMemcpyDefault, c->stream));
   CK(cudaMemsetAsync(c->grad_slot.p, 0, grad_floats(c) * 4, c->stream));
+  if (with_aux) {
+    CKR(ensure_buf(c, c->dl_aux, npix * (uint64_t)c->aux_dim * 4));
+    CKR(ensure_buf(c, c->d_aux, (uint64_t)c->M * c->aux_dim * 4));
+    if (dl_aux)
+      CK(cudaMemcpyAsync(c->dl_aux.p, dl_aux, npix * (uint64_t)c->aux_dim * 4, cudaMemcpyDefault, c->stream));
+    else
+      CK(cudaMemsetAsync(c->dl_aux.p, 0, npix * (uint64_t)c->aux_dim * 4, c->stream));
+    CK(cudaMemsetAsync(c->d_aux.p, 0, (uint64_t)c->M * c->aux_dim * 4, c->stream));
+  }
   Counters* cnt = c->counters_d.as<Counters>();
   CK(cudaMemsetAsync(&cnt->tile_ticket, 0, sizeof(uint32_t), c->stream));
   ViewParams* vd = c->views_d.as<ViewParams>();
@@ -1307,8 +1318,18 @@ int rmesh_backward(RmeshCtx* c, const float* dl, float* d_verts, float* d_dens, 
     TileArgs ta = base_tile_args(c, vd, 1, c->last_tiles, cnt);
     ta.rgba = c->rgba.as<float>();
     ta.dl_rgba = c->dl.as<float>();
-    CKR((launch_tile_m<kModeBackward, false>(c, ta, c->last_tiles, true)));
+    if (with_aux) {
+      ta.aux_data = c->aux_data.as<float>();
+      ta.aux_dim = c->aux_dim;
+      ta.dl_aux = c->dl_aux.as<float>();
+      ta.d_aux = c->d_aux.as<float>();
+      CKR((launch_tile_m<kModeBackward, true>(c, ta, c->last_tiles, true)));
+    } else {
+      CKR((launch_tile_m<kModeBackward, false>(c, ta, c->last_tiles, true)));
+    }
   }
+  if (d_aux && with_aux)
+    CK(cudaMemcpyAsync(d_aux, c->d_aux.p, (uint64_t)c->M * c->aux_dim * 4, cudaMemcpyDefault, c->stream));
   CKR(run_sh_backward(c, vd, 1, false));
   const size_t N = (size_t)c->N, M = (size_t)c->M;
   CKR(ensure_buf(c, c->out_a, 3 * N * 4));
@@ -1326,6 +1347,19 @@ int rmesh_backward(RmeshCtx* c, const float* dl, float* d_verts, float* d_dens, 
   if (d_cgrad) CK(cudaMemcpyAsync(d_cgrad, c->out_d.p, 3 * M * 4, cudaMemcpyDefault, c->stream));
   CKR(sync_counters(c, 1));
   return status_from_bits(c);
+}
+
+int rmesh_backward(RmeshCtx* c, const float* dl, float* d_verts, float* d_dens, float* d_base, float* d_cgrad) {
+  if (!c || !dl) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
+  return backward_impl(c, dl, nullptr, d_verts, d_dens, d_base, d_cgrad, nullptr);
+}
+
+int rmesh_backward_aux(RmeshCtx* c, const float* dl, const float* dl_aux, float* d_verts, float* d_dens,
+                       float* d_base, float* d_cgrad, float* d_aux) {
+  if (!c || !dl) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
+  return backward_impl(c, dl, dl_aux, d_verts, d_dens, d_base, d_cgrad, d_aux);
 }
 
 int rmesh_forward_error(RmeshCtx* c, const float* pixel_err, const float* ssim_err, float* tet_err,

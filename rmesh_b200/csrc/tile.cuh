@@ -68,6 +68,10 @@ struct TileArgs {
   const float* aux_data;       // [M][aux_dim] per-tet custom channels (aux_dim > 0)
   int aux_dim;
   const float* dl_rgba;        // [pixels][4] (backward mode)
+  // backward mode with AUX: gradient of the custom aux channels [pixels][aux_dim]
+  // and the per-tet aux data gradient [M][aux_dim] (accumulated)
+  const float* dl_aux;
+  float* d_aux;
   const float* gt_rgb;         // [pixels][3] (train mode)
   const float* pixel_err;      // [pixels] (error mode)
   const float* ssim_err;       // [pixels] (error mode)
@@ -110,7 +114,7 @@ struct __align__(16) TileSmem {
   float mom[kBatch][kMom];  // adjoint moments per tet (phase 2)
   float4 pdir[TS * TS];     // pixel ray direction
   float4 pdl[TS * TS];      // pixel dL/dRGB (adjoint)
-  float4 item[TileCfg<TS, AUX>::CAP];   // (cp.rgb, od) -> adjoint: (t_prev, d_od_state, has, -)
+  float4 item[TileCfg<TS, AUX>::CAP];   // (cp.rgb, od) -> adjoint: (t_prev, d_od_state, has, aux_s)
   float4 itemx[TileCfg<TS, AUX>::CAP];  // (t_min, t_max, packed faces | tet | pixel, alpha_t)
   float red[TileCfg<TS, AUX>::NW][32][kMomHalf + 1];  // per-warp transpose (odd row stride)
   uint32_t toff[kBatch + 1];   // tet-major item offsets
@@ -983,10 +987,20 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
                 logT = prev_logT;
                 if (t_prev >= 1e-6f) {
                   const float d_od_state = -dlogT;
-                  dlogT = clipf(dlogT + (dlr * c.x + dlg * c.y + dlb * c.z) * t_prev, kMinVal, kMaxVal);
-                  s.item[it] = make_float4(t_prev, d_od_state, 1.0f, 0.0f);
+                  // custom aux channels (aux += T alpha a[tet], rasterize_compute.wgsl:458-462)
+                  // continue the transmittance chain like a colour alpha a[tet]:
+                  // aux_s = sum_ai dl_aux[pixel][ai] a[tet][ai]
+                  float aux_s = 0.0f, aux_w = 0.0f;
+                  if (AUX && MODE == kModeBackward && a.dl_aux) {
+                    const float* dla = a.dl_aux + pix * (size_t)a.aux_dim;
+                    const float* ad = a.aux_data + (size_t)s.view[buf][k].meta.x * a.aux_dim;
+                    for (int ai = 0; ai < a.aux_dim; ++ai) aux_s += dla[ai] * ad[ai];
+                    aux_w = (1.0f - s.itemx[it].w) * aux_s;  // alpha * aux_s
+                  }
+                  dlogT = clipf(dlogT + (dlr * c.x + dlg * c.y + dlb * c.z + aux_w) * t_prev, kMinVal, kMaxVal);
+                  s.item[it] = make_float4(t_prev, d_od_state, 1.0f, aux_s);
                 } else {
-                  s.item[it].w = -1.0f;  // no gradient
+                  s.item[it] = make_float4(0.0f, 0.0f, 0.0f, -1.0f);  // no gradient
                 }
               }
             }
@@ -1049,7 +1063,9 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
               for (int q = 0; q < 16; ++q) fac[q] = 0.0f;
               for (uint32_t i = i0; i < i1; ++i) {
                 const float4 st = s.item[i];
-                if (!(st.w >= 0.0f && st.z > 0.5f)) continue;  // ray miss or no gradient
+                // (t_prev, d_od_state, 1, aux_s) for an item with a gradient; ray misses
+                // and items below the transmittance cut have z = 0
+                if (!(st.z > 0.5f)) continue;
                 const float4 ix = s.itemx[i];
                 const uint32_t pk = __float_as_uint(ix.z);
                 const int p = (int)(pk >> 10);
@@ -1077,7 +1093,23 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
                 const float dw0 = dph + I.alpha_t, dw1 = -dph;
                 const float d_od_int = dcpr * (I.cer * dw0 + I.csr * dw1) + dcpg * (I.ceg * dw0 + I.csg * dw1) +
                                        dcpb * (I.ceb * dw0 + I.csb * dw1);
-                const float d_od = clipf(d_od_state + d_od_int, kMinVal, kMaxVal);
+                float d_od_aux = 0.0f;
+                if (AUX && MODE == kModeBackward && a.dl_aux) {
+                  // the aux channels' own terms: d od += T_prev alpha_t aux_s (d alpha / d od =
+                  // alpha_t); d a[tet][ai] += dl_aux[pixel][ai] T_prev alpha
+                  d_od_aux = t_prev * I.alpha_t * st.w;
+                  const int pr = p / TS, pc = p - (p / TS) * TS;
+                  const size_t gp = (size_t)V.pix_base + (size_t)(tile_y * (uint32_t)TS + (uint32_t)pr) * (size_t)V.W +
+                                    (size_t)(tile_x * (uint32_t)TS + (uint32_t)pc);
+                  const float* dla = a.dl_aux + gp * (size_t)a.aux_dim;
+                  float* dst = a.d_aux + (size_t)tv.meta.x * a.aux_dim;
+                  const float wa = t_prev * (1.0f - I.alpha_t);
+                  for (int ai = 0; ai < a.aux_dim; ++ai) {
+                    const float v = dla[ai] * wa;
+                    if (v != 0.0f) atomicAdd(dst + ai, v);
+                  }
+                }
+                const float d_od = clipf(d_od_state + d_od_int + d_od_aux, kMinVal, kMaxVal);
                 const bool active = (I.od_raw >= 1e-8f) && (I.od_raw <= 88.0f);
                 const float d_od_raw = active ? d_od : 0.0f;
                 const float d_dist = clipf(d_od_raw * cb.w, kMinVal, kMaxVal);

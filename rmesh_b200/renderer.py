@@ -351,18 +351,39 @@ class RMeshRenderer:
         self._check(self._lib.rmesh_forward_tiled(self._ctx, ctypes.byref(cam), p, pa))
         return out
 
-    def backward(self, dl_d_image) -> dict:
+    def backward(self, dl_d_image, dl_d_aux=None) -> dict:
         """dict of 1-D float32 arrays d_vertices, d_densities, d_base_colors, d_color_grads
-        (and d_sh_coeffs when the colours come from SH coefficients)."""
+        (and d_sh_coeffs when the colours come from SH coefficients).
+
+        With custom aux channels (``aux_dim`` > 0) the dict also holds
+        ``d_aux_data`` [M * aux_dim], and ``dl_d_aux`` ([H, W, aux_dim], the loss
+        gradient of the aux image's custom channels; None = zero) contributes
+        to every gradient, as the reference's ``dl_d_aux`` argument
+        (crates/rmesh-python/src/lib.rs:2043-2090)."""
         obj, p = _as_array(dl_d_image, np.float32, "dl_d_image")
         if _numel(obj) != 4 * self._width * self._height:
             raise ValueError("dl_d_image must be [H, W, 4]")
         out = {"d_vertices": np.empty(3 * self._N, np.float32), "d_densities": np.empty(self._M, np.float32),
                "d_base_colors": np.empty(3 * self._M, np.float32),
                "d_color_grads": np.empty(3 * self._M, np.float32)}
-        self._check(self._lib.rmesh_backward(self._ctx, p, out["d_vertices"].ctypes.data,
-                                             out["d_densities"].ctypes.data, out["d_base_colors"].ctypes.data,
-                                             out["d_color_grads"].ctypes.data))
+        if self._aux_dim > 0:
+            pa = None
+            if dl_d_aux is not None:
+                aobj, pa = _as_array(dl_d_aux, np.float32, "dl_d_aux")
+                if _numel(aobj) != self._aux_dim * self._width * self._height:
+                    raise ValueError("dl_d_aux must be [H, W, aux_dim]")
+            out["d_aux_data"] = np.empty(self._aux_dim * self._M, np.float32)
+            self._check(self._lib.rmesh_backward_aux(self._ctx, p, pa, out["d_vertices"].ctypes.data,
+                                                     out["d_densities"].ctypes.data,
+                                                     out["d_base_colors"].ctypes.data,
+                                                     out["d_color_grads"].ctypes.data,
+                                                     out["d_aux_data"].ctypes.data))
+        else:
+            if dl_d_aux is not None:
+                raise ValueError("dl_d_aux needs a renderer with aux_dim > 0")
+            self._check(self._lib.rmesh_backward(self._ctx, p, out["d_vertices"].ctypes.data,
+                                                 out["d_densities"].ctypes.data, out["d_base_colors"].ctypes.data,
+                                                 out["d_color_grads"].ctypes.data))
         if self._sh_degree >= 0:
             out["d_sh_coeffs"] = self.sh_grad_into(np.empty(3 * self._nc * self._M, np.float32))
         return out
