@@ -206,10 +206,11 @@ def run_gpu(args):
     gt_dev = gt_host.to(f"cuda:{local}")
     torch.cuda.synchronize()
 
-    # tile size (and with it threads per tile and the pair-key width) picked by
-    # timing the step's forward + adjoint at 8, 12 and 16 (parameters unchanged)
-    tune_ms = None if args.no_autotune else r.autotune(cams, gt_dev, loss_type=1)
-    tile_size = int(r.info().tile_size)
+    # tile configuration (tile size x threads per tile, and per resolution)
+    # picked by timing the step's forward + adjoint over the whole grid
+    # (parameters unchanged); the pair-key width follows from the tile count
+    tune = None if args.no_autotune else r.autotune(cams, gt_dev, loss_type=1)
+    tile_size, tile_threads = r.tile_config()
     slots = r.grad_slots() if world > 1 else None
 
     def step(mode, gt):
@@ -315,7 +316,7 @@ def run_gpu(args):
         "dtype": "f32",
         "data": "synthetic (seeded Delaunay mesh, seeded targets)",
         "config": {**workload_config(args, r.n_tets, r.n_vertices, n_pix, world), "tile_size": tile_size,
-                   "autotune_ms_per_run": None if tune_ms is None else {str(k): round(v, 2) for k, v in tune_ms.items()}},
+                   "threads_per_tile": tile_threads, "autotune": tune},
         "mpix_per_s": round(world * n_pix / (ms_graph * 1e-3) / 1e6, 2),
         "plain": {"value": round(world * 1000.0 / ms_plain, 4), "unit": "train-steps/s", "ms_per_step": round(ms_plain, 4)},
         "batched_graph_vs_plain": round(ms_plain / ms_graph, 3),
@@ -331,7 +332,8 @@ def run_gpu(args):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
                      "traffic": int(TILE_DRAM_BYTES_PER_PAIR * int(info.n_pairs_last)),
-                     "kernel": f"tile_kernel<{tile_size},kModeTrain> (fused forward+loss+adjoint)",
+                     "kernel": f"tile_kernel<{tile_size},kModeTrain> (fused forward+loss+adjoint, "
+                               f"{tile_threads} threads per tile)",
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                      "fallback 6.65 TB/s", "launch_ms": round(comp_ms, 4), "algorithmic_bytes": alg,
                      "n_pairs": int(info.n_pairs_last)},
@@ -510,9 +512,12 @@ def run_training(args):
     W, H = cams[0].width, cams[0].height
 
     def renderer(sc, tile):
+        """tile: a tile size or a (tile size, threads per tile) configuration"""
+        ts, th = (tile, 0) if isinstance(tile, int) else tile
         r = RMeshRenderer(sc["vertices"], sc["indices"], sc["base_colors"], sc["densities"], sc["color_grads"],
-                          sc["circumdata"], W, H, tile_size=tile, sh_coeffs=sc["sh_coeffs"],
+                          sc["circumdata"], W, H, tile_size=ts, sh_coeffs=sc["sh_coeffs"],
                           sh_degree=args.sh_degree)
+        r.set_tile_config(ts, th)
         st = torch.cuda.Stream()
         r.set_stream(st.cuda_stream)
         return r, st
@@ -531,8 +536,8 @@ def run_training(args):
 
     # warm-up on a disposable student: module load, allocator, tile-size autotune
     rw, _ = renderer(student, args.tile_size)
-    tune_ms = None if args.no_autotune else rw.autotune(batches[0], dev[0], loss_type=1)
-    tile = int(rw.info().tile_size)
+    tune = None if args.no_autotune else rw.autotune(batches[0], dev[0], loss_type=1)
+    tile = rw.tile_config()
     for i in range(args.warmup):
         rw.train_step_views(batches[i % nb], dev[i % nb], loss_type=1, mode="graph", lr_sh=LR_SH, **LR)
     r0, _ = renderer(student, tile)
@@ -607,9 +612,8 @@ def run_training(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_graph, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded GMM teacher mesh renders the targets; perturbed student)",
-        "config": {**workload_config(args, n_tets, n_verts, n_pix, 1), "tile_size": tile,
-                   "autotune_ms_per_run": None if tune_ms is None else {str(k): round(v, 2)
-                                                                        for k, v in tune_ms.items()}},
+        "config": {**workload_config(args, n_tets, n_verts, n_pix, 1), "tile_size": tile[0],
+                   "threads_per_tile": tile[1], "autotune": tune},
         "mpix_per_s": round(n_pix / (ms_graph * 1e-3) / 1e6, 2),
         "plain": {"value": round(1000.0 / ms_plain, 4), "unit": "train-steps/s", "ms_per_step": round(ms_plain, 4),
                   "steps": n_plain},
@@ -622,7 +626,8 @@ def run_training(args):
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4),
                      "traffic": int(TILE_DRAM_BYTES_PER_PAIR * int(info.n_pairs_last)),
-                     "kernel": f"tile_kernel<{tile},kModeTrain> (fused forward+loss+adjoint)",
+                     "kernel": f"tile_kernel<{tile[0]},kModeTrain> (fused forward+loss+adjoint, "
+                               f"{tile[1]} threads per tile)",
                      "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else
                      "fallback 6.65 TB/s", "launch_ms": round(comp_ms, 4), "algorithmic_bytes": alg,
                      "n_pairs": int(info.n_pairs_last)},
@@ -761,7 +766,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-parity-check", action="store_true",
                     help="skip the oracle check of one view's image and gradients (outside the timed region)")
-    ap.add_argument("--no-autotune", action="store_true", help="keep --tile-size instead of timing 8/12/16")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep --tile-size instead of searching tile size x threads per tile (and per resolution)")
     ap.add_argument("--views", type=int, default=None, help="views per step (default: the workload's)")
     ap.add_argument("--sh-degree", type=int, default=3, choices=[-1, 0, 1, 2, 3],
                     help="SH degree of the colours (-1: base colours)")

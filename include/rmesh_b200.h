@@ -234,12 +234,56 @@ RMESH_API int rmesh_accumulate_views(RmeshCtx* ctx, const RmeshCamera* cams, int
                                      const RmeshTrainOpts* opts, float* loss_out);
 RMESH_API int rmesh_grad_slots(RmeshCtx* ctx, float** device_ptr, uint64_t* n_floats);
 
+/* Tile configurations (no reference counterpart; the reference fixes 12-pixel
+ * tiles, lib.rs:442).  A configuration is a tile size (8, 12 or 16) and the
+ * threads per tile: one per pixel rounded up to whole warps (64, 160, 256; pass
+ * 0 for it) or twice that (128, 320, 512: the item-parallel phases of the tile
+ * kernel get more threads and larger sub-batches, half as many tiles are
+ * resident per SM).  The pair-sort key width follows from the tile count.
+ * set_tile_config sets the default configuration; set_resolution_tile_config
+ * gives views of width x height their own (tile_size 0 removes it), so one
+ * multi-view step can run, e.g., its 256x256 views at tile 8 and the rest at
+ * 12 (the views of each configuration form one persistent launch).
+ * get_tile_config returns the configuration a view of that size would use
+ * (width, height 0: the default). */
+RMESH_API int rmesh_set_tile_config(RmeshCtx* ctx, int32_t tile_size, int32_t threads);
+RMESH_API int rmesh_set_resolution_tile_config(RmeshCtx* ctx, int32_t width, int32_t height, int32_t tile_size,
+                                               int32_t threads);
+RMESH_API int rmesh_get_tile_config(RmeshCtx* ctx, int32_t width, int32_t height, int32_t* tile_size,
+                                    int32_t* threads);
+
+/* One measurement of rmesh_autotune: ms per batched forward + loss + adjoint
+ * run of the views of width x height (0, 0: all views of the call; -1, -1:
+ * all views with the per-resolution configurations chosen) at tile_size /
+ * threads. */
+typedef struct {
+  int32_t width;
+  int32_t height;
+  int32_t tile_size;
+  int32_t threads;
+  float ms;
+} RmeshTuneEntry;
+
+/* Autotuner over the whole configuration grid (tile size x threads per tile):
+ * times every configuration on all views (no Adam, so the parameters are
+ * unchanged) and makes the fastest the default; with per_resolution != 0 and
+ * several resolutions among the views, also times every configuration on the
+ * views of each resolution, gives a resolution whose fastest configuration
+ * differs its own, and keeps those overrides only if the mixed step beats the
+ * best single configuration.  Every measurement goes to entries (up to
+ * max_entries; *n_entries = how many were made).  Reference design input:
+ * crates/rmesh-backward/examples/tile_size_sweep.rs:1-60. */
+RMESH_API int rmesh_autotune(RmeshCtx* ctx, const RmeshCamera* cams, int32_t n_views, const float* gt_rgb,
+                             const RmeshTrainOpts* opts, int32_t per_resolution, RmeshTuneEntry* entries,
+                             int32_t max_entries, int32_t* n_entries);
+
 /* Tile-size autotuner (no reference counterpart; the reference fixes 12):
  * times the batched forward + loss + adjoint of these views (no Adam, so the
  * parameters are unchanged) at tile sizes 8, 12 and 16 -- which also sets the
  * threads per tile (64, 160, 256) and the pair-sort key width -- keeps the
  * fastest and returns it in *tile_size_out; ms_out (optional, [3]) receives
- * the milliseconds per run of each size. */
+ * the milliseconds per run of each size.  Clears per-resolution configurations;
+ * rmesh_autotune searches the whole grid. */
 RMESH_API int rmesh_autotune_tile_size(RmeshCtx* ctx, const RmeshCamera* cams, int32_t n_views, const float* gt_rgb,
                                        const RmeshTrainOpts* opts, int32_t* tile_size_out, float* ms_out);
 RMESH_API int rmesh_apply_adam(RmeshCtx* ctx, const RmeshTrainOpts* opts);

@@ -32,13 +32,14 @@ STAGE_NAMES = ("records", "project", "tet_sort", "emit", "pair_sort", "ranges", 
 EXPORTED = (
     "rmesh_create", "rmesh_destroy", "rmesh_last_error", "rmesh_abi_version", "rmesh_set_stream",
     "rmesh_set_min_t", "rmesh_set_tile_size", "rmesh_update_params", "rmesh_get_params", "rmesh_get_info",
-    "rmesh_forward_tiled", "rmesh_forward_views", "rmesh_backward", "rmesh_backward_aux",
+    "rmesh_forward_tiled", "rmesh_forward_views", "rmesh_backward",
     "rmesh_adam_state_size", "rmesh_get_adam_state", "rmesh_set_adam_state", "rmesh_train_step", "rmesh_train_step_views",
     "rmesh_debug_tiles_touched", "rmesh_debug_pairs", "rmesh_debug_ranges", "rmesh_set_profiling",
     "rmesh_stage_times", "rmesh_accumulate_views", "rmesh_grad_slots", "rmesh_apply_adam",
     "rmesh_count_tiles_static", "rmesh_update_sh", "rmesh_get_sh", "rmesh_get_sh_grad", "rmesh_set_lr_sh",
     "rmesh_decode_scene", "rmesh_forward_error", "rmesh_set_aux_data", "rmesh_get_aux_data",
-    "rmesh_debug_timeouts", "rmesh_autotune_tile_size",
+    "rmesh_debug_timeouts", "rmesh_autotune_tile_size", "rmesh_backward_aux", "rmesh_set_tile_config",
+    "rmesh_set_resolution_tile_config", "rmesh_get_tile_config", "rmesh_autotune",
 )
 
 COUNTERS_BYTES = 792  # sizeof(rm::Counters), read back once per training run
@@ -77,6 +78,11 @@ class TrainOpts(ctypes.Structure):
         ("lr_base", ctypes.c_float), ("loss_type", ctypes.c_int32), ("mode", ctypes.c_int32),
         ("lr_sh", ctypes.c_float), ("reserved", ctypes.c_int32),
     ]
+
+
+class TuneEntry(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_int32), ("height", ctypes.c_int32), ("tile_size", ctypes.c_int32),
+                ("threads", ctypes.c_int32), ("ms", ctypes.c_float)]
 
 
 class Info(ctypes.Structure):
@@ -142,6 +148,10 @@ def load() -> ctypes.CDLL:
         "rmesh_get_aux_data": ([vp, vp], ctypes.c_int),
         "rmesh_debug_timeouts": ([vp], ctypes.c_int),
         "rmesh_autotune_tile_size": ([vp, P(Camera), i32, vp, P(TrainOpts), P(i32), vp], ctypes.c_int),
+        "rmesh_set_tile_config": ([vp, i32, i32], ctypes.c_int),
+        "rmesh_set_resolution_tile_config": ([vp, i32, i32, i32, i32], ctypes.c_int),
+        "rmesh_get_tile_config": ([vp, i32, i32, P(i32), P(i32)], ctypes.c_int),
+        "rmesh_autotune": ([vp, P(Camera), i32, vp, P(TrainOpts), i32, P(TuneEntry), i32, P(i32)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

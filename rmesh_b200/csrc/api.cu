@@ -88,6 +88,13 @@ struct RmeshCtx {
   bool own_stream = false;
   int64_t N = 0, M = 0;
   int width = 0, height = 0, tile_size = 12;
+  int tile_wide = 0;  // default tile configuration: tile_size, threads per tile doubled when set
+  // per-resolution tile configurations (views of that size use them)
+  struct ResConf {
+    int W, H, ts, wide;
+  };
+  std::vector<ResConf> res_conf;
+  int last_ts = 12, last_wide = 0;  // tile configuration of the last single-view forward
   float min_t = 0.0f;
   uint32_t step = 0;
   int sh_degree = -1;   // -1: base colours; 0..3: colours from SH coefficients
@@ -113,6 +120,7 @@ struct RmeshCtx {
   DevBuf rgba, aux, dl, gt, out_a, out_b, out_c, out_d;
   DevBuf span_cache;  // per-CTA adjoint span cache of persistent train launches
   DevBuf tile_order, order_hist;  // longest-first tile order of the run; bucket counts and cursors
+  DevBuf tickets;                 // persistent tile-queue heads, one per launch of a run
   DevBuf err_in, err_out;  // per-pixel error inputs, per-tet error statistics
   uint64_t cap_pairs = 0;
   uint64_t generation = 0;  // bumped whenever a buffer is reallocated
@@ -294,6 +302,56 @@ int ensure_buf(RmeshCtx* c, DevBuf& b, size_t bytes) {
     if (r__ != RMESH_OK) return r__; \
   } while (0)
 
+// ---------------------------------------------------------------- tile configurations
+// A tile configuration: tile size 8, 12 or 16 and the threads per tile (one per
+// pixel rounded up to whole warps, or twice that: WIDE).
+struct TileConf {
+  int ts = 12;
+  int wide = 0;
+  bool operator==(const TileConf& o) const { return ts == o.ts && wide == o.wide; }
+};
+constexpr int kMaxTileGroups = 8;
+
+int conf_threads(TileConf t) { return (t.wide ? 2 : 1) * (((t.ts * t.ts + 31) / 32) * 32); }
+int conf_minb(TileConf t) { return (t.wide ? 1 : 2) * (t.ts == 16 ? 1 : (t.ts == 12 ? 2 : 4)); }
+bool conf_from(int ts, int threads, TileConf* out) {
+  if (ts != 8 && ts != 12 && ts != 16) return false;
+  TileConf t{ts, 0};
+  if (threads == 0 || threads == conf_threads(t)) {
+    *out = t;
+    return true;
+  }
+  t.wide = 1;
+  if (threads == conf_threads(t)) {
+    *out = t;
+    return true;
+  }
+  return false;
+}
+
+// the configuration a view of this size runs with
+TileConf view_conf(const RmeshCtx* c, int W, int H) {
+  for (const auto& r : c->res_conf)
+    if (r.W == W && r.H == H) return TileConf{r.ts, r.wide};
+  return TileConf{c->tile_size, c->tile_wide};
+}
+
+// Views of one tile configuration are numbered back to back (contiguous global
+// tiles) and run as one persistent launch.
+struct TileGroup {
+  TileConf conf;
+  uint32_t tile_lo = 0, n_tiles = 0;
+};
+struct ViewPlan {
+  std::vector<int> order;        // order[i]: the caller's view placed at position i
+  std::vector<TileConf> conf;    // per caller view
+  std::vector<uint64_t> pix;     // first pixel of each caller view (caller order)
+  std::vector<TileGroup> groups;
+  uint64_t total_pix = 0;
+  uint32_t total_tiles = 0, max_tiles = 0;
+  int cache_units = 0;           // max over groups of resident CTAs per SM x tile size
+};
+
 // ---------------------------------------------------------------- sorting
 template <typename K>
 int radix_sort(RmeshCtx* c, K* keys, uint32_t* vals, K* keys_alt, uint32_t* vals_alt, const void* n_ptr, int n_is_u64,
@@ -350,13 +408,7 @@ int setup_sort_attrs() {
 // persistent grid (resident CTAs per SM the kernel is built for x SMs; a
 // larger grid runs without the cache)
 constexpr uint32_t kSpanCacheTets = 2048;
-uint64_t span_cache_slots(const RmeshCtx* c) {
-  const int minb = c->tile_size == 16 ? TileCfg<16, false>::MINB
-                                      : (c->tile_size == 12 ? TileCfg<12, false>::MINB : TileCfg<8, false>::MINB);
-  return (uint64_t)minb * (uint64_t)c->num_sms;
-}
-
-int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t total_tiles) {
+int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t total_tiles, int cache_units) {
   const uint64_t items = (uint64_t)n_views * (uint64_t)c->M;
   CKR(ensure_buf(c, c->vis_key, items * 8));
   CKR(ensure_buf(c, c->vis_key_alt, items * 8));
@@ -366,7 +418,8 @@ int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t
   CKR(ensure_buf(c, c->vis_cnt, items * 4));
   CKR(ensure_buf(c, c->vis_proj, items * 32));
   CKR(ensure_buf(c, c->vis_view, items * sizeof(TetView)));
-  CKR(ensure_buf(c, c->span_cache, span_cache_slots(c) * kSpanCacheTets * (uint64_t)c->tile_size * sizeof(short2)));
+  // resident CTAs x tile size of the largest configuration of the run
+  CKR(ensure_buf(c, c->span_cache, (uint64_t)cache_units * c->num_sms * kSpanCacheTets * sizeof(short2)));
   if (c->sh_degree >= 0) {
     CKR(ensure_buf(c, c->vis_color, items * 16));
     CKR(ensure_buf(c, c->vis_dcolor, items * 16));
@@ -383,7 +436,8 @@ int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t
   CKR(ensure_buf(c, c->scan_status, ((items + 255) / 256 + 2) * 8));
   CKR(ensure_buf(c, c->ranges, (uint64_t)std::max<uint32_t>(total_tiles, 1) * 8));
   CKR(ensure_buf(c, c->tile_order, (uint64_t)std::max<uint32_t>(total_tiles, 1) * 4));
-  CKR(ensure_buf(c, c->order_hist, 2 * kOrderBuckets * 4));
+  CKR(ensure_buf(c, c->order_hist, 2 * kOrderBuckets * 4 * kMaxTileGroups));
+  CKR(ensure_buf(c, c->tickets, kMaxTileGroups * 4));
   CKR(ensure_buf(c, c->rgba, std::max<uint64_t>(total_pixels, 1) * 16));
   return RMESH_OK;
 }
@@ -394,7 +448,7 @@ int upload_views(RmeshCtx* c, int n) {
   return RMESH_OK;
 }
 
-int fill_view(RmeshCtx* c, const RmeshCamera& cam, ViewParams& v, uint32_t tile_base, uint32_t pix_base) {
+int fill_view(RmeshCtx* c, const RmeshCamera& cam, ViewParams& v, uint32_t tile_base, uint32_t pix_base, TileConf tc) {
   if (cam.width <= 0 || cam.height <= 0 || cam.width > 65536 || cam.height > 65536)
     return fail(c, RMESH_ERR_INVALID_ARG, "camera width/height out of range");
   memset(&v, 0, sizeof(v));
@@ -418,11 +472,46 @@ int fill_view(RmeshCtx* c, const RmeshCamera& cam, ViewParams& v, uint32_t tile_
   v.Wf = (float)cam.width;
   v.Hf = (float)cam.height;
   v.n_pixels = (float)((uint32_t)cam.width * (uint32_t)cam.height);
-  v.TS = c->tile_size;
-  v.tiles_x = (cam.width + c->tile_size - 1) / c->tile_size;
-  v.tiles_y = (cam.height + c->tile_size - 1) / c->tile_size;
+  v.TS = tc.ts;
+  v.tiles_x = (cam.width + tc.ts - 1) / tc.ts;
+  v.tiles_y = (cam.height + tc.ts - 1) / tc.ts;
   v.tile_base = tile_base;
   v.pix_base = pix_base;
+  return RMESH_OK;
+}
+
+// Fills views_h[0..n) in plan order (views of one configuration together) and
+// the plan's groups.  plain: every view is its own run (tile ids from 0).
+int make_plan(RmeshCtx* c, const RmeshCamera* cams, int n_views, bool plain, ViewPlan& pl) {
+  pl = ViewPlan();
+  pl.conf.resize(n_views);
+  pl.pix.resize(n_views);
+  std::vector<TileConf> distinct;
+  for (int v = 0; v < n_views; ++v) {
+    pl.conf[v] = view_conf(c, cams[v].width, cams[v].height);
+    pl.pix[v] = pl.total_pix;
+    pl.total_pix += (uint64_t)cams[v].width * cams[v].height;
+    if (std::find(distinct.begin(), distinct.end(), pl.conf[v]) == distinct.end()) distinct.push_back(pl.conf[v]);
+  }
+  if ((int)distinct.size() > kMaxTileGroups) return fail(c, RMESH_ERR_INVALID_ARG, "too many tile configurations");
+  if (pl.total_pix >= (1ull << 32)) return fail(c, RMESH_ERR_INVALID_ARG, "too many pixels in one run");
+  for (const auto& tc : distinct) {
+    TileGroup g;
+    g.conf = tc;
+    g.tile_lo = pl.total_tiles;
+    for (int v = 0; v < n_views; ++v) {
+      if (!(pl.conf[v] == tc)) continue;
+      const int i = (int)pl.order.size();
+      pl.order.push_back(v);
+      CKR(fill_view(c, cams[v], c->views_h[i], plain ? 0u : pl.total_tiles, (uint32_t)pl.pix[v], tc));
+      const uint32_t t = (uint32_t)(c->views_h[i].tiles_x * c->views_h[i].tiles_y);
+      pl.total_tiles += t;
+      pl.max_tiles = std::max(pl.max_tiles, t);
+    }
+    g.n_tiles = pl.total_tiles - g.tile_lo;
+    pl.groups.push_back(g);
+    pl.cache_units = std::max(pl.cache_units, conf_minb(tc) * tc.ts);
+  }
   return RMESH_OK;
 }
 
@@ -440,7 +529,7 @@ int run_records(RmeshCtx* c, bool capturing) {
 
 // project -> tet sort -> emit -> pair sort -> ranges for n_views views at views_dev
 int run_bin(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t total_tiles, Counters* cnt,
-            bool capturing) {
+            bool capturing, const std::vector<TileGroup>& groups) {
   const uint64_t items = (uint64_t)n_views * (uint64_t)c->M;
   const unsigned nblk = (unsigned)((items + 255) / 256);
   unsigned long long* status = c->scan_status.as<unsigned long long>();
@@ -515,35 +604,43 @@ int run_bin(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t tota
     ranges_kernel<<<std::max(1, blocks), 256, 0, c->stream>>>(c->sorted_pair_key, &cnt->n_pairs, c->cap_pairs,
                                                                c->ranges.as<uint2>(), views_dev, n_views, cnt);
     CKL();
-    // longest-first order of the tiles for the persistent tile kernel
-    CK(cudaMemsetAsync(c->order_hist.p, 0, 2 * kOrderBuckets * 4, c->stream));
-    uint32_t* hist = c->order_hist.as<uint32_t>();
-    const int oblocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((total_tiles + 255) / 256, (uint64_t)c->num_sms * 2));
-    tile_order_hist_kernel<<<oblocks, 256, 0, c->stream>>>(c->ranges.as<uint2>(), total_tiles, hist);
-    CKL();
-    tile_order_scatter_kernel<<<oblocks, 256, 0, c->stream>>>(c->ranges.as<uint2>(), total_tiles, hist,
-                                                              hist + kOrderBuckets, c->tile_order.as<uint32_t>());
-    CKL();
+    // longest-first order of each launch's tiles for the persistent tile
+    // kernel (indices relative to the launch's first tile)
+    CK(cudaMemsetAsync(c->order_hist.p, 0, 2 * kOrderBuckets * 4 * groups.size(), c->stream));
+    CK(cudaMemsetAsync(c->tickets.p, 0, kMaxTileGroups * 4, c->stream));
+    for (size_t gi = 0; gi < groups.size(); ++gi) {
+      const TileGroup& g = groups[gi];
+      if (g.n_tiles == 0) continue;
+      uint32_t* hist = c->order_hist.as<uint32_t>() + 2 * kOrderBuckets * gi;
+      const int oblocks =
+          (int)std::max<uint64_t>(1, std::min<uint64_t>((g.n_tiles + 255) / 256, (uint64_t)c->num_sms * 2));
+      tile_order_hist_kernel<<<oblocks, 256, 0, c->stream>>>(c->ranges.as<uint2>() + g.tile_lo, g.n_tiles, hist);
+      CKL();
+      tile_order_scatter_kernel<<<oblocks, 256, 0, c->stream>>>(c->ranges.as<uint2>() + g.tile_lo, g.n_tiles, hist,
+                                                                hist + kOrderBuckets,
+                                                                c->tile_order.as<uint32_t>() + g.tile_lo);
+      CKL();
+    }
   }
   return RMESH_OK;
 }
 
-template <int TS, int MODE, bool AUX>
+template <int TS, int MODE, bool AUX, bool WIDE>
 int launch_tile_t(RmeshCtx* c, TileArgs& ta, uint32_t n_tiles, bool persistent) {
-  constexpr int NT = TileCfg<TS, AUX>::NT;
-  constexpr size_t smem = sizeof(TileSmem<TS, AUX>);
+  constexpr int NT = TileCfg<TS, AUX, WIDE>::NT;
+  constexpr size_t smem = sizeof(TileSmem<TS, AUX, WIDE>);
   static PerDeviceOnce attrs;  // per instantiation and device
   CK(attrs.run([]() -> cudaError_t {
-    cudaError_t e = cudaFuncSetAttribute(tile_kernel<TS, MODE, AUX>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(tile_kernel<TS, MODE, AUX, WIDE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     // the whole unified L1 as shared memory: resident CTAs are limited by it
-    return cudaFuncSetAttribute(tile_kernel<TS, MODE, AUX>, cudaFuncAttributePreferredSharedMemoryCarveout,
+    return cudaFuncSetAttribute(tile_kernel<TS, MODE, AUX, WIDE>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                 (int)cudaSharedmemCarveoutMaxShared);
   }));
   unsigned grid = n_tiles;
   if (persistent) {
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tile_kernel<TS, MODE, AUX>, NT, smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, tile_kernel<TS, MODE, AUX, WIDE>, NT, smem);
     grid = (unsigned)std::max(1, occ) * (unsigned)c->num_sms;
     grid = std::min<unsigned>(grid, std::max<uint32_t>(n_tiles, 1));
   }
@@ -554,19 +651,40 @@ int launch_tile_t(RmeshCtx* c, TileArgs& ta, uint32_t n_tiles, bool persistent) 
     ta.span_cache_tets = kSpanCacheTets;
   }
   if (grid == 0) return RMESH_OK;
-  tile_kernel<TS, MODE, AUX><<<grid, NT, smem, c->stream>>>(ta);
+  tile_kernel<TS, MODE, AUX, WIDE><<<grid, NT, smem, c->stream>>>(ta);
   CKL();
   return RMESH_OK;
 }
 
+// one launch over the tiles of a group (ta.tile_lo, ta.ticket set by the caller)
 template <int MODE, bool AUX>
-int launch_tile_m(RmeshCtx* c, TileArgs& ta, uint32_t n_tiles, bool persistent) {
-  switch (c->tile_size) {
-    case 8: return launch_tile_t<8, MODE, AUX>(c, ta, n_tiles, persistent);
-    case 12: return launch_tile_t<12, MODE, AUX>(c, ta, n_tiles, persistent);
-    case 16: return launch_tile_t<16, MODE, AUX>(c, ta, n_tiles, persistent);
+int launch_tile_m(RmeshCtx* c, TileArgs& ta, uint32_t n_tiles, bool persistent, TileConf tc) {
+  const int key = tc.ts * 2 + (tc.wide ? 1 : 0);
+  switch (key) {
+    case 16: return launch_tile_t<8, MODE, AUX, false>(c, ta, n_tiles, persistent);
+    case 17: return launch_tile_t<8, MODE, AUX, true>(c, ta, n_tiles, persistent);
+    case 24: return launch_tile_t<12, MODE, AUX, false>(c, ta, n_tiles, persistent);
+    case 25: return launch_tile_t<12, MODE, AUX, true>(c, ta, n_tiles, persistent);
+    case 32: return launch_tile_t<16, MODE, AUX, false>(c, ta, n_tiles, persistent);
+    case 33: return launch_tile_t<16, MODE, AUX, true>(c, ta, n_tiles, persistent);
     default: return fail(c, RMESH_ERR_INVALID_ARG, "tile size must be 8, 12 or 16");
   }
+}
+
+// one persistent launch per tile group of the run
+template <int MODE, bool AUX>
+int launch_groups(RmeshCtx* c, const TileArgs& base, const std::vector<TileGroup>& groups) {
+  for (size_t gi = 0; gi < groups.size(); ++gi) {
+    const TileGroup& g = groups[gi];
+    if (g.n_tiles == 0) continue;
+    TileArgs ta = base;
+    ta.n_tiles = g.n_tiles;
+    ta.tile_lo = g.tile_lo;
+    ta.ticket = c->tickets.as<uint32_t>() + gi;
+    ta.tile_order = c->tile_order.as<uint32_t>() + g.tile_lo;
+    CKR((launch_tile_m<MODE, AUX>(c, ta, g.n_tiles, true, g.conf)));
+  }
+  return RMESH_OK;
 }
 
 TileArgs base_tile_args(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t n_tiles, Counters* cnt) {
@@ -589,6 +707,8 @@ TileArgs base_tile_args(RmeshCtx* c, const ViewParams* views_dev, int n_views, u
   ta.counters = cnt;
   ta.hp = c->hp_d.as<AdamParams>();
   ta.tile_order = c->tile_order.as<uint32_t>();
+  ta.tile_lo = 0;
+  ta.ticket = c->tickets.as<uint32_t>();
   return ta;
 }
 
@@ -705,21 +825,16 @@ int train_views(RmeshCtx* c, const RmeshCamera* cams, int n_views, const float* 
   if (o->loss_type != 0 && o->loss_type != 1) return fail(c, RMESH_ERR_INVALID_ARG, "loss_type must be 0 or 1");
   const int mode = o->mode;
   const bool plain = mode == RMESH_MODE_PLAIN;
-  // view table: batched numbering (tiles and pixels back to back)
-  uint64_t total_pix = 0;
-  uint32_t total_tiles = 0, max_tiles = 0;
-  std::vector<uint32_t> view_tiles(n_views);
-  for (int v = 0; v < n_views; ++v) {
-    CKR(fill_view(c, cams[v], c->views_h[v], plain ? 0u : total_tiles, (uint32_t)total_pix));
-    view_tiles[v] = (uint32_t)(c->views_h[v].tiles_x * c->views_h[v].tiles_y);
-    total_tiles += view_tiles[v];
-    max_tiles = std::max(max_tiles, view_tiles[v]);
-    total_pix += (uint64_t)cams[v].width * cams[v].height;
-  }
+  // view table: batched numbering (tiles back to back, the views of each tile
+  // configuration together; pixels in the caller's order)
+  ViewPlan pl;
+  CKR(make_plan(c, cams, n_views, plain, pl));
+  const uint64_t total_pix = pl.total_pix;
+  const uint32_t total_tiles = pl.total_tiles, max_tiles = pl.max_tiles;
   const int run_views = plain ? 1 : n_views;
   const bool direct_gt = is_device_ptr(gt);
   for (int attempt = 0; attempt < 4; ++attempt) {
-    CKR(ensure_run_buffers(c, run_views, total_pix, plain ? max_tiles : total_tiles));
+    CKR(ensure_run_buffers(c, run_views, total_pix, plain ? max_tiles : total_tiles, pl.cache_units));
     if (!direct_gt) CKR(ensure_buf(c, c->gt, total_pix * 12));
     AdamParams& hp = *c->hp_h;
     hp.step = c->step + 1;
@@ -745,25 +860,28 @@ int train_views(RmeshCtx* c, const RmeshCamera* cams, int n_views, const float* 
       CKR(run_records(c, capturing));
       ViewParams* vd = c->views_d.as<ViewParams>();
       if (plain) {
-        for (int v = 0; v < n_views; ++v) {
-          CKR(run_bin(c, vd + v, 1, view_tiles[v], cnt + v, capturing));
+        for (int i = 0; i < n_views; ++i) {
+          const uint32_t vt = (uint32_t)(c->views_h[i].tiles_x * c->views_h[i].tiles_y);
+          const TileConf tc = pl.conf[pl.order[i]];
+          const std::vector<TileGroup> one{TileGroup{tc, 0u, vt}};
+          CKR(run_bin(c, vd + i, 1, vt, cnt + i, capturing, one));
           CKR(clear_dcolor(c, 1));
           {
             StageScope sc(c, kStComposite, capturing);
-            TileArgs ta = base_tile_args(c, vd + v, 1, view_tiles[v], cnt + v);
+            TileArgs ta = base_tile_args(c, vd + i, 1, vt, cnt + i);
             ta.gt_rgb = gt_dev;
-            CKR((launch_tile_m<kModeTrain, false>(c, ta, view_tiles[v], false)));
+            CKR((launch_tile_m<kModeTrain, false>(c, ta, vt, false, tc)));
           }
-          CKR(run_sh_backward(c, vd + v, 1, capturing));
+          CKR(run_sh_backward(c, vd + i, 1, capturing));
         }
       } else {
-        CKR(run_bin(c, vd, n_views, total_tiles, cnt, capturing));
+        CKR(run_bin(c, vd, n_views, total_tiles, cnt, capturing, pl.groups));
         CKR(clear_dcolor(c, n_views));
         {
           StageScope sc(c, kStComposite, capturing);
           TileArgs ta = base_tile_args(c, vd, n_views, total_tiles, cnt);
           ta.gt_rgb = gt_dev;
-          CKR((launch_tile_m<kModeTrain, false>(c, ta, total_tiles, true)));
+          CKR((launch_groups<kModeTrain, false>(c, ta, pl.groups)));
         }
         CKR(run_sh_backward(c, vd, n_views, capturing));
       }
@@ -772,11 +890,12 @@ int train_views(RmeshCtx* c, const RmeshCamera* cams, int n_views, const float* 
     };
 
     if (mode == RMESH_MODE_GRAPH) {
-      std::vector<int64_t> sig = {n_views, c->tile_size, (int64_t)c->cap_pairs, (int64_t)c->generation,
+      std::vector<int64_t> sig = {n_views, 0, (int64_t)c->cap_pairs, (int64_t)c->generation,
                                   (int64_t)(uintptr_t)gt_dev, o->loss_type, do_adam ? 1 : 0};
       for (int v = 0; v < n_views; ++v) {
         sig.push_back(cams[v].width);
         sig.push_back(cams[v].height);
+        sig.push_back(pl.conf[v].ts * 2 + pl.conf[v].wide);
       }
       // graphs captured before a reallocation point at freed buffers
       for (size_t i = c->graphs.size(); i-- > 0;)
@@ -826,8 +945,9 @@ int train_views(RmeshCtx* c, const RmeshCamera* cams, int n_views, const float* 
     c->have_forward = false;
     c->last_cnt = n_cnt;
     if (loss_out) {
-      for (int v = 0; v < n_views; ++v) {
-        const double l = plain ? c->counters_h[v].loss[0] : c->counters_h[0].loss[v];
+      for (int i = 0; i < n_views; ++i) {
+        const int v = pl.order[i];
+        const double l = plain ? c->counters_h[i].loss[0] : c->counters_h[0].loss[i];
         loss_out[v] = (float)(l / (double)((uint64_t)cams[v].width * cams[v].height));
       }
     }
@@ -1050,7 +1170,39 @@ int rmesh_set_tile_size(RmeshCtx* c, int32_t ts) {
   DevGuard dg__(c);
   if (ts != 8 && ts != 12 && ts != 16) return fail(c, RMESH_ERR_INVALID_ARG, "tile size must be 8, 12 or 16");
   c->tile_size = ts;
+  c->tile_wide = 0;
   c->have_forward = false;
+  return RMESH_OK;
+}
+
+int rmesh_set_tile_config(RmeshCtx* c, int32_t ts, int32_t threads) {
+  if (!c) return RMESH_ERR_INVALID_ARG;
+  TileConf tc;
+  if (!conf_from(ts, threads, &tc)) return fail(c, RMESH_ERR_INVALID_ARG, "unsupported tile size / threads per tile");
+  c->tile_size = tc.ts;
+  c->tile_wide = tc.wide;
+  c->have_forward = false;
+  return RMESH_OK;
+}
+
+int rmesh_set_resolution_tile_config(RmeshCtx* c, int32_t width, int32_t height, int32_t ts, int32_t threads) {
+  if (!c) return RMESH_ERR_INVALID_ARG;
+  auto& rc = c->res_conf;
+  rc.erase(std::remove_if(rc.begin(), rc.end(), [&](const RmeshCtx::ResConf& r) { return r.W == width && r.H == height; }),
+           rc.end());
+  c->have_forward = false;
+  if (ts == 0) return RMESH_OK;  // override removed
+  TileConf tc;
+  if (!conf_from(ts, threads, &tc)) return fail(c, RMESH_ERR_INVALID_ARG, "unsupported tile size / threads per tile");
+  rc.push_back(RmeshCtx::ResConf{width, height, tc.ts, tc.wide});
+  return RMESH_OK;
+}
+
+int rmesh_get_tile_config(RmeshCtx* c, int32_t width, int32_t height, int32_t* ts, int32_t* threads) {
+  if (!c || !ts || !threads) return RMESH_ERR_INVALID_ARG;
+  const TileConf tc = (width > 0 && height > 0) ? view_conf(c, width, height) : TileConf{c->tile_size, c->tile_wide};
+  *ts = tc.ts;
+  *threads = conf_threads(tc);
   return RMESH_OK;
 }
 
@@ -1205,23 +1357,20 @@ int rmesh_forward_views(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views, f
   if (!c || !cams || !rgba_out) return RMESH_ERR_INVALID_ARG;
   DevGuard dg__(c);
   if (n_views <= 0 || n_views > kMaxViews) return fail(c, RMESH_ERR_INVALID_ARG, "n_views out of range");
-  uint64_t total_pix = 0;
-  uint32_t total_tiles = 0;
-  for (int v = 0; v < n_views; ++v) {
-    CKR(fill_view(c, cams[v], c->views_h[v], total_tiles, (uint32_t)total_pix));
-    total_tiles += (uint32_t)(c->views_h[v].tiles_x * c->views_h[v].tiles_y);
-    total_pix += (uint64_t)cams[v].width * cams[v].height;
-  }
+  ViewPlan pl;
+  CKR(make_plan(c, cams, n_views, false, pl));
+  const uint64_t total_pix = pl.total_pix;
+  const uint32_t total_tiles = pl.total_tiles;
   const uint64_t aux_floats = total_pix * (8 + (uint64_t)c->aux_dim);
   for (int attempt = 0; attempt < 4; ++attempt) {
-    CKR(ensure_run_buffers(c, n_views, total_pix, total_tiles));
+    CKR(ensure_run_buffers(c, n_views, total_pix, total_tiles, pl.cache_units));
     if (aux_out) CKR(ensure_buf(c, c->aux, aux_floats * 4));
     CKR(upload_views(c, n_views));
     Counters* cnt = c->counters_d.as<Counters>();
     CK(cudaMemsetAsync(cnt, 0, sizeof(Counters), c->stream));
     CKR(run_records(c, false));
     ViewParams* vd = c->views_d.as<ViewParams>();
-    CKR(run_bin(c, vd, n_views, total_tiles, cnt, false));
+    CKR(run_bin(c, vd, n_views, total_tiles, cnt, false, pl.groups));
     {
       StageScope sc(c, kStComposite, false);
       TileArgs ta = base_tile_args(c, vd, n_views, total_tiles, cnt);
@@ -1230,9 +1379,9 @@ int rmesh_forward_views(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views, f
         ta.aux = c->aux.as<float>();
         ta.aux_data = c->aux_data.as<float>();
         ta.aux_dim = c->aux_dim;
-        CKR((launch_tile_m<kModeForward, true>(c, ta, total_tiles, true)));
+        CKR((launch_groups<kModeForward, true>(c, ta, pl.groups)));
       } else {
-        CKR((launch_tile_m<kModeForward, false>(c, ta, total_tiles, true)));
+        CKR((launch_groups<kModeForward, false>(c, ta, pl.groups)));
       }
     }
     CKR(sync_counters(c, 1));
@@ -1252,17 +1401,19 @@ int rmesh_forward_tiled(RmeshCtx* c, const RmeshCamera* cam, float* rgba_out, fl
   if (!c || !cam || !rgba_out) return RMESH_ERR_INVALID_ARG;
   DevGuard dg__(c);
   const uint64_t npix = (uint64_t)cam->width * cam->height;
+  const TileConf tc = view_conf(c, cam->width, cam->height);
   for (int attempt = 0; attempt < 4; ++attempt) {
-    CKR(fill_view(c, *cam, c->views_h[0], 0, 0));
+    CKR(fill_view(c, *cam, c->views_h[0], 0, 0, tc));
     const uint32_t tiles = (uint32_t)(c->views_h[0].tiles_x * c->views_h[0].tiles_y);
-    CKR(ensure_run_buffers(c, 1, npix, tiles));
+    const std::vector<TileGroup> one{TileGroup{tc, 0u, tiles}};
+    CKR(ensure_run_buffers(c, 1, npix, tiles, conf_minb(tc) * tc.ts));
     if (aux_out) CKR(ensure_buf(c, c->aux, npix * (8 + (uint64_t)c->aux_dim) * 4));
     CKR(upload_views(c, 1));
     Counters* cnt = c->counters_d.as<Counters>();
     CK(cudaMemsetAsync(cnt, 0, sizeof(Counters), c->stream));
     CKR(run_records(c, false));
     ViewParams* vd = c->views_d.as<ViewParams>();
-    CKR(run_bin(c, vd, 1, tiles, cnt, false));
+    CKR(run_bin(c, vd, 1, tiles, cnt, false, one));
     {
       StageScope sc(c, kStComposite, false);
       TileArgs ta = base_tile_args(c, vd, 1, tiles, cnt);
@@ -1271,9 +1422,9 @@ int rmesh_forward_tiled(RmeshCtx* c, const RmeshCamera* cam, float* rgba_out, fl
         ta.aux = c->aux.as<float>();
         ta.aux_data = c->aux_data.as<float>();
         ta.aux_dim = c->aux_dim;
-        CKR((launch_tile_m<kModeForward, true>(c, ta, tiles, true)));
+        CKR((launch_groups<kModeForward, true>(c, ta, one)));
       } else {
-        CKR((launch_tile_m<kModeForward, false>(c, ta, tiles, true)));
+        CKR((launch_groups<kModeForward, false>(c, ta, one)));
       }
     }
     CKR(sync_counters(c, 1));
@@ -1285,6 +1436,8 @@ int rmesh_forward_tiled(RmeshCtx* c, const RmeshCamera* cam, float* rgba_out, fl
     c->have_forward = true;
     c->last_tiles = tiles;
     c->last_views = 1;
+    c->last_ts = tc.ts;
+    c->last_wide = tc.wide;
     return RMESH_OK;
   }
   return fail(c, RMESH_ERR_PAIR_OVERFLOW, "pair buffers could not be grown enough");
@@ -1310,7 +1463,8 @@ static int backward_impl(RmeshCtx* c, const float* dl, const float* dl_aux, floa
     CK(cudaMemsetAsync(c->d_aux.p, 0, (uint64_t)c->M * c->aux_dim * 4, c->stream));
   }
   Counters* cnt = c->counters_d.as<Counters>();
-  CK(cudaMemsetAsync(&cnt->tile_ticket, 0, sizeof(uint32_t), c->stream));
+  CK(cudaMemsetAsync(c->tickets.p, 0, kMaxTileGroups * 4, c->stream));
+  const std::vector<TileGroup> one{TileGroup{TileConf{c->last_ts, c->last_wide}, 0u, c->last_tiles}};
   ViewParams* vd = c->views_d.as<ViewParams>();
   CKR(clear_dcolor(c, 1));
   {
@@ -1323,9 +1477,9 @@ static int backward_impl(RmeshCtx* c, const float* dl, const float* dl_aux, floa
       ta.aux_dim = c->aux_dim;
       ta.dl_aux = c->dl_aux.as<float>();
       ta.d_aux = c->d_aux.as<float>();
-      CKR((launch_tile_m<kModeBackward, true>(c, ta, c->last_tiles, true)));
+      CKR((launch_groups<kModeBackward, true>(c, ta, one)));
     } else {
-      CKR((launch_tile_m<kModeBackward, false>(c, ta, c->last_tiles, true)));
+      CKR((launch_groups<kModeBackward, false>(c, ta, one)));
     }
   }
   if (d_aux && with_aux)
@@ -1377,7 +1531,8 @@ int rmesh_forward_error(RmeshCtx* c, const float* pixel_err, const float* ssim_e
   CK(cudaMemcpyAsync(pe + npix, ssim_err, npix * 4, cudaMemcpyDefault, c->stream));
   CK(cudaMemsetAsync(c->err_out.p, 0, M * 18 * 4, c->stream));
   Counters* cnt = c->counters_d.as<Counters>();
-  CK(cudaMemsetAsync(&cnt->tile_ticket, 0, sizeof(uint32_t), c->stream));
+  CK(cudaMemsetAsync(c->tickets.p, 0, kMaxTileGroups * 4, c->stream));
+  const std::vector<TileGroup> one{TileGroup{TileConf{c->last_ts, c->last_wide}, 0u, c->last_tiles}};
   ViewParams* vd = c->views_d.as<ViewParams>();
   {
     StageScope sc(c, kStComposite, false);
@@ -1386,7 +1541,7 @@ int rmesh_forward_error(RmeshCtx* c, const float* pixel_err, const float* ssim_e
     ta.ssim_err = pe + npix;
     ta.tet_err = c->err_out.as<float>();
     ta.tet_count = reinterpret_cast<int*>(c->err_out.as<float>() + M * 16);
-    CKR((launch_tile_m<kModeError, false>(c, ta, c->last_tiles, true)));
+    CKR((launch_groups<kModeError, false>(c, ta, one)));
   }
   CK(cudaMemcpyAsync(tet_err, c->err_out.p, M * 16 * 4, cudaMemcpyDefault, c->stream));
   CK(cudaMemcpyAsync(tet_count, c->err_out.as<float>() + M * 16, M * 8, cudaMemcpyDefault, c->stream));
@@ -1426,47 +1581,127 @@ int rmesh_accumulate_views(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views
   return train_views(c, cams, n_views, gt, opts, loss_out, false);
 }
 
-int rmesh_autotune_tile_size(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views, const float* gt,
-                             const RmeshTrainOpts* opts, int32_t* tile_size_out, float* ms_out) {
-  if (!c || !opts || !tile_size_out) return RMESH_ERR_INVALID_ARG;
-  DevGuard dg__(c);
+}  // extern "C"
+
+namespace {
+
+// ms per batched forward + loss + adjoint run (no Adam: parameters unchanged)
+// of these views at the context's current tile configurations: one warm-up
+// run (sizes the buffers), then two timed runs
+int time_views(RmeshCtx* c, const RmeshCamera* cams, int n, const float* gt, const RmeshTrainOpts& o,
+               cudaEvent_t e0, cudaEvent_t e1, float* ms) {
+  c->have_forward = false;
+  CKR(train_views(c, cams, n, gt, &o, nullptr, false));
+  CK(cudaEventRecord(e0, c->stream));
+  for (int r = 0; r < 2; ++r) CKR(train_views(c, cams, n, gt, &o, nullptr, false));
+  CK(cudaEventRecord(e1, c->stream));
+  CK(cudaEventSynchronize(e1));
+  CK(cudaEventElapsedTime(ms, e0, e1));
+  *ms *= 0.5f;
+  return RMESH_OK;
+}
+
+int autotune_impl(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views, const float* gt, const RmeshTrainOpts* opts,
+                  bool wide_too, bool per_resolution, std::vector<RmeshTuneEntry>& out) {
   RmeshTrainOpts o = *opts;
   o.mode = RMESH_MODE_BATCHED;
-  const int sizes[3] = {8, 12, 16};
-  float best_ms = 0.f;
-  int best = c->tile_size;
+  std::vector<TileConf> grid;
+  for (int ts : {8, 12, 16})
+    for (int w = 0; w < (wide_too ? 2 : 1); ++w) grid.push_back(TileConf{ts, w});
   cudaEvent_t e0, e1;
   CK(cudaEventCreate(&e0));
   CK(cudaEventCreate(&e1));
-  int rc = RMESH_OK;
-  for (int i = 0; i < 3 && rc == RMESH_OK; ++i) {
-    c->tile_size = sizes[i];
-    c->have_forward = false;
-    // a warm-up run sizes the buffers; then two timed runs (no Adam: the
-    // parameters are left as they were, the gradient slots hold the last run)
-    rc = train_views(c, cams, n_views, gt, &o, nullptr, false);
-    if (rc != RMESH_OK) break;
-    float ms = 0.f;
-    if (cudaEventRecord(e0, c->stream) != cudaSuccess) { rc = RMESH_ERR_CUDA; break; }
-    for (int r = 0; r < 2 && rc == RMESH_OK; ++r) rc = train_views(c, cams, n_views, gt, &o, nullptr, false);
-    if (rc != RMESH_OK) break;
-    if (cudaEventRecord(e1, c->stream) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess ||
-        cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) {
-      rc = RMESH_ERR_CUDA;
-      break;
+  struct EvGuard {
+    cudaEvent_t a, b;
+    ~EvGuard() {
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
     }
-    ms *= 0.5f;
-    if (ms_out) ms_out[i] = ms;
+  } evg{e0, e1};
+  c->res_conf.clear();
+  // every configuration on all views
+  TileConf best{c->tile_size, c->tile_wide};
+  float best_ms = 0.f;
+  for (size_t i = 0; i < grid.size(); ++i) {
+    c->tile_size = grid[i].ts;
+    c->tile_wide = grid[i].wide;
+    float ms = 0.f;
+    CKR(time_views(c, cams, n_views, gt, o, e0, e1, &ms));
+    out.push_back(RmeshTuneEntry{0, 0, grid[i].ts, conf_threads(grid[i]), ms});
     if (i == 0 || ms < best_ms) {
       best_ms = ms;
-      best = sizes[i];
+      best = grid[i];
     }
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  c->tile_size = best;
+  c->tile_size = best.ts;
+  c->tile_wide = best.wide;
+  // every configuration on the views of each resolution; a resolution whose
+  // best configuration differs from the overall best gets an override, kept
+  // only if the mixed step beats the best single configuration
+  std::vector<std::pair<int, int>> res;
+  for (int v = 0; v < n_views; ++v) {
+    const std::pair<int, int> r{cams[v].width, cams[v].height};
+    if (std::find(res.begin(), res.end(), r) == res.end()) res.push_back(r);
+  }
+  if (!per_resolution || res.size() < 2) return RMESH_OK;
+  std::vector<RmeshCtx::ResConf> chosen;
+  for (const auto& r : res) {
+    std::vector<RmeshCamera> sub;
+    for (int v = 0; v < n_views; ++v)
+      if (cams[v].width == r.first && cams[v].height == r.second) sub.push_back(cams[v]);
+    TileConf rb = best;
+    float rb_ms = 0.f;
+    for (size_t i = 0; i < grid.size(); ++i) {
+      c->tile_size = grid[i].ts;
+      c->tile_wide = grid[i].wide;
+      float ms = 0.f;
+      CKR(time_views(c, sub.data(), (int)sub.size(), gt, o, e0, e1, &ms));
+      out.push_back(RmeshTuneEntry{r.first, r.second, grid[i].ts, conf_threads(grid[i]), ms});
+      if (i == 0 || ms < rb_ms) {
+        rb_ms = ms;
+        rb = grid[i];
+      }
+    }
+    if (!(rb == best)) chosen.push_back(RmeshCtx::ResConf{r.first, r.second, rb.ts, rb.wide});
+  }
+  c->tile_size = best.ts;
+  c->tile_wide = best.wide;
+  if (chosen.empty()) return RMESH_OK;
+  c->res_conf = chosen;
+  float mixed_ms = 0.f;
+  CKR(time_views(c, cams, n_views, gt, o, e0, e1, &mixed_ms));
+  out.push_back(RmeshTuneEntry{-1, -1, 0, 0, mixed_ms});
+  if (mixed_ms >= best_ms) c->res_conf.clear();
+  return RMESH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rmesh_autotune(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views, const float* gt,
+                   const RmeshTrainOpts* opts, int32_t per_resolution, RmeshTuneEntry* entries, int32_t max_entries,
+                   int32_t* n_entries) {
+  if (!c || !cams || !gt || !opts || !n_entries || (max_entries > 0 && !entries)) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
+  std::vector<RmeshTuneEntry> out;
+  const int rc = autotune_impl(c, cams, n_views, gt, opts, true, per_resolution != 0, out);
   c->have_forward = false;
-  *tile_size_out = best;
+  *n_entries = (int32_t)out.size();
+  for (int i = 0; i < (int)out.size() && i < max_entries; ++i) entries[i] = out[i];
+  return rc;
+}
+
+int rmesh_autotune_tile_size(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views, const float* gt,
+                             const RmeshTrainOpts* opts, int32_t* tile_size_out, float* ms_out) {
+  if (!c || !cams || !gt || !opts || !tile_size_out) return RMESH_ERR_INVALID_ARG;
+  DevGuard dg__(c);
+  std::vector<RmeshTuneEntry> out;
+  const int rc = autotune_impl(c, cams, n_views, gt, opts, false, false, out);
+  c->have_forward = false;
+  for (size_t i = 0; i < out.size() && i < 3; ++i)
+    if (ms_out) ms_out[i] = out[i].ms;
+  *tile_size_out = c->tile_size;
   return rc;
 }
 

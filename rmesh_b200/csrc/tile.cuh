@@ -93,52 +93,62 @@ struct TileArgs {
   uint32_t span_cache_tets;
   // persistent launches: ticket -> tile (longest lists first); nullptr = identity
   const uint32_t* tile_order;
+  // the launch covers global tiles [tile_lo, tile_lo + n_tiles) (the views of
+  // one tile configuration); tile_order holds indices relative to tile_lo
+  uint32_t tile_lo;
+  uint32_t* ticket;  // persistent tile-queue head of this launch (zeroed before it)
 };
 
-template <int TS, bool AUX>
+// Launch shape of a tile size.  WIDE doubles the threads per tile: the pixel
+// phases use the first TS*TS threads, the item-parallel phases all of them,
+// with larger sub-batches and half the resident CTAs.
+template <int TS, bool AUX, bool WIDE = false>
 struct TileCfg {
-  static constexpr int NT = ((TS * TS + 31) / 32) * 32;
+  static constexpr int NT = (WIDE ? 2 : 1) * (((TS * TS + 31) / 32) * 32);
   static constexpr int NW = NT / 32;
   // items per sub-batch; 800 for 12x12 tiles fills a quarter of the SM's
   // 228 KB of shared memory (four resident CTAs, the register limit at 96
   // registers per thread): fewer sub-batches, fewer block barriers
-  static constexpr int CAP = TS == 12 ? 800 : 512;
+  static constexpr int CAP = WIDE ? (TS == 8 ? 512 : (TS == 12 ? 2048 : 1024)) : (TS == 12 ? 800 : 512);
   // resident CTAs per SM the register budget is sized for
-  static constexpr int MINB = TS == 16 ? 2 : (TS == 12 ? 4 : 8);
+  static constexpr int MINB = (WIDE ? 1 : 2) * (TS == 16 ? 1 : (TS == 12 ? 2 : 4));
 };
 
-template <int TS, bool AUX>
+template <int TS, bool AUX, bool WIDE = false>
 struct __align__(16) TileSmem {
+  using Cfg = TileCfg<TS, AUX, WIDE>;
   TetView view[2][kBatch];  // staged per-view tet records (double buffered)
   short2 span_pf[kBatch][TS];  // adjoint: the next batch's cached spans (bulk copy)
   float mom[kBatch][kMom];  // adjoint moments per tet (phase 2)
   float4 pdir[TS * TS];     // pixel ray direction
   float4 pdl[TS * TS];      // pixel dL/dRGB (adjoint)
-  float4 item[TileCfg<TS, AUX>::CAP];   // (cp.rgb, od) -> adjoint: (t_prev, d_od_state, has, aux_s)
-  float4 itemx[TileCfg<TS, AUX>::CAP];  // (t_min, t_max, packed faces | tet | pixel, alpha_t)
-  float red[TileCfg<TS, AUX>::NW][32][kMomHalf + 1];  // per-warp transpose (odd row stride)
+  float4 item[Cfg::CAP];    // (cp.rgb, od) -> adjoint: (t_prev, d_od_state, has, aux_s)
+  float4 itemx[Cfg::CAP];   // (t_min, t_max, packed faces | tet | pixel, alpha_t)
+  float red[Cfg::NW][32][kMomHalf + 1];  // per-warp transpose (odd row stride)
   uint32_t toff[kBatch + 1];   // tet-major item offsets
   uint32_t pmask[TS * TS];
   short2 span[kBatch][TS];
   // per (tet, row): item index of the row's column 0 -- relative to the tet's
   // first item after the prefixes, to the sub-batch's first item after fill
   int16_t rowoff[kBatch][TS];
-  uint16_t ipix[TileCfg<TS, AUX>::CAP];  // (tet slot << 8) | pixel of each item of the sub-batch (tet-major)
+  uint16_t ipix[Cfg::CAP];  // (tet slot << 8) | pixel of each item of the sub-batch (tet-major)
   uint64_t bar[2];
   float lsum[16];
   uint32_t tile;
 };
 
 // Pixel of thread tid: 8x4 pixel blocks per warp for 16x16 tiles, row-major
-// otherwise.  Threads past TS*TS (12x12 tiles use 160 threads) get a real
-// pixel's coordinates but are marked out of tile.
+// otherwise.  Threads past TS*TS (12x12 tiles use 160 threads, and the wide
+// configurations twice the pixel count) get a real pixel's coordinates but are
+// marked out of tile.
 template <int TS>
 __device__ __forceinline__ void pixel_of_thread(int tid, int& row, int& col, bool& in_tile) {
   if (TS == 16) {
-    const int w = tid >> 5, l = tid & 31;
+    const int t = tid & 255;
+    const int w = t >> 5, l = t & 31;
     col = (w & 1) * 8 + (l & 7);
     row = (w >> 1) * 4 + (l >> 3);
-    in_tile = true;
+    in_tile = tid < 256;
   } else {
     in_tile = tid < TS * TS;
     const int t = in_tile ? tid : TS * TS - 1;
@@ -213,14 +223,14 @@ __device__ __forceinline__ uint32_t pack_item(int fmin, int fmax, int k, int p) 
   return (uint32_t)fmin | ((uint32_t)fmax << 3) | ((uint32_t)k << 5) | ((uint32_t)p << 10);
 }
 
-template <int TS, int MODE, bool AUX>
-__global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) tile_kernel(TileArgs a) {
-  using Cfg = TileCfg<TS, AUX>;
+template <int TS, int MODE, bool AUX, bool WIDE>
+__global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, WIDE>::MINB) tile_kernel(TileArgs a) {
+  using Cfg = TileCfg<TS, AUX, WIDE>;
   constexpr int NT = Cfg::NT;
   constexpr int NW = Cfg::NW;
   constexpr int CAP = Cfg::CAP;
   extern __shared__ __align__(16) unsigned char tile_smem_raw[];
-  TileSmem<TS, AUX>& s = *reinterpret_cast<TileSmem<TS, AUX>*>(tile_smem_raw);
+  TileSmem<TS, AUX, WIDE>& s = *reinterpret_cast<TileSmem<TS, AUX, WIDE>*>(tile_smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   int prow, pcol;
   bool in_tile;
@@ -246,15 +256,15 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX>::NT, TileCfg<TS, AUX>::MINB) 
     if (tid == 0) {
       uint32_t t = first_tile;
       if (a.persistent) {
-        t = atomicAdd(&a.counters->tile_ticket, 1u);
+        t = atomicAdd(a.ticket, 1u);
         if (a.tile_order && t < a.n_tiles) t = a.tile_order[t];
         else if (t >= a.n_tiles) t = 0xFFFFFFFFu;
       }
       s.tile = t;
     }
     __syncthreads();
-    const uint32_t g = s.tile;
-    if (g >= a.n_tiles || failed) break;
+    if (s.tile >= a.n_tiles || failed) break;
+    const uint32_t g = s.tile + a.tile_lo;  // global tile id
     const int view = view_of_tile(a.views, a.n_views, g);
     const ViewParams& V = a.views[view];
     const uint32_t local_tile = g - V.tile_base;

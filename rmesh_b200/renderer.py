@@ -223,6 +223,24 @@ class RMeshRenderer:
         self._check(self._lib.rmesh_set_tile_size(self._ctx, int(tile_size)))
         self._tile_size = int(tile_size)
 
+    def set_tile_config(self, tile_size: int, threads: int = 0):
+        """Default tile configuration: tile size 8, 12 or 16 and threads per
+        tile (0: one per pixel rounded up to warps; or twice that)."""
+        self._check(self._lib.rmesh_set_tile_config(self._ctx, int(tile_size), int(threads)))
+        self._tile_size = int(tile_size)
+
+    def set_resolution_tile_config(self, width: int, height: int, tile_size: int, threads: int = 0):
+        """Views of width x height use this configuration (tile_size 0 removes it)."""
+        self._check(self._lib.rmesh_set_resolution_tile_config(self._ctx, int(width), int(height), int(tile_size),
+                                                                int(threads)))
+
+    def tile_config(self, width: int = 0, height: int = 0):
+        """(tile_size, threads per tile) a view of width x height runs with (0, 0: the default)."""
+        ts, th = ctypes.c_int32(0), ctypes.c_int32(0)
+        self._check(self._lib.rmesh_get_tile_config(self._ctx, int(width), int(height), ctypes.byref(ts),
+                                                     ctypes.byref(th)))
+        return int(ts.value), int(th.value)
+
     def set_stream(self, stream_handle: int):
         self._check(self._lib.rmesh_set_stream(self._ctx, ctypes.c_void_p(int(stream_handle))))
         self._stream_handle = int(stream_handle)
@@ -507,10 +525,10 @@ class RMeshRenderer:
         self._check(self._lib.rmesh_accumulate_views(self._ctx, cams, n, p, ctypes.byref(o), losses.ctypes.data))
         return losses
 
-    def autotune(self, cameras: Sequence, gt_images, loss_type: int = 1) -> dict:
+    def autotune_tile_size(self, cameras: Sequence, gt_images, loss_type: int = 1) -> dict:
         """Times the batched forward + loss + adjoint of ``cameras`` at tile
-        sizes 8, 12 and 16 (parameters unchanged), keeps the fastest and
-        returns {tile_size: ms per run}."""
+        sizes 8, 12 and 16 with one thread per pixel (parameters unchanged),
+        keeps the fastest and returns {tile_size: ms per run}."""
         n, cams, keep, p, o = self._views_args(cameras, gt_images, 0.0, 0.0, 0.0, loss_type, 0.0, "batched")
         best = ctypes.c_int32(0)
         ms = np.zeros(3, np.float32)
@@ -518,6 +536,34 @@ class RMeshRenderer:
                                                        ms.ctypes.data))
         self._tile_size = int(best.value)
         return {8: float(ms[0]), 12: float(ms[1]), 16: float(ms[2])}
+
+    def autotune(self, cameras: Sequence, gt_images, loss_type: int = 1, per_resolution: bool = True) -> dict:
+        """Searches tile size x threads per tile (parameters unchanged): every
+        configuration on all views, then (``per_resolution``) on the views of
+        each resolution, keeping per-resolution configurations only if the mixed
+        step is faster.  Returns {"grid": [{"views", "tile_size", "threads",
+        "ms"}, ...], "chosen": {"default": (tile_size, threads),
+        "per_resolution": {"WxH": (tile_size, threads)}}}."""
+        n, cams, keep, p, o = self._views_args(cameras, gt_images, 0.0, 0.0, 0.0, loss_type, 0.0, "batched")
+        cap = 6 + 6 * 16 + 1
+        entries = (_lib.TuneEntry * cap)()
+        got = ctypes.c_int32(0)
+        self._check(self._lib.rmesh_autotune(self._ctx, cams, n, p, ctypes.byref(o), 1 if per_resolution else 0,
+                                             entries, cap, ctypes.byref(got)))
+        grid = []
+        for e in entries[:min(int(got.value), cap)]:
+            views = "all" if e.width == 0 else ("all, per-resolution configurations" if e.width < 0
+                                                else f"{e.width}x{e.height}")
+            grid.append({"views": views, "tile_size": int(e.tile_size), "threads": int(e.threads),
+                         "ms": round(float(e.ms), 3)})
+        self._tile_size, threads = self.tile_config()
+        per = {}
+        for c in cameras:
+            key = f"{int(c.width)}x{int(c.height)}"
+            cfg = self.tile_config(int(c.width), int(c.height))
+            if cfg != (self._tile_size, threads):
+                per[key] = cfg
+        return {"grid": grid, "chosen": {"default": (self._tile_size, threads), "per_resolution": per}}
 
     def grad_slots(self):
         """The device gradient buffer as a flat torch CUDA tensor view: [M, 20]

@@ -178,7 +178,7 @@ def test_autotune_keeps_parameters(c1_scene):
     gts = [np.random.default_rng(i).uniform(0, 1, (128, 128, 3)).astype(np.float32) for i in range(3)]
     r = make_renderer(c1_scene, cams[0])
     before = r.get_params()
-    ms = r.autotune(cams, gts)
+    ms = r.autotune_tile_size(cams, gts)
     assert set(ms) == {8, 12, 16} and all(v > 0 for v in ms.values())
     ts = r.info().tile_size
     assert ms[ts] == min(ms.values())
