@@ -958,6 +958,13 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
           const uint32_t next_lo = lo + (uint32_t)nb;
           wait_buf(buf);
           if (failed) break;
+          // the flush reads this batch's tet records (vertex positions): start
+          // bringing them into L1 now, one thread per tet
+          if (tid < nb) {
+            const TetRec* rp = a.rec + s.view[buf][tid].meta.x;
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(rp));
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(reinterpret_cast<const char*>(rp) + 32));
+          }
           // adjoint: edge crossings only, from the forward's cache when it
           // covered the whole batch
           if (span_cached(lo, nb))
