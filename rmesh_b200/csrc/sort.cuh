@@ -4,7 +4,8 @@
 // (crates/rmesh-sort/src/drs.rs:180-279, wgsl/drs_{upsweep,scan,downsweep}.wgsl):
 // one histogram kernel computes the digit counts of every pass in a single
 // read of the keys, then each pass is ONE kernel that ranks a 4096-key
-// partition in shared memory (warp multi-split with match.any), looks back
+// partition in shared memory (warp multi-split: peers of a digit found by one
+// ballot per digit bit), looks back
 // across earlier partitions for the per-digit global offset, and scatters
 // through shared memory so the writes are digit-contiguous.
 //
@@ -142,15 +143,22 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(const K* __restr
 #pragma unroll
   for (int i = 0; i < SortCfg<K>::KPT; ++i) {
     const uint32_t d = digit_of(k[i], shift);
-    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    // lanes holding the same digit: one ballot per digit bit
+    unsigned peers = 0xffffffffu;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const bool bit = (d >> b) & 1u;
+      const unsigned bb = __ballot_sync(0xffffffffu, bit);
+      peers &= bit ? bb : ~bb;
+    }
     const int leader = __ffs(peers) - 1;
+    // the leader advances the warp's digit counter; the shuffle that hands the
+    // old count to its peers also orders this key's update before the next
+    // key's (whose leader may be another lane)
     uint32_t old = 0u;
-    if (lane == leader) old = s_whist[warp * 256 + d];
+    if (lane == leader) old = atomicAdd(&s_whist[warp * 256 + d], (uint32_t)__popc(peers));
     old = __shfl_sync(0xffffffffu, old, leader);
     rank[i] = old + __popc(peers & lt_mask);
-    __syncwarp();
-    if (lane == leader) s_whist[warp * 256 + d] = old + __popc(peers);
-    __syncwarp();
   }
   __syncthreads();
 
