@@ -349,7 +349,7 @@ struct ViewPlan {
   std::vector<TileGroup> groups;
   uint64_t total_pix = 0;
   uint32_t total_tiles = 0, max_tiles = 0;
-  int cache_units = 0;           // max over groups of resident CTAs per SM x tile size
+  int cache_units = 0;           // max over groups of resident CTAs per SM (span-cache slots per SM)
 };
 
 // ---------------------------------------------------------------- sorting
@@ -418,8 +418,8 @@ int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t
   CKR(ensure_buf(c, c->vis_cnt, items * 4));
   CKR(ensure_buf(c, c->vis_proj, items * 32));
   CKR(ensure_buf(c, c->vis_view, items * sizeof(TetView)));
-  // resident CTAs x tile size of the largest configuration of the run
-  CKR(ensure_buf(c, c->span_cache, (uint64_t)cache_units * c->num_sms * kSpanCacheTets * sizeof(short2)));
+  // span-cache slots: resident CTAs per SM of the run's largest configuration
+  CKR(ensure_buf(c, c->span_cache, (uint64_t)cache_units * c->num_sms * kSpanCacheTets * kSpanRows));
   if (c->sh_degree >= 0) {
     CKR(ensure_buf(c, c->vis_color, items * 16));
     CKR(ensure_buf(c, c->vis_dcolor, items * 16));
@@ -510,7 +510,7 @@ int make_plan(RmeshCtx* c, const RmeshCamera* cams, int n_views, bool plain, Vie
     }
     g.n_tiles = pl.total_tiles - g.tile_lo;
     pl.groups.push_back(g);
-    pl.cache_units = std::max(pl.cache_units, conf_minb(tc) * tc.ts);
+    pl.cache_units = std::max(pl.cache_units, conf_minb(tc));
   }
   return RMESH_OK;
 }
@@ -616,9 +616,8 @@ int run_bin(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t tota
           (int)std::max<uint64_t>(1, std::min<uint64_t>((g.n_tiles + 255) / 256, (uint64_t)c->num_sms * 2));
       tile_order_hist_kernel<<<oblocks, 256, 0, c->stream>>>(c->ranges.as<uint2>() + g.tile_lo, g.n_tiles, hist);
       CKL();
-      tile_order_scatter_kernel<<<oblocks, 256, 0, c->stream>>>(c->ranges.as<uint2>() + g.tile_lo, g.n_tiles, hist,
-                                                                hist + kOrderBuckets,
-                                                                c->tile_order.as<uint32_t>() + g.tile_lo);
+      tile_order_stable_kernel<<<1, kOrderThreads, 0, c->stream>>>(c->ranges.as<uint2>() + g.tile_lo, g.n_tiles,
+                                                                  hist, c->tile_order.as<uint32_t>() + g.tile_lo);
       CKL();
     }
   }
@@ -646,8 +645,8 @@ int launch_tile_t(RmeshCtx* c, TileArgs& ta, uint32_t n_tiles, bool persistent) 
   }
   ta.persistent = persistent ? 1 : 0;
   if (MODE == kModeTrain && persistent && c->span_cache.p &&
-      (uint64_t)grid * kSpanCacheTets * TS * sizeof(short2) <= c->span_cache.bytes) {
-    ta.span_cache = c->span_cache.as<short2>();
+      (uint64_t)grid * kSpanCacheTets * kSpanRows <= c->span_cache.bytes) {
+    ta.span_cache = c->span_cache.as<uint8_t>();
     ta.span_cache_tets = kSpanCacheTets;
   }
   if (grid == 0) return RMESH_OK;
@@ -1406,7 +1405,7 @@ int rmesh_forward_tiled(RmeshCtx* c, const RmeshCamera* cam, float* rgba_out, fl
     CKR(fill_view(c, *cam, c->views_h[0], 0, 0, tc));
     const uint32_t tiles = (uint32_t)(c->views_h[0].tiles_x * c->views_h[0].tiles_y);
     const std::vector<TileGroup> one{TileGroup{tc, 0u, tiles}};
-    CKR(ensure_run_buffers(c, 1, npix, tiles, conf_minb(tc) * tc.ts));
+    CKR(ensure_run_buffers(c, 1, npix, tiles, conf_minb(tc)));
     if (aux_out) CKR(ensure_buf(c, c->aux, npix * (8 + (uint64_t)c->aux_dim) * 4));
     CKR(upload_views(c, 1));
     Counters* cnt = c->counters_d.as<Counters>();

@@ -141,22 +141,56 @@ __global__ void __launch_bounds__(256) tile_order_hist_kernel(const uint2* __res
     if (sh[i]) atomicAdd(&hist[i], sh[i]);
 }
 
-// order[pos] = tile, bucket by bucket from the longest lists down
-__global__ void __launch_bounds__(256) tile_order_scatter_kernel(const uint2* __restrict__ ranges, uint32_t n_tiles,
-                                                                 const uint32_t* hist, uint32_t* cursor,
-                                                                 uint32_t* order) {
-  __shared__ uint32_t start[kOrderBuckets];
-  if (threadIdx.x == 0) {
+// order[pos] = tile, bucket by bucket from the longest lists down, and inside
+// a bucket in tile order (a stable counting sort by bucket): tiles of one view
+// are numbered together, so a bucket's tiles of a view run close in time and
+// share their tet records and span-cache lines in L2.  One block walks the
+// tiles in chunks of kOrderThreads: each tile's rank among the chunk's tiles
+// of its bucket comes from per-warp peer masks (one ballot per bucket bit)
+// and a per-bucket scan over the warps.
+constexpr int kOrderThreads = 1024;
+__global__ void __launch_bounds__(kOrderThreads) tile_order_stable_kernel(const uint2* __restrict__ ranges,
+                                                                          uint32_t n_tiles, const uint32_t* hist,
+                                                                          uint32_t* order) {
+  constexpr int kW = kOrderThreads / 32;
+  __shared__ uint32_t cursor[kOrderBuckets];
+  __shared__ uint32_t wcnt[kW][kOrderBuckets];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  if (tid == 0) {
     uint32_t acc = 0u;
     for (int b = kOrderBuckets - 1; b >= 0; --b) {
-      start[b] = acc;
+      cursor[b] = acc;
       acc += hist[b];
     }
   }
-  __syncthreads();
-  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < n_tiles; t += gridDim.x * blockDim.x) {
-    const int b = order_bucket(ranges[t]);
-    order[start[b] + atomicAdd(&cursor[b], 1u)] = t;
+  for (uint32_t base = 0; base < n_tiles; base += kOrderThreads) {
+    for (int i = tid; i < kW * kOrderBuckets; i += kOrderThreads) (&wcnt[0][0])[i] = 0u;
+    __syncthreads();
+    const uint32_t t = base + (uint32_t)tid;
+    const bool live = t < n_tiles;
+    const int b = live ? order_bucket(ranges[t]) : 63;  // 63: no bucket
+    unsigned peers = 0xffffffffu;
+#pragma unroll
+    for (int bit = 0; bit < 6; ++bit) {
+      const bool v = (b >> bit) & 1;
+      const unsigned bb = __ballot_sync(0xffffffffu, v);
+      peers &= v ? bb : ~bb;
+    }
+    const uint32_t rank = (uint32_t)__popc(peers & ((1u << lane) - 1u));
+    if (live && lane == __ffs(peers) - 1) wcnt[warp][b] = (uint32_t)__popc(peers);
+    __syncthreads();
+    if (tid < kOrderBuckets) {  // exclusive scan of bucket tid over the warps
+      uint32_t off = cursor[tid];
+      for (int w = 0; w < kW; ++w) {
+        const uint32_t c = wcnt[w][tid];
+        wcnt[w][tid] = off;
+        off += c;
+      }
+      cursor[tid] = off;
+    }
+    __syncthreads();
+    if (live) order[wcnt[warp][b] + rank] = t;
+    __syncthreads();
   }
 }
 

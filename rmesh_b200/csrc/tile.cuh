@@ -48,6 +48,17 @@
 namespace rm {
 
 constexpr int kBatch = 32;
+// Adjoint span cache rows per tet (tile rows, padded to 16: a tet's cached rows
+// are one 16-byte line).  A row's span [lo, hi] (columns < 16) is one byte,
+// lo << 4 | hi; an empty row is 0xF0 (lo > hi).
+constexpr int kSpanRows = 16;
+__device__ __forceinline__ uint8_t pack_span(short2 sp) {
+  return sp.x > sp.y ? (uint8_t)0xF0u : (uint8_t)((sp.x << 4) | sp.y);
+}
+__device__ __forceinline__ short2 unpack_span(uint8_t v) {
+  const int lo = v >> 4, hi = v & 15;
+  return lo > hi ? make_short2(0, -1) : make_short2((short)lo, (short)hi);
+}
 constexpr int kMom = 24;      // adjoint moments per tet (see phase 2)
 constexpr int kMomHalf = 12;  // moments transposed per reduction pass
 
@@ -87,9 +98,9 @@ struct TileArgs {
   const AdamParams* hp;
   int persistent;
   // train mode, persistent launches: per-CTA cache of the adjoint's pixel
-  // spans (span_cache_tets entries of TS rows per CTA), written by the forward
-  // pass of the same tile; nullptr disables it
-  short2* span_cache;
+  // spans (span_cache_tets entries of kSpanRows one-byte rows per CTA, see
+  // pack_span), written by the forward pass of the same tile; nullptr disables it
+  uint8_t* span_cache;
   uint32_t span_cache_tets;
   // persistent launches: ticket -> tile (longest lists first); nullptr = identity
   const uint32_t* tile_order;
@@ -106,10 +117,10 @@ template <int TS, bool AUX, bool WIDE = false>
 struct TileCfg {
   static constexpr int NT = (WIDE ? 2 : 1) * (((TS * TS + 31) / 32) * 32);
   static constexpr int NW = NT / 32;
-  // items per sub-batch; 800 for 12x12 tiles fills a quarter of the SM's
+  // items per sub-batch; 832 for 12x12 tiles fills a quarter of the SM's
   // 228 KB of shared memory (four resident CTAs, the register limit at 96
   // registers per thread): fewer sub-batches, fewer block barriers
-  static constexpr int CAP = WIDE ? (TS == 8 ? 512 : (TS == 12 ? 2048 : 1024)) : (TS == 12 ? 800 : 512);
+  static constexpr int CAP = WIDE ? (TS == 8 ? 512 : (TS == 12 ? 2048 : 1024)) : (TS == 12 ? 832 : 512);
   // resident CTAs per SM the register budget is sized for
   static constexpr int MINB = (WIDE ? 1 : 2) * (TS == 16 ? 1 : (TS == 12 ? 2 : 4));
 };
@@ -118,7 +129,7 @@ template <int TS, bool AUX, bool WIDE = false>
 struct __align__(16) TileSmem {
   using Cfg = TileCfg<TS, AUX, WIDE>;
   TetView view[2][kBatch];  // staged per-view tet records (double buffered)
-  short2 span_pf[kBatch][TS];  // adjoint: the next batch's cached spans (bulk copy)
+  uint8_t span_pf[kBatch][kSpanRows];  // adjoint: the next batch's cached spans (bulk copy, packed)
   float mom[kBatch][kMom];  // adjoint moments per tet (phase 2)
   float4 pdir[TS * TS];     // pixel ray direction
   float4 pdl[TS * TS];      // pixel dL/dRGB (adjoint)
@@ -248,9 +259,9 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
   bool failed = false;
 
   // this CTA's span cache slot (persistent train launches only)
-  short2* const scache = (MODE == kModeTrain && a.span_cache)
-                             ? a.span_cache + (size_t)blockIdx.x * a.span_cache_tets * TS
-                             : nullptr;
+  uint8_t* const scache = (MODE == kModeTrain && a.span_cache)
+                              ? a.span_cache + (size_t)blockIdx.x * a.span_cache_tets * kSpanRows
+                              : nullptr;
   const uint32_t first_tile = blockIdx.x;
   while (true) {
     if (tid == 0) {
@@ -313,11 +324,11 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
     };
     // span_src (adjoint): the batch's cached spans, copied into span_pf on the
     // same barrier
-    auto issue = [&](int buf, int nb, uint32_t idx, const short2* span_src) {
+    auto issue = [&](int buf, int nb, uint32_t idx, const uint8_t* span_src) {
       if (warp == 0) {
         if (lane == 0) {
           fence_proxy_async_smem();
-          const uint32_t span_bytes = span_src ? (uint32_t)(nb * TS * (int)sizeof(short2)) : 0u;
+          const uint32_t span_bytes = span_src ? (uint32_t)(nb * kSpanRows) : 0u;
           mbar_arrive_expect_tx(&s.bar[buf], (uint32_t)nb * (uint32_t)sizeof(TetView) + span_bytes);
           if (span_src) bulk_copy_g2s(&s.span_pf[0][0], span_src, span_bytes, &s.bar[buf]);
         }
@@ -405,7 +416,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
     auto task_row = [&](int t, int k) -> int { return __shfl_sync(0xffffffffu, rr_lo - (rr_pre - rr_n), k) + t; };
     // cache: the forward (vertex_rows) also stores each task's adjoint span
     // (edge crossings only) at its list position first + dir * k
-    auto spans = [&](int buf, int nb, bool vertex_rows, short2* cache, uint32_t first, int dir) {
+    auto spans = [&](int buf, int nb, bool vertex_rows, uint8_t* cache, uint32_t first, int dir) {
       row_ranges(buf, nb);
       for (int i = tid; i < TS * TS; i += NT) s.pmask[i] = 0u;
       for (int t0 = warp * 32; t0 < rr_total; t0 += NT) {  // warp-uniform trip count
@@ -414,12 +425,12 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
         const int row = task_row(t, k);
         if (t >= rr_total) continue;
         short2 sp = make_short2(0, -1);
-        short2* slot = nullptr;
+        uint8_t* slot = nullptr;
         if (cache) {
           const uint32_t rel = first + (uint32_t)(dir * k) - rs;
           if (rel < a.span_cache_tets) {
-            slot = cache + (size_t)rel * TS + row;
-            *slot = sp;  // overwritten below when the row has crossings
+            slot = cache + (size_t)rel * kSpanRows + row;
+            *slot = pack_span(sp);  // overwritten below when the row has crossings
           }
         }
         const TetView& tv = s.view[buf][k];
@@ -452,7 +463,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
           }
           // the adjoint's span of this row: the same edge crossings, no
           // vertex rows (empty when no edge crosses yc)
-          if (slot) *slot = span_of(xl, xr);
+          if (slot) *slot = pack_span(span_of(xl, xr));
           if (vertex_rows) {
             const float blo = fs(yc, 0.5f), bhi = fa(yc, 0.5f);
 #pragma unroll
@@ -474,7 +485,10 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
     auto cached_spans = [&](int buf, int nb) {
       row_ranges(buf, nb);
       for (int i = tid; i < TS * TS; i += NT) s.pmask[i] = 0u;
-      for (int task = tid; task < nb * TS; task += NT) (&s.span[0][0])[task] = (&s.span_pf[0][0])[task];
+      for (int task = tid; task < nb * TS; task += NT) {
+        const int k = task / TS, row = task - (task / TS) * TS;
+        s.span[k][row] = unpack_span(s.span_pf[k][row]);
+      }
     };
     // per-tet row prefix sums over the tet's reachable rows and tet-major item
     // offsets (after spans; warp 0, lane = tet)
@@ -935,8 +949,8 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
       auto span_cached = [&](uint32_t lo, int nb) -> bool {
         return scache && lo >= span_lo && lo + (uint32_t)nb - rs <= a.span_cache_tets;
       };
-      auto span_src = [&](uint32_t lo, int nb) -> const short2* {
-        return span_cached(lo, nb) ? scache + (size_t)(lo - rs) * TS : nullptr;
+      auto span_src = [&](uint32_t lo, int nb) -> const uint8_t* {
+        return span_cached(lo, nb) ? scache + (size_t)(lo - rs) * kSpanRows : nullptr;
       };
       if (re > rs) {
         // the forward's span-cache writes, before the bulk copies that read them
