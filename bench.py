@@ -48,15 +48,15 @@ N_VIEWS = 16
 LR = dict(lr_verts=1e-4, lr_dens=1e-2, lr_grads=1e-3)
 LR_SH = 2.5e-3
 # DRAM bytes (read + write) per (tile, tet) pair of the fused compositing
-# kernel, from one ncu capture of this workload's step
-# (dram__bytes_read.sum + dram__bytes_write.sum = 18.12 GB for 38.33 M pairs,
-# tiles taken longest list first, entries numbered tet-major); the
-# roofline's "traffic" scales it to the run's pair count.
-TILE_DRAM_BYTES_PER_PAIR = 473.0
+# kernel, from a one-kernel ncu capture of a 4-view case of this workload's
+# mesh and resolution mix (bench.py --views 4: 8.13 M pairs,
+# dram__bytes_read.sum + dram__bytes_write.sum = 2.437 GB); the roofline's
+# "traffic" scales it to the run's pair count.
+TILE_DRAM_BYTES_PER_PAIR = 300.0
 # Warp instructions per (tile, tet) pair of the same kernel, from the same
-# capture (smsp__inst_executed.sum = 57.42 G for 38.33 M pairs); the issue
-# ceiling is 148 SMs x 4 schedulers x one instruction per clock.
-TILE_WARP_INST_PER_PAIR = 1498.0
+# capture (smsp__inst_executed.sum = 10.16 G); the issue ceiling is 148 SMs x
+# 4 schedulers x one instruction per clock.
+TILE_WARP_INST_PER_PAIR = 1249.0
 
 
 def issue_roofline(n_pairs: int, launch_ms: float, sm_mhz) -> dict:
