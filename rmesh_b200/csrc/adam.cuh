@@ -69,12 +69,32 @@ __global__ void __launch_bounds__(256) adam_kernel(AdamArgs a) {
   const float step_f = (float)hp.step;
   const float b1p = expf(step_f * logf(hp.beta1));
   const float b2p = expf(step_f * logf(hp.beta2));
-  const long long total = (long long)a.N + a.M + (a.sh && hp.lr_sh > 0.0f ? a.n_sh : 0);
+  // units: N vertices, M tets, then the SH coefficients four at a time (16-byte
+  // loads and stores: the coefficient arrays and their gradients start on
+  // 16-byte boundaries), the last unit taking the 1-3 left over one by one
+  const long long n_sh = a.sh && hp.lr_sh > 0.0f ? a.n_sh : 0;
+  const long long total = (long long)a.N + a.M + (n_sh + 3) / 4;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
        i += (long long)gridDim.x * blockDim.x) {
     if (i >= (long long)a.N + a.M) {
-      const size_t e = (size_t)(i - a.N - a.M);
-      adam_elem(a.sh[e], a.m_sh[e], a.v_sh[e], a.d_sh[e], hp.lr_sh, hp.beta1, hp.beta2, hp.eps, b1p, b2p);
+      const long long e0 = 4 * (i - a.N - a.M);
+      if (e0 + 4 <= n_sh) {
+        const size_t q = (size_t)(e0 >> 2);
+        float4 p = reinterpret_cast<float4*>(a.sh)[q];
+        float4 m = reinterpret_cast<float4*>(a.m_sh)[q];
+        float4 v = reinterpret_cast<float4*>(a.v_sh)[q];
+        const float4 g = reinterpret_cast<const float4*>(a.d_sh)[q];
+        adam_elem(p.x, m.x, v.x, g.x, hp.lr_sh, hp.beta1, hp.beta2, hp.eps, b1p, b2p);
+        adam_elem(p.y, m.y, v.y, g.y, hp.lr_sh, hp.beta1, hp.beta2, hp.eps, b1p, b2p);
+        adam_elem(p.z, m.z, v.z, g.z, hp.lr_sh, hp.beta1, hp.beta2, hp.eps, b1p, b2p);
+        adam_elem(p.w, m.w, v.w, g.w, hp.lr_sh, hp.beta1, hp.beta2, hp.eps, b1p, b2p);
+        reinterpret_cast<float4*>(a.sh)[q] = p;
+        reinterpret_cast<float4*>(a.m_sh)[q] = m;
+        reinterpret_cast<float4*>(a.v_sh)[q] = v;
+      } else {
+        for (long long e = e0; e < n_sh; ++e)
+          adam_elem(a.sh[e], a.m_sh[e], a.v_sh[e], a.d_sh[e], hp.lr_sh, hp.beta1, hp.beta2, hp.eps, b1p, b2p);
+      }
     } else if (i < a.N) {
       const uint32_t vtx = (uint32_t)i;
 #pragma unroll

@@ -809,7 +809,7 @@ int launch_adam(RmeshCtx* c, int n_cnt, bool capturing) {
   aa.hp = c->hp_d.as<AdamParams>();
   aa.counters = c->counters_d.as<Counters>();
   aa.n_counters = n_cnt;
-  const int blocks = (int)std::min<int64_t>((c->N + c->M + aa.n_sh + 255) / 256, (int64_t)c->num_sms * 16);
+  const int blocks = (int)std::min<int64_t>((c->N + c->M + (aa.n_sh + 3) / 4 + 255) / 256, (int64_t)c->num_sms * 16);
   adam_kernel<<<std::max(1, blocks), 256, 0, c->stream>>>(aa);
   CKL();
   return RMESH_OK;
