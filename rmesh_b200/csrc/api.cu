@@ -114,8 +114,10 @@ struct RmeshCtx {
 
   // per-run
   DevBuf views_d, counters_d, hp_d, sort_state, sort_status, scan_status;
-  DevBuf vis_key, vis_val, vis_tet, vis_cnt, vis_proj, vis_view, vis_key_alt, vis_val_alt, tiles_touched;
-  DevBuf vis_color, vis_dcolor, vis_index;  // SH colours per entry, their gradients, (view, tet) -> entry
+  // per (tet, view) item, at tet * n_views + view: tiles touched, projections,
+  // tile-kernel record; compacted sort keys and values (item indices)
+  DevBuf vis_key, vis_val, vis_cnt, vis_proj, vis_view, vis_key_alt, vis_val_alt, group_off;
+  DevBuf vis_color, vis_dcolor;  // SH colours per entry and their gradients
   DevBuf pair_key, pair_val, pair_key_alt, pair_val_alt, ranges;
   DevBuf rgba, aux, dl, gt, out_a, out_b, out_c, out_d;
   DevBuf span_cache;  // per-CTA adjoint span cache of persistent train launches
@@ -414,8 +416,8 @@ int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t
   CKR(ensure_buf(c, c->vis_key_alt, items * 8));
   CKR(ensure_buf(c, c->vis_val, items * 4));
   CKR(ensure_buf(c, c->vis_val_alt, items * 4));
-  CKR(ensure_buf(c, c->vis_tet, items * 4));
   CKR(ensure_buf(c, c->vis_cnt, items * 4));
+  CKR(ensure_buf(c, c->group_off, ((items + 255) / 256 + 1) * 8));
   CKR(ensure_buf(c, c->vis_proj, items * 32));
   CKR(ensure_buf(c, c->vis_view, items * sizeof(TetView)));
   // span-cache slots: resident CTAs per SM of the run's largest configuration
@@ -423,9 +425,7 @@ int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t
   if (c->sh_degree >= 0) {
     CKR(ensure_buf(c, c->vis_color, items * 16));
     CKR(ensure_buf(c, c->vis_dcolor, items * 16));
-    CKR(ensure_buf(c, c->vis_index, items * 4));
   }
-  CKR(ensure_buf(c, c->tiles_touched, items * 4));
   if (c->cap_pairs == 0) c->cap_pairs = std::max<uint64_t>(8 * items, 1u << 16);
   CKR(ensure_buf(c, c->pair_key, c->cap_pairs * 4));
   CKR(ensure_buf(c, c->pair_val, c->cap_pairs * 4));
@@ -531,21 +531,18 @@ int run_records(RmeshCtx* c, bool capturing) {
 int run_bin(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t total_tiles, Counters* cnt,
             bool capturing, const std::vector<TileGroup>& groups) {
   const uint64_t items = (uint64_t)n_views * (uint64_t)c->M;
-  const unsigned nblk = (unsigned)((items + 255) / 256);
+  // chained scans over blocks of kCompactItems items (key compaction) and
+  // sorted entries (pair offsets)
+  const unsigned nscan = (unsigned)((items + kCompactItems - 1) / kCompactItems);
   unsigned long long* status = c->scan_status.as<unsigned long long>();
-  uint32_t* ticket = reinterpret_cast<uint32_t*>(status + nblk + 1);
+  uint32_t* ticket = reinterpret_cast<uint32_t*>(status + nscan + 1);
   {
     StageScope sc(c, kStProject, capturing);
-    CK(cudaMemsetAsync(status, 0, (size_t)(nblk + 2) * 8, c->stream));
     ProjectArgs pa;
     pa.M = (int)c->M;
     pa.n_views = n_views;
     pa.views = views_dev;
     pa.rec = c->rec.as<TetRec>();
-    pa.circ = c->circ.as<float4>();
-    pa.vis_key = c->vis_key.as<unsigned long long>();
-    pa.vis_val = c->vis_val.as<uint32_t>();
-    pa.vis_tet = c->vis_tet.as<uint32_t>();
     pa.vis_cnt = c->vis_cnt.as<uint32_t>();
     pa.vis_proj = c->vis_proj.as<float4>();
     pa.vis_view = c->vis_view.as<TetView>();
@@ -554,12 +551,21 @@ int run_bin(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t tota
     pa.sh = c->sh_degree >= 0 ? c->sh.as<float>() : nullptr;
     pa.sh_degree = c->sh_degree;
     pa.vis_color = c->vis_color.as<float4>();
-    pa.vis_index = c->vis_index.as<uint32_t>();
-    pa.tiles_touched = c->tiles_touched.as<uint32_t>();
-    pa.status = status;
-    pa.ticket = ticket;
-    pa.counters = cnt;
-    project_kernel<<<nblk, 256, 0, c->stream>>>(pa);
+    project_kernel<<<(unsigned)((items + 255) / 256), 256, 0, c->stream>>>(pa);
+    CKL();
+    CK(cudaMemsetAsync(status, 0, (size_t)(nscan + 2) * 8, c->stream));
+    CompactArgs ca;
+    ca.M = (int)c->M;
+    ca.n_views = n_views;
+    ca.views = views_dev;
+    ca.circ = c->circ.as<float4>();
+    ca.vis_cnt = c->vis_cnt.as<uint32_t>();
+    ca.vis_key = c->vis_key.as<unsigned long long>();
+    ca.vis_val = c->vis_val.as<uint32_t>();
+    ca.status = status;
+    ca.ticket = ticket;
+    ca.counters = cnt;
+    compact_keys_kernel<<<nscan, 256, 0, c->stream>>>(ca);
     CKL();
   }
   unsigned long long* tk = nullptr;
@@ -573,7 +579,18 @@ int run_bin(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t tota
   }
   {
     StageScope sc(c, kStEmit, capturing);
-    CK(cudaMemsetAsync(status, 0, (size_t)(nblk + 2) * 8, c->stream));
+    CK(cudaMemsetAsync(status, 0, (size_t)(nscan + 2) * 8, c->stream));
+    EmitScanArgs es;
+    es.tet_key_sorted = tk;
+    es.tet_val_sorted = tv;
+    es.vis_cnt = c->vis_cnt.as<uint32_t>();
+    es.n_vis_ptr = &cnt->n_vis;
+    es.group_off = c->group_off.as<unsigned long long>();
+    es.status = status;
+    es.ticket = ticket;
+    es.counters = cnt;
+    emit_scan_kernel<<<nscan, 256, 0, c->stream>>>(es);
+    CKL();
     EmitArgs ea;
     ea.views = views_dev;
     ea.tet_key_sorted = tk;
@@ -581,13 +598,12 @@ int run_bin(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t tota
     ea.vis_cnt = c->vis_cnt.as<uint32_t>();
     ea.vis_proj = c->vis_proj.as<float4>();
     ea.n_vis_ptr = &cnt->n_vis;
+    ea.group_off = c->group_off.as<unsigned long long>();
     ea.pair_key = c->pair_key.as<uint32_t>();
     ea.pair_val = c->pair_val.as<uint32_t>();
     ea.cap = c->cap_pairs;
-    ea.status = status;
-    ea.ticket = ticket;
     ea.counters = cnt;
-    emit_kernel<<<nblk, 256, 0, c->stream>>>(ea);
+    emit_kernel<<<(unsigned)((items + 255) / 256), 256, 0, c->stream>>>(ea);
     CKL();
   }
   {
@@ -728,7 +744,7 @@ int run_sh_backward(RmeshCtx* c, const ViewParams* views_dev, int n_views, bool 
   sa.views = views_dev;
   sa.rec = c->rec.as<TetRec>();
   sa.sh = c->sh.as<float>();
-  sa.vis_index = c->vis_index.as<uint32_t>();
+  sa.vis_cnt = c->vis_cnt.as<uint32_t>();
   sa.vis_dcolor = c->vis_dcolor.as<float4>();
   sa.d_sh = sh_grad(c);
   sa.grad_slot = c->grad_slot.as<float>();
@@ -1294,11 +1310,12 @@ int rmesh_get_info(RmeshCtx* c, RmeshInfo* info) {
   DevBuf* all[] = {&c->verts, &c->idx, &c->dens, &c->cgrad, &c->base, &c->circ, &c->m_verts, &c->v_verts,
                    &c->m_dens, &c->v_dens, &c->m_cgrad, &c->v_cgrad, &c->m_base, &c->v_base, &c->rec,
                    &c->color4, &c->grad_slot, &c->csr_off, &c->csr_ref, &c->views_d, &c->counters_d, &c->hp_d,
-                   &c->sort_state, &c->sort_status, &c->scan_status, &c->vis_key, &c->vis_val, &c->vis_tet,
-                   &c->vis_cnt, &c->vis_proj, &c->vis_view, &c->vis_key_alt, &c->vis_val_alt, &c->tiles_touched, &c->pair_key,
+                   &c->sort_state, &c->sort_status, &c->scan_status, &c->vis_key, &c->vis_val, &c->group_off,
+                   &c->vis_cnt, &c->vis_proj, &c->vis_view, &c->vis_key_alt, &c->vis_val_alt, &c->pair_key,
                    &c->pair_val, &c->pair_key_alt, &c->pair_val_alt, &c->ranges, &c->rgba, &c->aux, &c->dl,
                    &c->gt, &c->out_a, &c->out_b, &c->out_c, &c->out_d, &c->sh, &c->m_sh, &c->v_sh,
-                   &c->vis_color, &c->vis_dcolor, &c->vis_index, &c->err_in, &c->err_out, &c->aux_data};
+                   &c->vis_color, &c->vis_dcolor, &c->err_in, &c->err_out, &c->aux_data, &c->dl_aux, &c->d_aux,
+                   &c->span_cache, &c->tile_order, &c->order_hist, &c->tickets};
   for (DevBuf* b : all) info->device_bytes += b->bytes;
   return RMESH_OK;
 }
@@ -1737,7 +1754,8 @@ int rmesh_debug_tiles_touched(RmeshCtx* c, uint32_t* out) {
   if (!c || !out) return RMESH_ERR_INVALID_ARG;
   DevGuard dg__(c);
   if (!c->have_forward) return fail(c, RMESH_ERR_STATE, "no forward yet");
-  CK(cudaMemcpyAsync(out, c->tiles_touched.p, (size_t)c->M * 4, cudaMemcpyDefault, c->stream));
+  // the single-view forward's items are the tet ids
+  CK(cudaMemcpyAsync(out, c->vis_cnt.p, (size_t)c->M * 4, cudaMemcpyDefault, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return RMESH_OK;
 }
@@ -1750,13 +1768,13 @@ int rmesh_debug_pairs(RmeshCtx* c, uint32_t* tiles, uint32_t* tets, uint64_t cap
   const uint64_t k = std::min<uint64_t>(cap, c->last_n_pairs);
   if (k && tiles) CK(cudaMemcpyAsync(tiles, c->sorted_pair_key, k * 4, cudaMemcpyDefault, c->stream));
   if (k && tets) {
-    // the pair payload is the compact (view, tet) index: map it to tet ids in
-    // the pair buffer the sort left free
+    // the pair payload is the item index tet * n_views + view: map it to tet
+    // ids in the pair buffer the sort left free
     uint32_t* scratch = c->sorted_pair_val == c->pair_val.as<uint32_t>() ? c->pair_val_alt.as<uint32_t>()
                                                                           : c->pair_val.as<uint32_t>();
     const int blocks = (int)std::min<uint64_t>((k + 255) / 256, (uint64_t)c->num_sms * 8);
-    pair_tets_kernel<<<blocks, 256, 0, c->stream>>>(c->sorted_pair_key, c->sorted_pair_val, c->vis_tet.as<uint32_t>(),
-                                                     k, scratch);
+    pair_tets_kernel<<<blocks, 256, 0, c->stream>>>(c->sorted_pair_key, c->sorted_pair_val,
+                                                     (uint32_t)std::max(c->last_views, 1), k, scratch);
     CKL();
     CK(cudaMemcpyAsync(tets, scratch, k * 4, cudaMemcpyDefault, c->stream));
   }

@@ -1,8 +1,9 @@
 // Tile binning: emit (tile, tet) pairs in depth order, then per-tile ranges.
 //
 // Order of work (B200 design): tets are first sorted by (view, ~depth) at tet
-// granularity (onesweep, 32 + view bits), then each tet emits its tiles at
-// offsets given by a chained scan of tiles_touched in that order, and a short
+// granularity (onesweep, 32 + view bits; the tile count rides in the key's
+// high bits), then each tet emits its tiles at offsets given by a scan of
+// tiles_touched in that order (emit_scan_kernel), and a short
 // stable sort on the global tile id (ceil(log2 tiles) bits) finishes the job.
 // Per tile this yields exactly the reference's order -- ascending 64-bit key
 // (tile << 32 | ~depth) with ties broken by tet id -- while the pair-level sort
@@ -20,36 +21,95 @@
 
 namespace rm {
 
-struct EmitArgs {
-  const ViewParams* views;
-  const unsigned long long* tet_key_sorted;  // (view << 32) | ~depth, sorted
-  const uint32_t* tet_val_sorted;            // compact index j
-  const uint32_t* vis_cnt;
-  const float4* vis_proj;
+// Pair offsets of the sorted entries: a chained scan of their tile counts in
+// sorted order over blocks of kCompactItems entries (kCompactPerThread
+// consecutive entries per thread).  It writes the exclusive offset of every
+// 256-entry group (the emission kernel's blocks; group g of a scan block is
+// warp g's entries) and the total pair count.
+struct EmitScanArgs {
+  const unsigned long long* tet_key_sorted;  // count << 40 | view << 32 | ~depth, sorted
+  const uint32_t* tet_val_sorted;            // item index
+  const uint32_t* vis_cnt;                   // counts of items whose key count saturated
   const uint32_t* n_vis_ptr;
-  uint32_t* pair_key;   // global tile id
-  uint32_t* pair_val;   // compact index j of the (view, tet) entry (its per-view record)
-  unsigned long long cap;
+  unsigned long long* group_off;             // [ceil(n / 256)] exclusive pair offset of each group
   unsigned long long* status;
   uint32_t* ticket;
   Counters* counters;
 };
 
-__global__ void __launch_bounds__(256) emit_kernel(EmitArgs a) {
+__device__ __forceinline__ uint32_t key_count(unsigned long long key, uint32_t val, const uint32_t* vis_cnt) {
+  const uint32_t c = (uint32_t)(key >> 40);
+  return c < kKeyCountMax ? c : vis_cnt[val];
+}
+
+__global__ void __launch_bounds__(256) emit_scan_kernel(EmitScanArgs a) {
   __shared__ uint32_t s_blk;
-  __shared__ unsigned long long s_wsum[8];
+  __shared__ unsigned long long s_warp[8];
   __shared__ unsigned long long s_prefix;
   if (threadIdx.x == 0) s_blk = atomicAdd(a.ticket, 1u);
   __syncthreads();
   const uint32_t blk = s_blk;
   const uint32_t n = *a.n_vis_ptr;
-  if ((unsigned long long)blk * 256ull >= n) return;  // later blocks never wait on this one
+  if ((unsigned long long)blk * kCompactItems >= n) return;  // later blocks never wait on this one
+  const unsigned long long k0 = (unsigned long long)blk * kCompactItems + (unsigned long long)threadIdx.x * kCompactPerThread;
+  unsigned long long mine = 0;
+#pragma unroll
+  for (int q = 0; q < kCompactPerThread; ++q)
+    if (k0 + q < n) mine += key_count(a.tet_key_sorted[k0 + q], a.tet_val_sorted[k0 + q], a.vis_cnt);
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned long long x = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  unsigned long long woff = 0, btot = 0;
+#pragma unroll
+  for (int w = 0; w < 8; ++w) {
+    if (w < warp) woff += s_warp[w];
+    btot += s_warp[w];
+  }
+  if (warp == 0) {
+    const unsigned long long pre = chained_lookback(a.status, blk, btot, &a.counters->err);
+    if (lane == 0) s_prefix = pre;
+  }
+  __syncthreads();
+  const unsigned long long group = (unsigned long long)blk * (kCompactItems / 256) + (unsigned long long)warp;
+  if (lane == 0 && group * 256ull < n) a.group_off[group] = s_prefix + woff;
+  if (threadIdx.x == 0 && (unsigned long long)(blk + 1) * kCompactItems >= n) a.counters->n_pairs = s_prefix + btot;
+}
+
+struct EmitArgs {
+  const ViewParams* views;
+  const unsigned long long* tet_key_sorted;  // count << 40 | view << 32 | ~depth, sorted
+  const uint32_t* tet_val_sorted;            // item index i (its per-view record and projections)
+  const uint32_t* vis_cnt;
+  const float4* vis_proj;
+  const uint32_t* n_vis_ptr;
+  const unsigned long long* group_off;       // from emit_scan_kernel
+  uint32_t* pair_key;   // global tile id
+  uint32_t* pair_val;   // item index of the (view, tet) entry
+  unsigned long long cap;
+  Counters* counters;
+};
+
+// One thread per sorted entry, 256 entries per block: the block's pair
+// offset comes from emit_scan_kernel, so blocks never wait on each other.
+__global__ void __launch_bounds__(256) emit_kernel(EmitArgs a) {
+  __shared__ unsigned long long s_wsum[8];
+  const uint32_t blk = blockIdx.x;
+  const uint32_t n = *a.n_vis_ptr;
+  if ((unsigned long long)blk * 256ull >= n) return;
   const uint32_t k = blk * 256u + threadIdx.x;
   const bool in = k < n;
+  unsigned long long key = 0ull;
   uint32_t j = 0, cnt = 0;
   if (in) {
+    key = a.tet_key_sorted[k];
     j = a.tet_val_sorted[k];
-    cnt = a.vis_cnt[j];
+    cnt = key_count(key, j, a.vis_cnt);
   }
   // block exclusive scan of cnt (64-bit)
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -61,25 +121,16 @@ __global__ void __launch_bounds__(256) emit_kernel(EmitArgs a) {
   }
   if (lane == 31) s_wsum[warp] = x;
   __syncthreads();
-  unsigned long long woff = 0, btot = 0;
+  unsigned long long woff = 0;
 #pragma unroll
-  for (int w = 0; w < 8; ++w) {
+  for (int w = 0; w < 8; ++w)
     if (w < warp) woff += s_wsum[w];
-    btot += s_wsum[w];
-  }
-  if (warp == 0) {
-    const unsigned long long pre = chained_lookback(a.status, blk, btot, &a.counters->err);
-    if (lane == 0) s_prefix = pre;
-  }
-  __syncthreads();
-  const unsigned long long off = s_prefix + woff + x - cnt;
-  if (!in) return;
-  if (k == n - 1) a.counters->n_pairs = off + cnt;
-  if (cnt == 0) return;
+  if (!in || cnt == 0) return;
+  const unsigned long long off = a.group_off[blk] + woff + x - cnt;
 
-  const uint32_t view = (uint32_t)(a.tet_key_sorted[k] >> 32);
+  const uint32_t view = (uint32_t)(key >> 32) & 0xFFu;
   const ViewParams& V = a.views[view];
-  const float4 q0 = a.vis_proj[2 * j], q1 = a.vis_proj[2 * j + 1];
+  const float4 q0 = a.vis_proj[2 * (size_t)j], q1 = a.vis_proj[2 * (size_t)j + 1];
   const float px[4] = {q0.x, q0.z, q1.x, q1.z};
   const float py[4] = {q0.y, q0.w, q1.y, q1.w};
   uint32_t local = 0;
@@ -220,14 +271,14 @@ __global__ void __launch_bounds__(256) ranges_kernel(const uint32_t* __restrict_
   }
 }
 
-// Debug view of the sorted pairs: the pair payload is the compact (view, tet)
-// index; map it back to the tet id (sentinel slots keep the reference's 0).
+// Debug view of the sorted pairs: the pair payload is the item index
+// tet * n_views + view; map it back to the tet id (sentinel slots keep the
+// reference's 0).
 __global__ void __launch_bounds__(256) pair_tets_kernel(const uint32_t* __restrict__ keys,
-                                                        const uint32_t* __restrict__ vals,
-                                                        const uint32_t* __restrict__ vis_tet, uint64_t n,
-                                                        uint32_t* __restrict__ out) {
+                                                        const uint32_t* __restrict__ vals, uint32_t n_views,
+                                                        uint64_t n, uint32_t* __restrict__ out) {
   for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
-    out[i] = keys[i] == kSentinel ? 0u : vis_tet[vals[i]];
+    out[i] = keys[i] == kSentinel ? 0u : vals[i] / n_views;
 }
 
 }  // namespace rm

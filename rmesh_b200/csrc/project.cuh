@@ -4,8 +4,9 @@
 // Reference: crates/rmesh-render/src/wgsl/project_compute.wgsl:88-325 (cull,
 // tiles_touched, colours) and tile_gen_scan_compute.wgsl:135-143 (the
 // circumsphere depth key used for the tile sort).  The reference compacts with
-// atomicAdd (project_compute.wgsl:181); here compaction is a single-pass
-// chained scan in (view, tet) order, so downstream order is deterministic.
+// atomicAdd (project_compute.wgsl:181); here every (tet, view) item keeps its
+// own slot and only the sort keys are compacted, by a chained scan in item
+// order, so downstream order is deterministic.
 #pragma once
 #include <cuda_fp16.h>
 
@@ -250,34 +251,144 @@ struct ProjectArgs {
   int n_views;
   const ViewParams* views;
   const TetRec* rec;
-  const float4* circ;
-  // compaction outputs, index j over the tile-touching (tet, view) items in
-  // tet-major order (within one view: ascending tet id, which is the tie
-  // order of the stable (view, depth) sort)
-  unsigned long long* vis_key;  // (view << 32) | ~bits(depth)
-  uint32_t* vis_val;            // j (sort payload)
-  uint32_t* vis_tet;
-  uint32_t* vis_cnt;            // tiles_touched
+  // per-item outputs at the item index i = tet * n_views + view (an entry's
+  // index is its item index; items that touch no tile write only vis_cnt)
+  uint32_t* vis_cnt;            // tiles_touched of a tile-touching item, 0 otherwise
   float4* vis_proj;             // 2 per entry: division-projected pixel coords (emission)
   TetView* vis_view;            // per entry: the tile kernel's per-(view, tet) record
   const float4* color4;         // tet colours, [view * color_view_stride + tet]
   uint32_t color_view_stride;
   // SH colours (sh != nullptr): coefficients [M][3][nc]; the colour of each
-  // tile-touching entry goes to vis_color[j], and vis_index maps every item
-  // (tet * n_views + view) to its entry j (0xFFFFFFFF when it touches no tile)
+  // tile-touching entry goes to vis_color[i]
   const float* sh;
   int sh_degree;
   float4* vis_color;
-  uint32_t* vis_index;
-  uint32_t* tiles_touched;      // optional [M * n_views], indexed by tet * n_views + view
-  unsigned long long* status;   // chained-scan status, one word per block (zeroed)
-  uint32_t* ticket;             // block ticket (zeroed)
-  Counters* counters;
 };
 
+// One thread per (tet, view) item, items tet-major: a tet's views are
+// neighbouring threads, so its record and SH coefficients are read once for
+// all views.  A pure map (no scan, no block barrier): the entry data goes to
+// the item's own index, and compact_keys_kernel then packs the sort keys of
+// the tile-touching items in item order.
 // 3 resident blocks per SM: the register cap keeps the SH coefficients of
 // the 16-byte loads in registers without dropping to 2 blocks
 __global__ void __launch_bounds__(256, 3) project_kernel(ProjectArgs a) {
+  const unsigned long long total_items = (unsigned long long)a.M * (unsigned long long)a.n_views;
+  const unsigned long long i = (unsigned long long)blockIdx.x * 256ull + threadIdx.x;
+  if (i >= total_items) return;
+  const uint32_t tet = (uint32_t)(i / (unsigned long long)a.n_views);
+  const uint32_t view = (uint32_t)(i - (unsigned long long)tet * a.n_views);
+  const ViewParams& V = a.views[view];
+  const TetRec r = a.rec[tet];
+  const float vx[4] = {r.a.x, r.b.x, r.c.x, r.d.x};
+  const float vy[4] = {r.a.y, r.b.y, r.c.y, r.d.y};
+  const float vz[4] = {r.a.z, r.b.z, r.c.z, r.d.z};
+  float p[4][4], c[4][4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    clip_exact(V.vp, vx[k], vy[k], vz[k], c[k]);
+    const float inv_w = fdv(1.0f, fa(c[k][3], 1e-6f));
+    p[k][0] = fm(c[k][0], inv_w);
+    p[k][1] = fm(c[k][1], inv_w);
+    p[k][2] = fm(c[k][2], inv_w);
+    p[k][3] = c[k][3];
+  }
+  const bool any_behind = (p[0][3] <= 0.0f) || (p[1][3] <= 0.0f) || (p[2][3] <= 0.0f) || (p[3][3] <= 0.0f);
+  bool visible = true;
+  if (!any_behind) {
+    const float min_x = fminf(fminf(p[0][0], p[1][0]), fminf(p[2][0], p[3][0]));
+    const float max_x = fmaxf(fmaxf(p[0][0], p[1][0]), fmaxf(p[2][0], p[3][0]));
+    const float min_y = fminf(fminf(p[0][1], p[1][1]), fminf(p[2][1], p[3][1]));
+    const float max_y = fmaxf(fmaxf(p[0][1], p[1][1]), fmaxf(p[2][1], p[3][1]));
+    const float min_z = fminf(fminf(p[0][2], p[1][2]), fminf(p[2][2], p[3][2]));
+    if (max_x < -1.0f || min_x > 1.0f || max_y < -1.0f || min_y > 1.0f || min_z > 1.0f) visible = false;
+    const float ext_x = fm(fs(max_x, min_x), V.Wf);
+    const float ext_y = fm(fs(max_y, min_y), V.Hf);
+    if (fm(ext_x, ext_y) < 1.0f) visible = false;
+  }
+  if (visible) {  // optical-depth cull (project_compute.wgsl:146-162)
+    float e2[6];
+    const int ei[6] = {1, 2, 3, 2, 3, 3};
+    const int ej[6] = {0, 0, 0, 1, 1, 2};
+#pragma unroll
+    for (int e = 0; e < 6; ++e) {
+      const float dx = fs(vx[ei[e]], vx[ej[e]]), dy = fs(vy[ei[e]], vy[ej[e]]), dz = fs(vz[ei[e]], vz[ej[e]]);
+      e2[e] = dot3x(dx, dy, dz, dx, dy, dz);
+    }
+    const float m = fmaxf(fmaxf(e2[0], fmaxf(e2[1], e2[2])), fmaxf(e2[3], fmaxf(e2[4], e2[5])));
+    if (fm(r.a.w, __fsqrt_rn(m)) < 0.01f) visible = false;
+  }
+  uint32_t count = 0;
+  if (visible && !any_behind) {
+    float px[4], py[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      px[k] = fm(fm(fa(p[k][0], 1.0f), 0.5f), V.Wf);
+      py[k] = fm(fm(fs(1.0f, p[k][1]), 0.5f), V.Hf);
+    }
+    scanline_tiles(px, py, V.Wf, V.Hf, (uint32_t)V.TS,
+                   [&](uint32_t, uint32_t tx0, uint32_t tx1) { count += tx1 - tx0 + 1u; });
+  }
+  const bool flag = visible && count > 0u;
+  a.vis_cnt[i] = flag ? count : 0u;
+  if (!flag) return;
+  // division-projected coords used by the emission stage (tile_gen_scan_compute.wgsl:108-117)
+  float qx[4], qy[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float w = fa(c[k][3], 1e-6f);
+    qx[k] = fm(fm(fa(fdv(c[k][0], w), 1.0f), 0.5f), V.Wf);
+    qy[k] = fm(fm(fs(1.0f, fdv(c[k][1], w)), 0.5f), V.Hf);
+  }
+  a.vis_proj[2 * i] = make_float4(qx[0], qy[0], qx[1], qy[1]);
+  a.vis_proj[2 * i + 1] = make_float4(qx[2], qy[2], qx[3], qy[3]);
+  if (a.vis_view) {
+    float4 col;
+    if (a.sh) {
+      const int nc = (a.sh_degree + 1) * (a.sh_degree + 1);
+      col = sh_color_deg(a.sh_degree, r, a.sh + (size_t)tet * 3 * nc, V.cam);
+      a.vis_color[i] = col;
+    } else {
+      col = a.color4[(size_t)a.color_view_stride * view + tet];
+    }
+    write_tet_view(a.vis_view + i, r, col, V, tet, (uint32_t)i);
+  }
+}
+
+// Depth key of (tet, view) (tile_gen_scan_compute.wgsl:136-143): ~bits of the
+// squared distance camera -> circumcentre minus the squared circumradius, so
+// an ascending sort is back to front.
+__device__ __forceinline__ uint32_t depth_key(const float4 C, const float* cam) {
+  const float dx = fs(C.x, cam[0]), dy = fs(C.y, cam[1]), dz = fs(C.z, cam[2]);
+  const float depth = fs(dot3x(dx, dy, dz, dx, dy, dz), C.w);
+  return ~__float_as_uint(depth);
+}
+
+// Sort keys of the tile-touching items, compacted in item order (within one
+// view: ascending tet id, the tie order of the stable (view, depth) sort):
+//   key = count << 40 | view << 32 | ~bits(depth),  value = item index.
+// The sort orders bits 0..39 only (view < 64); the tile count rides in bits
+// 40..63 for the emission stage (saturated at kKeyCountMax, which then reads
+// vis_cnt).  A chained scan over blocks of kCompactItems items, each thread
+// taking kCompactPerThread consecutive items.
+constexpr int kCompactPerThread = 8;
+constexpr int kCompactItems = 256 * kCompactPerThread;
+constexpr uint32_t kKeyCountMax = (1u << 24) - 1u;
+
+struct CompactArgs {
+  int M;
+  int n_views;
+  const ViewParams* views;
+  const float4* circ;
+  const uint32_t* vis_cnt;
+  unsigned long long* vis_key;
+  uint32_t* vis_val;
+  unsigned long long* status;  // chained-scan status, one word per block (zeroed)
+  uint32_t* ticket;            // block ticket (zeroed)
+  Counters* counters;
+};
+
+__global__ void __launch_bounds__(256) compact_keys_kernel(CompactArgs a) {
   __shared__ uint32_t s_blk;
   __shared__ uint32_t s_warp[8];
   __shared__ unsigned long long s_prefix;
@@ -285,88 +396,29 @@ __global__ void __launch_bounds__(256, 3) project_kernel(ProjectArgs a) {
   __syncthreads();
   const uint32_t blk = s_blk;
   const unsigned long long total_items = (unsigned long long)a.M * (unsigned long long)a.n_views;
-  const unsigned long long i = (unsigned long long)blk * 256ull + threadIdx.x;
-
-  bool flag = false;
-  uint32_t count = 0, inv_depth = 0, view = 0, tet = 0;
-  float qx[4], qy[4];
-  if (i < total_items) {
-    // items tet-major: a tet's views are neighbouring threads, so its record
-    // and SH coefficients are read once for all views
-    tet = (uint32_t)(i / (unsigned long long)a.n_views);
-    view = (uint32_t)(i - (unsigned long long)tet * a.n_views);
-    const ViewParams& V = a.views[view];
-    const TetRec r = a.rec[tet];
-    const float vx[4] = {r.a.x, r.b.x, r.c.x, r.d.x};
-    const float vy[4] = {r.a.y, r.b.y, r.c.y, r.d.y};
-    const float vz[4] = {r.a.z, r.b.z, r.c.z, r.d.z};
-    float p[4][4], c[4][4];
+  const unsigned long long i0 = (unsigned long long)blk * kCompactItems + (unsigned long long)threadIdx.x * kCompactPerThread;
+  uint32_t cnt[kCompactPerThread];
+  if (i0 + kCompactPerThread <= total_items) {  // i0 is a multiple of 8: 32-byte aligned
+    const uint4 c0 = __ldg(reinterpret_cast<const uint4*>(a.vis_cnt + i0));
+    const uint4 c1 = __ldg(reinterpret_cast<const uint4*>(a.vis_cnt + i0 + 4));
+    cnt[0] = c0.x; cnt[1] = c0.y; cnt[2] = c0.z; cnt[3] = c0.w;
+    cnt[4] = c1.x; cnt[5] = c1.y; cnt[6] = c1.z; cnt[7] = c1.w;
+  } else {
 #pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      clip_exact(V.vp, vx[k], vy[k], vz[k], c[k]);
-      const float inv_w = fdv(1.0f, fa(c[k][3], 1e-6f));
-      p[k][0] = fm(c[k][0], inv_w);
-      p[k][1] = fm(c[k][1], inv_w);
-      p[k][2] = fm(c[k][2], inv_w);
-      p[k][3] = c[k][3];
-    }
-    const bool any_behind = (p[0][3] <= 0.0f) || (p[1][3] <= 0.0f) || (p[2][3] <= 0.0f) || (p[3][3] <= 0.0f);
-    bool visible = true;
-    if (!any_behind) {
-      const float min_x = fminf(fminf(p[0][0], p[1][0]), fminf(p[2][0], p[3][0]));
-      const float max_x = fmaxf(fmaxf(p[0][0], p[1][0]), fmaxf(p[2][0], p[3][0]));
-      const float min_y = fminf(fminf(p[0][1], p[1][1]), fminf(p[2][1], p[3][1]));
-      const float max_y = fmaxf(fmaxf(p[0][1], p[1][1]), fmaxf(p[2][1], p[3][1]));
-      const float min_z = fminf(fminf(p[0][2], p[1][2]), fminf(p[2][2], p[3][2]));
-      if (max_x < -1.0f || min_x > 1.0f || max_y < -1.0f || min_y > 1.0f || min_z > 1.0f) visible = false;
-      const float ext_x = fm(fs(max_x, min_x), V.Wf);
-      const float ext_y = fm(fs(max_y, min_y), V.Hf);
-      if (fm(ext_x, ext_y) < 1.0f) visible = false;
-    }
-    if (visible) {  // optical-depth cull (project_compute.wgsl:146-162)
-      float e2[6];
-      const int ei[6] = {1, 2, 3, 2, 3, 3};
-      const int ej[6] = {0, 0, 0, 1, 1, 2};
-#pragma unroll
-      for (int e = 0; e < 6; ++e) {
-        const float dx = fs(vx[ei[e]], vx[ej[e]]), dy = fs(vy[ei[e]], vy[ej[e]]), dz = fs(vz[ei[e]], vz[ej[e]]);
-        e2[e] = dot3x(dx, dy, dz, dx, dy, dz);
-      }
-      const float m = fmaxf(fmaxf(e2[0], fmaxf(e2[1], e2[2])), fmaxf(e2[3], fmaxf(e2[4], e2[5])));
-      if (fm(r.a.w, __fsqrt_rn(m)) < 0.01f) visible = false;
-    }
-    if (visible && !any_behind) {
-      float px[4], py[4];
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        px[k] = fm(fm(fa(p[k][0], 1.0f), 0.5f), V.Wf);
-        py[k] = fm(fm(fs(1.0f, p[k][1]), 0.5f), V.Hf);
-      }
-      scanline_tiles(px, py, V.Wf, V.Hf, (uint32_t)V.TS,
-                     [&](uint32_t, uint32_t tx0, uint32_t tx1) { count += tx1 - tx0 + 1u; });
-    }
-    if (a.tiles_touched) a.tiles_touched[i] = (visible ? count : 0u);
-    flag = visible && count > 0u;
-    if (a.vis_index && !flag) a.vis_index[i] = kSentinel;
-    if (flag) {
-      // depth key (tile_gen_scan_compute.wgsl:136-143)
-      const float4 C = a.circ[tet];
-      const float dx = fs(C.x, V.cam[0]), dy = fs(C.y, V.cam[1]), dz = fs(C.z, V.cam[2]);
-      const float depth = fs(dot3x(dx, dy, dz, dx, dy, dz), C.w);
-      inv_depth = ~__float_as_uint(depth);
-      // division-projected coords used by the emission stage (:108-117)
-#pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const float w = fa(c[k][3], 1e-6f);
-        qx[k] = fm(fm(fa(fdv(c[k][0], w), 1.0f), 0.5f), V.Wf);
-        qy[k] = fm(fm(fs(1.0f, fdv(c[k][1], w)), 0.5f), V.Hf);
-      }
-    }
+    for (int q = 0; q < kCompactPerThread; ++q) cnt[q] = i0 + q < total_items ? a.vis_cnt[i0 + q] : 0u;
   }
-  // block-level exclusive scan of flags
+  uint32_t mine = 0;
+#pragma unroll
+  for (int q = 0; q < kCompactPerThread; ++q) mine += cnt[q] ? 1u : 0u;
+  // block exclusive scan of the per-thread flag counts
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const unsigned ballot = __ballot_sync(0xffffffffu, flag);
-  if (lane == 0) s_warp[warp] = __popc(ballot);
+  uint32_t x = mine;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
   __syncthreads();
   uint32_t warp_off = 0, block_total = 0;
 #pragma unroll
@@ -380,33 +432,30 @@ __global__ void __launch_bounds__(256, 3) project_kernel(ProjectArgs a) {
     if (lane == 0) s_prefix = pre;
   }
   __syncthreads();
-  const unsigned long long base = s_prefix;
-  if (flag) {
-    const unsigned long long j = base + warp_off + __popc(ballot & ((1u << lane) - 1u));
-    a.vis_key[j] = ((unsigned long long)view << 32) | inv_depth;
-    a.vis_val[j] = (uint32_t)j;
-    a.vis_tet[j] = tet;
-    a.vis_cnt[j] = count;
-    a.vis_proj[2 * j] = make_float4(qx[0], qy[0], qx[1], qy[1]);
-    a.vis_proj[2 * j + 1] = make_float4(qx[2], qy[2], qx[3], qy[3]);
-    if (a.vis_view) {
-      const TetRec r = a.rec[tet];
-      float4 col;
-      if (a.sh) {
-        const int nc = (a.sh_degree + 1) * (a.sh_degree + 1);
-        col = sh_color_deg(a.sh_degree, r, a.sh + (size_t)tet * 3 * nc, a.views[view].cam);
-        a.vis_color[j] = col;
-        a.vis_index[i] = (uint32_t)j;
-      } else {
-        col = a.color4[(size_t)a.color_view_stride * view + tet];
+  unsigned long long j = s_prefix + warp_off + x - mine;
+  if (mine) {
+    uint32_t tet = (uint32_t)(i0 / (unsigned long long)a.n_views);
+    uint32_t view = (uint32_t)(i0 - (unsigned long long)tet * a.n_views);
+    float4 C = a.circ[tet];
+#pragma unroll
+    for (int q = 0; q < kCompactPerThread; ++q) {
+      if (cnt[q]) {
+        const unsigned long long c24 = cnt[q] < kKeyCountMax ? cnt[q] : kKeyCountMax;
+        a.vis_key[j] = (c24 << 40) | ((unsigned long long)view << 32) | depth_key(C, a.views[view].cam);
+        a.vis_val[j] = (uint32_t)(i0 + q);
+        ++j;
       }
-      write_tet_view(a.vis_view + j, r, col, a.views[view], tet, (uint32_t)j);
+      if (++view == (uint32_t)a.n_views && q + 1 < kCompactPerThread) {
+        view = 0;
+        ++tet;
+        if (i0 + q + 1 < total_items) C = a.circ[tet];
+      }
     }
   }
-  // the block holding the last item publishes the visible count
-  if (threadIdx.x == 0 && (unsigned long long)(blk + 1) * 256ull >= total_items &&
-      (unsigned long long)blk * 256ull < total_items)
-    a.counters->n_vis = (uint32_t)(base + block_total);
+  // the block holding the last item publishes the compacted count
+  if (threadIdx.x == 0 && (unsigned long long)(blk + 1) * kCompactItems >= total_items &&
+      (unsigned long long)blk * kCompactItems < total_items)
+    a.counters->n_vis = (uint32_t)(s_prefix + block_total);
 }
 
 }  // namespace rm

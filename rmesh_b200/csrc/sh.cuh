@@ -5,8 +5,9 @@
 // c the tet centroid and dir = normalize(c - cam).  The reference has no
 // adjoint for it; this kernel is one.  The tile kernel leaves, for every
 // tile-touching (view, tet) entry j, the gradient of the loss with respect to
-// that entry's colour in vis_dcolor[j].  One thread per tet then walks the
-// run's views, finds its entry through vis_index[tet * n_views + view], and chains
+// that entry's colour in vis_dcolor[j], j = tet * n_views + view.  One thread
+// per tet then walks the run's views (an entry exists where vis_cnt[j] > 0, the
+// tet touched a tile of that view; its gradients are contiguous), and chains
 // the colour gradient through softplus (math.wgsl:27-33), the SH basis, the
 // offset dot(g, v0 - c) and the view direction:
 //   d coeff[ch][i] += d_rgb[ch] * basis_i(dir)
@@ -70,8 +71,8 @@ struct ShBackwardArgs {
   const ViewParams* views;
   const TetRec* rec;
   const float* sh;           // [M][3][nc] fp32 coefficients (read as f16, as in the forward)
-  const uint32_t* vis_index; // [M * n_views] entry of (tet, view) at tet * n_views + view, or kSentinel
-  const float4* vis_dcolor;  // [entries] colour gradient per entry
+  const uint32_t* vis_cnt;   // [M * n_views] tiles touched by (tet, view) at tet * n_views + view
+  const float4* vis_dcolor;  // [M * n_views] colour gradient per entry
   float* d_sh;               // [M][3][nc], accumulated
   float* grad_slot;          // [M][kGradSlot], colour gradient [4..6] and vertices [7..18] accumulated
 };
@@ -84,7 +85,7 @@ __global__ void __launch_bounds__(128, 4) sh_backward_kernel(ShBackwardArgs a) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= a.M) return;
   bool any = false;
-  for (int v = 0; v < a.n_views && !any; ++v) any = a.vis_index[(size_t)t * a.n_views + v] != kSentinel;
+  for (int v = 0; v < a.n_views && !any; ++v) any = a.vis_cnt[(size_t)t * a.n_views + v] != 0u;
   if (!any) return;
   const TetRec r = a.rec[t];
   // a tet's 3 nc floats keep 16-byte alignment at degrees 1 and 3: vector
@@ -109,8 +110,8 @@ __global__ void __launch_bounds__(128, 4) sh_backward_kernel(ShBackwardArgs a) {
   float dc0 = 0.f, dc1 = 0.f, dc2 = 0.f;  // d centroid
   float dv00 = 0.f, dv01 = 0.f, dv02 = 0.f;  // d v0 beyond the centroid share
   for (int v = 0; v < a.n_views; ++v) {
-    const uint32_t j = a.vis_index[(size_t)t * a.n_views + v];
-    if (j == kSentinel) continue;
+    const size_t j = (size_t)t * a.n_views + v;
+    if (a.vis_cnt[j] == 0u) continue;
     const float4 dcol = a.vis_dcolor[j];
     if (dcol.x == 0.f && dcol.y == 0.f && dcol.z == 0.f) continue;
     float3 cen, dir;

@@ -55,9 +55,11 @@ def _as_array(x, dtype, name: str):
                 x = x.to(torch.int32)
             else:
                 raise TypeError(f"{name}: expected a {tdt} tensor, got {x.dtype}")
+        x = x.contiguous()
+        # the library reads the tensor on its own stream: finish torch's pending
+        # work on it first (including the copy contiguous() may have queued)
         if x.is_cuda:
             torch.cuda.current_stream(x.device).synchronize()
-        x = x.contiguous()
         return x, x.data_ptr()
     a = np.asarray(x)
     if a.dtype != dtype:
