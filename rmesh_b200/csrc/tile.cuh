@@ -61,6 +61,9 @@ __device__ __forceinline__ short2 unpack_span(uint8_t v) {
 }
 constexpr int kMom = 24;      // adjoint moments per tet (see phase 2)
 constexpr int kMomHalf = 12;  // moments transposed per reduction pass
+// per-lane row of the warp's reduction buffer: 16 face sums (face f at 4f..4f+3)
+// and the tet slot at column 16; odd stride, so lanes hit distinct banks
+constexpr int kRedCols = 17;
 
 enum TileMode : int { kModeForward = 0, kModeBackward = 1, kModeTrain = 2, kModeError = 3 };
 
@@ -117,10 +120,10 @@ template <int TS, bool AUX, bool WIDE = false>
 struct TileCfg {
   static constexpr int NT = (WIDE ? 2 : 1) * (((TS * TS + 31) / 32) * 32);
   static constexpr int NW = NT / 32;
-  // items per sub-batch; 832 for 12x12 tiles fills a quarter of the SM's
+  // items per sub-batch; 792 for 12x12 tiles fills a quarter of the SM's
   // 228 KB of shared memory (four resident CTAs, the register limit at 96
   // registers per thread): fewer sub-batches, fewer block barriers
-  static constexpr int CAP = WIDE ? (TS == 8 ? 512 : (TS == 12 ? 2048 : 1024)) : (TS == 12 ? 832 : 512);
+  static constexpr int CAP = WIDE ? (TS == 8 ? 512 : (TS == 12 ? 2048 : 1024)) : (TS == 12 ? 792 : 512);
   // resident CTAs per SM the register budget is sized for
   static constexpr int MINB = (WIDE ? 1 : 2) * (TS == 16 ? 1 : (TS == 12 ? 2 : 4));
 };
@@ -135,10 +138,10 @@ struct __align__(16) TileSmem {
   float4 pdl[TS * TS];      // pixel dL/dRGB (adjoint)
   float4 item[Cfg::CAP];    // (cp.rgb, od) -> adjoint: (t_prev, d_od_state, has, aux_s)
   float4 itemx[Cfg::CAP];   // (t_min, t_max, packed faces | tet | pixel, alpha_t)
-  float red[Cfg::NW][32][kMomHalf + 1];  // per-warp transpose (odd row stride)
+  float red[Cfg::NW][32][kRedCols];  // per-warp face sums and transpose (odd row stride)
   uint32_t toff[kBatch + 1];   // tet-major item offsets
   uint32_t pmask[TS * TS];
-  short2 span[kBatch][TS];
+  uint8_t span[kBatch][TS];  // per (tet, row): the row's pixel span, packed as pack_span
   // per (tet, row): item index of the row's column 0 -- relative to the tet's
   // first item after the prefixes, to the sub-batch's first item after fill
   int16_t rowoff[kBatch][TS];
@@ -446,7 +449,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
           const float yhi = fmaxf(fmaxf(vpy[0], vpy[1]), fmaxf(vpy[2], vpy[3]));
           const bool reach = vertex_rows ? (yhi >= fs(yc, 0.5f) && ylo < fa(yc, 0.5f)) : (ylo <= yc && yhi > yc);
           if (!reach) {
-            s.span[k][row] = sp;
+            s.span[k][row] = pack_span(sp);
             continue;
           }
           const int ei[6] = {0, 0, 0, 1, 1, 2};
@@ -477,7 +480,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
           }
           sp = span_of(xl, xr);
         }
-        s.span[k][row] = sp;
+        s.span[k][row] = pack_span(sp);
       }
     };
     // the adjoint's spans of a cached batch, already copied into span_pf (the
@@ -487,7 +490,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
       for (int i = tid; i < TS * TS; i += NT) s.pmask[i] = 0u;
       for (int task = tid; task < nb * TS; task += NT) {
         const int k = task / TS, row = task - (task / TS) * TS;
-        s.span[k][row] = unpack_span(s.span_pf[k][row]);
+        s.span[k][row] = s.span_pf[k][row];
       }
     };
     // per-tet row prefix sums over the tet's reachable rows and tet-major item
@@ -499,7 +502,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
           const int k = lane;
           uint32_t acc = 0;
           for (int r = rr_lo; r < rr_lo + rr_n; ++r) {
-            const short2 sp = s.span[k][r];
+            const short2 sp = unpack_span(s.span[k][r]);
             s.rowoff[k][r] = (int16_t)((int)acc - (int)sp.x);
             acc += (uint32_t)max(sp.y - sp.x + 1, 0);
           }
@@ -529,7 +532,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
         const int k = task_tet(t);
         const int row = task_row(t, k);
         if (t >= te) continue;
-        const short2 sp = s.span[k][row];
+        const short2 sp = unpack_span(s.span[k][row]);
         if (sp.x > sp.y) continue;
         // rebase the row's offset onto the sub-batch (read by item_of)
         const int ro = (int)s.rowoff[k][row] + (int)(s.toff[k] - base0);
@@ -810,7 +813,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
             __syncthreads();
             // phase 2: per-tet sums of the item statistics (12 columns; column 11
             // is a maximum), a segment of rows per lane as in the adjoint
-            float(*red)[kMomHalf + 1] = s.red[warp];
+            float(*red)[kRedCols] = s.red[warp];
             for (uint32_t chunk = (uint32_t)warp * 32u; chunk < n_items; chunk += (uint32_t)NT) {
               const uint32_t i = chunk + (uint32_t)lane;
               float m[kMomHalf];
@@ -1049,16 +1052,19 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
             // Each tet's items are cut into runs of at most R consecutive items
             // (its pixels along its rows), R chosen so that the sub-batch has at
             // most one run per thread; thread t takes run t and sums its items'
-            // moments in registers (the 8 tet moments and (S, P) of each of the
-            // 4 faces).  The runs' sums (lanes in run order, so a tet's lanes are
-            // adjacent) are then combined per warp by a transpose through shared
-            // memory, half of the moments at a time: lane (h, q) with q < kMomHalf
-            // walks column q over rows [16h, 16h + 16) and adds a partial sum to
-            // the tet's moment at every tet boundary and at the end of its rows.
+            // moments: the 8 tet moments in registers, the (S, P) of the 4 faces
+            // in the lane's row of the warp buffer (an item adds to the rows of
+            // its entry and exit faces by address, where registers would need a
+            // select over all 16 sums per side).  The runs' sums (lanes in run
+            // order, so a tet's lanes are adjacent) are then combined per warp
+            // through that buffer, half of the moments at a time: lane (h, q)
+            // with q < kMomHalf walks one column over rows [16h, 16h + 16) and adds
+            // a partial sum to the tet's moment at every tet boundary and at the
+            // end of its rows.
             {
               const int nsub = k1 - k0;
               const uint32_t R = max(1u, (n_items + (uint32_t)(NT - nsub) - 1u) / (uint32_t)(NT - nsub));
-              float(*red)[kMomHalf + 1] = s.red[warp];
+              float(*red)[kRedCols] = s.red[warp];
               // cumulative run counts of the sub-batch's tets (each warp its own copy)
               int* crun = reinterpret_cast<int*>(&red[0][0]);
               {
@@ -1086,10 +1092,13 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
                 i0 = s.toff[k] - base + (uint32_t)(tid - crun[lo]) * R;
                 i1 = min(i0 + R, s.toff[k + 1] - base);
               }
-              __syncwarp();  // crun is overwritten by the transpose below
-              float acc[8], fac[16];
+              __syncwarp();  // crun is overwritten by the face sums below
+              float acc[8];
 #pragma unroll
               for (int q = 0; q < 8; ++q) acc[q] = 0.0f;
+              // this lane's face sums live in its row of the warp buffer, so the
+              // item's entry / exit face is an address, not a 16-way select
+              float* fac = red[lane];
 #pragma unroll
               for (int q = 0; q < 16; ++q) fac[q] = 0.0f;
               for (uint32_t i = i0; i < i1; ++i) {
@@ -1172,39 +1181,41 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
                   const float inv_den = fabsf(den) < kTiny ? clipf(1.0f / kTiny, kMinVal, kMaxVal)
                                                            : clipf(__fdividef(1.0f, den), kMinVal, kMaxVal);
                   const float sv = dt * inv_den, st_ = sv * tt;
-#pragma unroll
-                  for (int ff = 0; ff < 4; ++ff) {
-                    if (f == ff) {
-                      fac[4 * ff] += sv;
-                      fac[4 * ff + 1] += st_ * d.x;
-                      fac[4 * ff + 2] += st_ * d.y;
-                      fac[4 * ff + 3] += st_ * d.z;
-                    }
-                  }
+                  float* fp = fac + 4 * f;
+                  fp[0] += sv;
+                  fp[1] += st_ * d.x;
+                  fp[2] += st_ * d.y;
+                  fp[3] += st_ * d.z;
                 }
               }
               // warp combine of the runs' sums (lanes without a run come last)
               const int kp = __shfl_up_sync(0xffffffffu, k, 1);
               const unsigned heads = __ballot_sync(0xffffffffu, k >= 0 && (lane == 0 || kp != k));
               const int n_rows = __popc(__ballot_sync(0xffffffffu, k >= 0));
+              red[lane][16] = __int_as_float(k);
+              __syncwarp();
               if (n_rows > 0) {
                 const int wq = lane & 15, wr0 = (lane >> 4) * 16;
                 const int wr1 = min(wr0 + 16, n_rows);
 #pragma unroll
                 for (int hm = 0; hm < 2; ++hm) {
-                  // row layout: half 0 = the 8 tet moments + face 0's (S, P); half 1 = faces 1..3
+                  // pass 0: faces 1..3 (moments 12..23) from columns 4..15; pass 1: the
+                  // 8 tet moments, written over columns 4..11, and face 0 (moments
+                  // 8..11) from columns 0..3
+                  if (hm == 1) {
 #pragma unroll
-                  for (int q = 0; q < kMomHalf; ++q) red[lane][q] = hm == 0 ? (q < 8 ? acc[q] : fac[q - 8]) : fac[4 + q];
-                  red[lane][kMomHalf] = __int_as_float(k);
-                  __syncwarp();
+                    for (int q = 0; q < 8; ++q) red[lane][4 + q] = acc[q];
+                    __syncwarp();
+                  }
                   if (wq < kMomHalf && wr0 < wr1) {
-                    const int col = hm * kMomHalf + wq;
+                    const int col = hm == 0 ? kMomHalf + wq : wq;
+                    const int src = hm == 0 ? 4 + wq : (wq < 8 ? 4 + wq : wq - 8);
                     for (int r0 = wr0; r0 < wr1;) {  // one tet segment [r0, r1) at a time
                       const unsigned later = heads & ~((2u << r0) - 1u);
                       const int r1 = later ? min(__ffs(later) - 1, wr1) : wr1;
                       float sum = 0.0f;
-                      for (int row = r0; row < r1; ++row) sum += red[row][wq];
-                      if (sum != 0.0f) atomicAdd(&s.mom[__float_as_int(red[r0][kMomHalf])][col], sum);
+                      for (int row = r0; row < r1; ++row) sum += red[row][src];
+                      if (sum != 0.0f) atomicAdd(&s.mom[__float_as_int(red[r0][16])][col], sum);
                       r0 = r1;
                     }
                   }
