@@ -120,7 +120,7 @@ struct RmeshCtx {
   DevBuf vis_color, vis_dcolor;  // SH colours per entry and their gradients
   DevBuf pair_key, pair_val, pair_key_alt, pair_val_alt, ranges;
   DevBuf rgba, aux, dl, gt, out_a, out_b, out_c, out_d;
-  DevBuf span_cache;  // per-CTA adjoint span cache of persistent train launches
+  DevBuf spans_fwd, spans_adj;  // per sorted pair: pixel spans of its tile rows (forward / adjoint rule)
   DevBuf tile_order, order_hist;  // longest-first tile order of the run; bucket counts and cursors
   DevBuf tickets;                 // persistent tile-queue heads, one per launch of a run
   DevBuf err_in, err_out;  // per-pixel error inputs, per-tet error statistics
@@ -351,7 +351,6 @@ struct ViewPlan {
   std::vector<TileGroup> groups;
   uint64_t total_pix = 0;
   uint32_t total_tiles = 0, max_tiles = 0;
-  int cache_units = 0;           // max over groups of resident CTAs per SM (span-cache slots per SM)
 };
 
 // ---------------------------------------------------------------- sorting
@@ -406,11 +405,7 @@ int setup_sort_attrs() {
 }
 
 // ---------------------------------------------------------------- buffers
-// Adjoint span cache: tile-list entries per CTA slot, and slots for a
-// persistent grid (resident CTAs per SM the kernel is built for x SMs; a
-// larger grid runs without the cache)
-constexpr uint32_t kSpanCacheTets = 2048;
-int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t total_tiles, int cache_units) {
+int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t total_tiles) {
   const uint64_t items = (uint64_t)n_views * (uint64_t)c->M;
   CKR(ensure_buf(c, c->vis_key, items * 8));
   CKR(ensure_buf(c, c->vis_key_alt, items * 8));
@@ -420,8 +415,6 @@ int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t
   CKR(ensure_buf(c, c->group_off, ((items + 255) / 256 + 1) * 8));
   CKR(ensure_buf(c, c->vis_proj, items * 32));
   CKR(ensure_buf(c, c->vis_view, items * sizeof(TetView)));
-  // span-cache slots: resident CTAs per SM of the run's largest configuration
-  CKR(ensure_buf(c, c->span_cache, (uint64_t)cache_units * c->num_sms * kSpanCacheTets * kSpanRows));
   if (c->sh_degree >= 0) {
     CKR(ensure_buf(c, c->vis_color, items * 16));
     CKR(ensure_buf(c, c->vis_dcolor, items * 16));
@@ -431,6 +424,8 @@ int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t
   CKR(ensure_buf(c, c->pair_val, c->cap_pairs * 4));
   CKR(ensure_buf(c, c->pair_key_alt, c->cap_pairs * 4));
   CKR(ensure_buf(c, c->pair_val_alt, c->cap_pairs * 4));
+  CKR(ensure_buf(c, c->spans_fwd, c->cap_pairs * kSpanRows));
+  CKR(ensure_buf(c, c->spans_adj, c->cap_pairs * kSpanRows));
   const uint64_t sort_items = std::max<uint64_t>(std::max<uint64_t>(items, c->cap_pairs), 4ull * c->M);
   CKR(ensure_buf(c, c->sort_status, ((sort_items + kSortPart - 1) / kSortPart + 1) * 256 * 8));
   CKR(ensure_buf(c, c->scan_status, ((items + 255) / 256 + 2) * 8));
@@ -510,7 +505,6 @@ int make_plan(RmeshCtx* c, const RmeshCamera* cams, int n_views, bool plain, Vie
     }
     g.n_tiles = pl.total_tiles - g.tile_lo;
     pl.groups.push_back(g);
-    pl.cache_units = std::max(pl.cache_units, conf_minb(tc));
   }
   return RMESH_OK;
 }
@@ -620,6 +614,19 @@ int run_bin(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t tota
     ranges_kernel<<<std::max(1, blocks), 256, 0, c->stream>>>(c->sorted_pair_key, &cnt->n_pairs, c->cap_pairs,
                                                                c->ranges.as<uint2>(), views_dev, n_views, cnt);
     CKL();
+    PairSpanArgs sa;
+    sa.views = views_dev;
+    sa.n_views = n_views;
+    sa.keys = c->sorted_pair_key;
+    sa.vals = c->sorted_pair_val;
+    sa.n_ptr = &cnt->n_pairs;
+    sa.cap = c->cap_pairs;
+    sa.vis_view = c->vis_view.as<TetView>();
+    sa.spans_fwd = c->spans_fwd.as<uint8_t>();
+    sa.spans_adj = c->spans_adj.as<uint8_t>();
+    const int sblocks = (int)std::min<uint64_t>((c->cap_pairs + 255) / 256, (uint64_t)c->num_sms * 8);
+    pair_spans_kernel<<<std::max(1, sblocks), 256, 0, c->stream>>>(sa);
+    CKL();
     // longest-first order of each launch's tiles for the persistent tile
     // kernel (indices relative to the launch's first tile)
     CK(cudaMemsetAsync(c->order_hist.p, 0, 2 * kOrderBuckets * 4 * groups.size(), c->stream));
@@ -660,11 +667,6 @@ int launch_tile_t(RmeshCtx* c, TileArgs& ta, uint32_t n_tiles, bool persistent) 
     grid = std::min<unsigned>(grid, std::max<uint32_t>(n_tiles, 1));
   }
   ta.persistent = persistent ? 1 : 0;
-  if (MODE == kModeTrain && persistent && c->span_cache.p &&
-      (uint64_t)grid * kSpanCacheTets * kSpanRows <= c->span_cache.bytes) {
-    ta.span_cache = c->span_cache.as<uint8_t>();
-    ta.span_cache_tets = kSpanCacheTets;
-  }
   if (grid == 0) return RMESH_OK;
   tile_kernel<TS, MODE, AUX, WIDE><<<grid, NT, smem, c->stream>>>(ta);
   CKL();
@@ -721,6 +723,8 @@ TileArgs base_tile_args(RmeshCtx* c, const ViewParams* views_dev, int n_views, u
   }
   ta.counters = cnt;
   ta.hp = c->hp_d.as<AdamParams>();
+  ta.spans_fwd = c->spans_fwd.as<uint8_t>();
+  ta.spans_adj = c->spans_adj.as<uint8_t>();
   ta.tile_order = c->tile_order.as<uint32_t>();
   ta.tile_lo = 0;
   ta.ticket = c->tickets.as<uint32_t>();
@@ -849,7 +853,7 @@ int train_views(RmeshCtx* c, const RmeshCamera* cams, int n_views, const float* 
   const int run_views = plain ? 1 : n_views;
   const bool direct_gt = is_device_ptr(gt);
   for (int attempt = 0; attempt < 4; ++attempt) {
-    CKR(ensure_run_buffers(c, run_views, total_pix, plain ? max_tiles : total_tiles, pl.cache_units));
+    CKR(ensure_run_buffers(c, run_views, total_pix, plain ? max_tiles : total_tiles));
     if (!direct_gt) CKR(ensure_buf(c, c->gt, total_pix * 12));
     AdamParams& hp = *c->hp_h;
     hp.step = c->step + 1;
@@ -1315,7 +1319,7 @@ int rmesh_get_info(RmeshCtx* c, RmeshInfo* info) {
                    &c->pair_val, &c->pair_key_alt, &c->pair_val_alt, &c->ranges, &c->rgba, &c->aux, &c->dl,
                    &c->gt, &c->out_a, &c->out_b, &c->out_c, &c->out_d, &c->sh, &c->m_sh, &c->v_sh,
                    &c->vis_color, &c->vis_dcolor, &c->err_in, &c->err_out, &c->aux_data, &c->dl_aux, &c->d_aux,
-                   &c->span_cache, &c->tile_order, &c->order_hist, &c->tickets};
+                   &c->spans_fwd, &c->spans_adj, &c->tile_order, &c->order_hist, &c->tickets};
   for (DevBuf* b : all) info->device_bytes += b->bytes;
   return RMESH_OK;
 }
@@ -1379,7 +1383,7 @@ int rmesh_forward_views(RmeshCtx* c, const RmeshCamera* cams, int32_t n_views, f
   const uint32_t total_tiles = pl.total_tiles;
   const uint64_t aux_floats = total_pix * (8 + (uint64_t)c->aux_dim);
   for (int attempt = 0; attempt < 4; ++attempt) {
-    CKR(ensure_run_buffers(c, n_views, total_pix, total_tiles, pl.cache_units));
+    CKR(ensure_run_buffers(c, n_views, total_pix, total_tiles));
     if (aux_out) CKR(ensure_buf(c, c->aux, aux_floats * 4));
     CKR(upload_views(c, n_views));
     Counters* cnt = c->counters_d.as<Counters>();
@@ -1422,7 +1426,7 @@ int rmesh_forward_tiled(RmeshCtx* c, const RmeshCamera* cam, float* rgba_out, fl
     CKR(fill_view(c, *cam, c->views_h[0], 0, 0, tc));
     const uint32_t tiles = (uint32_t)(c->views_h[0].tiles_x * c->views_h[0].tiles_y);
     const std::vector<TileGroup> one{TileGroup{tc, 0u, tiles}};
-    CKR(ensure_run_buffers(c, 1, npix, tiles, conf_minb(tc)));
+    CKR(ensure_run_buffers(c, 1, npix, tiles));
     if (aux_out) CKR(ensure_buf(c, c->aux, npix * (8 + (uint64_t)c->aux_dim) * 4));
     CKR(upload_views(c, 1));
     Counters* cnt = c->counters_d.as<Counters>();

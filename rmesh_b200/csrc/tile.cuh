@@ -100,11 +100,11 @@ struct TileArgs {
   Counters* counters;
   const AdamParams* hp;
   int persistent;
-  // train mode, persistent launches: per-CTA cache of the adjoint's pixel
-  // spans (span_cache_tets entries of kSpanRows one-byte rows per CTA, see
-  // pack_span), written by the forward pass of the same tile; nullptr disables it
-  uint8_t* span_cache;
-  uint32_t span_cache_tets;
+  // per sorted pair position: the pair's pixel spans of the tile's rows under
+  // the forward's rule and under the adjoint's (kSpanRows one-byte rows each,
+  // see pack_span), from pair_spans_kernel
+  const uint8_t* spans_fwd;
+  const uint8_t* spans_adj;
   // persistent launches: ticket -> tile (longest lists first); nullptr = identity
   const uint32_t* tile_order;
   // the launch covers global tiles [tile_lo, tile_lo + n_tiles) (the views of
@@ -232,6 +232,61 @@ __device__ __forceinline__ void integrate(const float4& cb, float dcdt, float t_
   I.w1 = 1.0f - I.ph;
 }
 
+// Pixel spans of tile row `row` of one (tile, tet) pair, packed as pack_span:
+// fwd under the forward's rule (rasterize_compute.wgsl:170-275: a row is
+// reached when an edge crosses its centre line or a vertex lies in the row),
+// adj under the adjoint's (backward_tiled_compute.wgsl:241-299: edge crossings
+// only).  vpx, vpy: the vertex projections minus the tile origin; columns past
+// valid_cols (outside the image) are dropped, as the reference skips their
+// pixels (rasterize_compute.wgsl:332).  The projections use fast arithmetic,
+// and spans include pixels up to 0.001 px outside the silhouette, where the
+// exact ray test misses anyway, so a last-bit difference in a span end changes
+// no pixel value.
+__device__ __forceinline__ short2 span_of_cols(float xl, float xr, int valid_cols) {
+  short2 sp = make_short2(0, -1);
+  if (xl <= xr) {
+    // directed-rounding conversions: ceil / floor and the conversion in one step
+    const int32_t lo = max(__float2int_ru(xl - 0.5f - 0.001f), 0);
+    const int32_t hi = min(__float2int_rd(xr - 0.5f + 0.001f), valid_cols - 1);
+    if (lo <= hi) sp = make_short2((short)lo, (short)hi);
+  }
+  return sp;
+}
+__device__ __forceinline__ void row_spans(const float vpx[4], const float vpy[4], int row, int valid_cols, uint8_t& fwd,
+                                          uint8_t& adj) {
+  fwd = 0xF0u;
+  adj = 0xF0u;
+  const float yc = fa((float)row, 0.5f);
+  const float ylo = fminf(fminf(vpy[0], vpy[1]), fminf(vpy[2], vpy[3]));
+  const float yhi = fmaxf(fmaxf(vpy[0], vpy[1]), fmaxf(vpy[2], vpy[3]));
+  // the adjoint's reach (some edge crosses yc) implies the forward's
+  if (!(yhi >= fs(yc, 0.5f) && ylo < fa(yc, 0.5f))) return;
+  float xl = 1e10f, xr = -1e10f;
+  const int ei[6] = {0, 0, 0, 1, 1, 2};
+  const int ej[6] = {1, 2, 3, 2, 3, 3};
+#pragma unroll
+  for (int e = 0; e < 6; ++e) {
+    const float yi = vpy[ei[e]], yj = vpy[ej[e]];
+    if ((yi <= yc && yj > yc) || (yj <= yc && yi > yc)) {
+      const float t = __fdividef(yc - yi, yj - yi);
+      const float x = vpx[ei[e]] + t * (vpx[ej[e]] - vpx[ei[e]]);
+      xl = fminf(xl, x);
+      xr = fmaxf(xr, x);
+    }
+  }
+  adj = pack_span(span_of_cols(xl, xr, valid_cols));  // empty when no edge crosses yc
+  const float blo = fs(yc, 0.5f), bhi = fa(yc, 0.5f);
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const float vyq = vpy[q];
+    if (vyq >= blo && vyq < bhi) {
+      xl = fminf(xl, vpx[q]);
+      xr = fmaxf(xr, vpx[q]);
+    }
+  }
+  fwd = pack_span(span_of_cols(xl, xr, valid_cols));
+}
+
 // itemx.z packs the adjoint's exit/entry faces, the tet's batch slot and the pixel
 __device__ __forceinline__ uint32_t pack_item(int fmin, int fmax, int k, int p) {
   return (uint32_t)fmin | ((uint32_t)fmax << 3) | ((uint32_t)k << 5) | ((uint32_t)p << 10);
@@ -261,10 +316,6 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
   uint32_t phase_bits = 0u;  // parity of the next phase of bar[0] (bit 0) and bar[1] (bit 1)
   bool failed = false;
 
-  // this CTA's span cache slot (persistent train launches only)
-  uint8_t* const scache = (MODE == kModeTrain && a.span_cache)
-                              ? a.span_cache + (size_t)blockIdx.x * a.span_cache_tets * kSpanRows
-                              : nullptr;
   const uint32_t first_tile = blockIdx.x;
   while (true) {
     if (tid == 0) {
@@ -292,7 +343,6 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
     const uint2 range = a.ranges[g];
     const uint32_t rs = range.x, re = range.y;
     // pixels of this tile inside the image
-    const int valid_cols = min(TS, V.W - (int)(tile_x * TS));
     const int valid_rows = min(TS, V.H - (int)(tile_y * TS));
 
     // pixel ray (rasterize_compute.wgsl:343-349), explicitly rounded: the ray and
@@ -325,8 +375,8 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
       if (warp != 0 || lane >= nb) return 0u;
       return a.pair_val[dir < 0 ? first - (uint32_t)lane : first + (uint32_t)lane];
     };
-    // span_src (adjoint): the batch's cached spans, copied into span_pf on the
-    // same barrier
+    // span_src: the batch's pixel spans (kSpanRows bytes per list position,
+    // ascending), copied into span_pf on the same barrier
     auto issue = [&](int buf, int nb, uint32_t idx, const uint8_t* span_src) {
       if (warp == 0) {
         if (lane == 0) {
@@ -348,25 +398,6 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
         failed = true;
         if (tid == 0) atomicOr(&a.counters->err, kErrSpinTimeout);
       }
-    };
-    // per-(tet,row) pixel spans -> span table.  vertex_rows selects the forward
-    // rule (rasterize_compute.wgsl:170-275); without it this is the adjoint rule
-    // (backward_tiled_compute.wgsl:241-299).
-    // Rows/columns outside the image are dropped (their pixels are skipped by
-    // the reference too, rasterize_compute.wgsl:332).
-    // The tile-local vertex projections use fast arithmetic (the record's
-    // px/py, minus the tile origin): spans include pixels up to 0.001 px
-    // outside the silhouette, where the exact ray test misses anyway, so a
-    // last-bit difference in a span end changes no pixel value.
-    // span of pixel columns [xl, xr] of one row (empty when xl > xr)
-    auto span_of = [&](float xl, float xr) -> short2 {
-      short2 sp = make_short2(0, -1);
-      if (xl <= xr) {
-        const int32_t lo = max(__float2int_rz(ceilf(xl - 0.5f - 0.001f)), 0);
-        const int32_t hi = min(min(__float2int_rz(floorf(xr - 0.5f + 0.001f)), TS - 1), valid_cols - 1);
-        if (lo <= hi) sp = make_short2((short)lo, (short)hi);
-      }
-      return sp;
     };
     // Row table of the batch, kept in registers by every warp: lane l < nb holds
     // tet l's first row and row count under the forward's reach rule (a row is
@@ -417,80 +448,15 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
     };
     // row of task t of tet k (all lanes call)
     auto task_row = [&](int t, int k) -> int { return __shfl_sync(0xffffffffu, rr_lo - (rr_pre - rr_n), k) + t; };
-    // cache: the forward (vertex_rows) also stores each task's adjoint span
-    // (edge crossings only) at its list position first + dir * k
-    auto spans = [&](int buf, int nb, bool vertex_rows, uint8_t* cache, uint32_t first, int dir) {
-      row_ranges(buf, nb);
-      for (int i = tid; i < TS * TS; i += NT) s.pmask[i] = 0u;
-      for (int t0 = warp * 32; t0 < rr_total; t0 += NT) {  // warp-uniform trip count
-        const int t = t0 + lane;
-        const int k = task_tet(t);
-        const int row = task_row(t, k);
-        if (t >= rr_total) continue;
-        short2 sp = make_short2(0, -1);
-        uint8_t* slot = nullptr;
-        if (cache) {
-          const uint32_t rel = first + (uint32_t)(dir * k) - rs;
-          if (rel < a.span_cache_tets) {
-            slot = cache + (size_t)rel * kSpanRows + row;
-            *slot = pack_span(sp);  // overwritten below when the row has crossings
-          }
-        }
-        const TetView& tv = s.view[buf][k];
-        {
-          const float4 gx4 = tv.px, gy4 = tv.py;
-          const float vpx[4] = {gx4.x - tile_ox, gx4.y - tile_ox, gx4.z - tile_ox, gx4.w - tile_ox};
-          const float vpy[4] = {gy4.x - tile_oy, gy4.y - tile_oy, gy4.z - tile_oy, gy4.w - tile_oy};
-          float xl = 1e10f, xr = -1e10f;
-          const float yc = fa((float)row, 0.5f);
-          // rows the tet cannot reach: no edge crosses yc (and, for the forward,
-          // no vertex lies in [yc - 0.5, yc + 0.5)), so the span stays empty
-          const float ylo = fminf(fminf(vpy[0], vpy[1]), fminf(vpy[2], vpy[3]));
-          const float yhi = fmaxf(fmaxf(vpy[0], vpy[1]), fmaxf(vpy[2], vpy[3]));
-          const bool reach = vertex_rows ? (yhi >= fs(yc, 0.5f) && ylo < fa(yc, 0.5f)) : (ylo <= yc && yhi > yc);
-          if (!reach) {
-            s.span[k][row] = pack_span(sp);
-            continue;
-          }
-          const int ei[6] = {0, 0, 0, 1, 1, 2};
-          const int ej[6] = {1, 2, 3, 2, 3, 3};
-#pragma unroll
-          for (int e = 0; e < 6; ++e) {
-            const float yi = vpy[ei[e]], yj = vpy[ej[e]];
-            if ((yi <= yc && yj > yc) || (yj <= yc && yi > yc)) {
-              const float t = __fdividef(yc - yi, yj - yi);
-              const float x = vpx[ei[e]] + t * (vpx[ej[e]] - vpx[ei[e]]);
-              xl = fminf(xl, x);
-              xr = fmaxf(xr, x);
-            }
-          }
-          // the adjoint's span of this row: the same edge crossings, no
-          // vertex rows (empty when no edge crosses yc)
-          if (slot) *slot = pack_span(span_of(xl, xr));
-          if (vertex_rows) {
-            const float blo = fs(yc, 0.5f), bhi = fa(yc, 0.5f);
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-              const float vyq = vpy[q];
-              if (vyq >= blo && vyq < bhi) {
-                xl = fminf(xl, vpx[q]);
-                xr = fmaxf(xr, vpx[q]);
-              }
-            }
-          }
-          sp = span_of(xl, xr);
-        }
-        s.span[k][row] = pack_span(sp);
-      }
-    };
-    // the adjoint's spans of a cached batch, already copied into span_pf (the
-    // forward wrote every row of the table above for each cached tet)
-    auto cached_spans = [&](int buf, int nb) {
+    // the batch's spans, already copied into span_pf by the batch's bulk copy
+    // (pair_spans_kernel wrote them per list position): tet k is list position
+    // k of the copy, or nb - 1 - k when the batch runs front to back (rev)
+    auto load_spans = [&](int buf, int nb, bool rev) {
       row_ranges(buf, nb);
       for (int i = tid; i < TS * TS; i += NT) s.pmask[i] = 0u;
       for (int task = tid; task < nb * TS; task += NT) {
         const int k = task / TS, row = task - (task / TS) * TS;
-        s.span[k][row] = s.span_pf[k][row];
+        s.span[k][row] = s.span_pf[rev ? nb - 1 - k : k][row];
       }
     };
     // per-tet row prefix sums over the tet's reachable rows and tet-major item
@@ -622,7 +588,6 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
     };
 
     float Cr = 0.f, Cg = 0.f, Cb = 0.f, logT = 0.f;
-    uint32_t span_lo = re;  // the forward cached the adjoint spans of list positions [span_lo, re)
     float nd0 = 0.f, nd1 = 0.f, nd2 = 0.f, nd3 = 0.f, en0 = 0.f, en1 = 0.f, en2 = 0.f, en3 = 0.f;
 
     // =============== forward (front to back) ===============
@@ -638,7 +603,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
       if (re > rs) {
         {
           const int nb0 = (int)min((uint32_t)kBatch, re - rs);
-          issue(0, nb0, load_idx(re - 1u, nb0, -1), nullptr);
+          issue(0, nb0, load_idx(re - 1u, nb0, -1), a.spans_fwd + (size_t)(re - (uint32_t)nb0) * kSpanRows);
         }
         uint32_t idx_next = 0u;  // record indices of the batch after the current one
         if (re - rs > (uint32_t)kBatch) {
@@ -652,15 +617,15 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
           const uint32_t next_hi = hi - (uint32_t)nb;
           wait_buf(buf);
           if (failed) break;
+          load_spans(buf, nb, true);
+          __syncthreads();
+          // the next batch's copies, after span_pf has been read
           if (next_hi > rs) {
             const int nbn = (int)min((uint32_t)kBatch, next_hi - rs);
-            issue(buf ^ 1, nbn, idx_next, nullptr);
+            issue(buf ^ 1, nbn, idx_next, a.spans_fwd + (size_t)(next_hi - (uint32_t)nbn) * kSpanRows);
             const uint32_t h2 = next_hi - (uint32_t)nbn;
             if (h2 > rs) idx_next = load_idx(h2 - 1u, (int)min((uint32_t)kBatch, h2 - rs), -1);
           }
-          spans(buf, nb, true, scache, hi - 1u, -1);
-          span_lo = next_hi;  // the adjoint spans of [next_hi, hi) are cached
-          __syncthreads();
           prefixes(nb);
           __syncthreads();
           int k1 = sub_end(0, nb);
@@ -761,7 +726,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
       if (re > rs) {
         {
           const int nb0 = (int)min((uint32_t)kBatch, re - rs);
-          issue(0, nb0, load_idx(re - 1u, nb0, -1), nullptr);
+          issue(0, nb0, load_idx(re - 1u, nb0, -1), a.spans_fwd + (size_t)(re - (uint32_t)nb0) * kSpanRows);
         }
         uint32_t idx_next = 0u;
         if (re - rs > (uint32_t)kBatch) {
@@ -775,14 +740,14 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
           const uint32_t next_hi = hi - (uint32_t)nb;
           wait_buf(buf);
           if (failed) break;
+          load_spans(buf, nb, true);
+          __syncthreads();
           if (next_hi > rs) {
             const int nbn = (int)min((uint32_t)kBatch, next_hi - rs);
-            issue(buf ^ 1, nbn, idx_next, nullptr);
+            issue(buf ^ 1, nbn, idx_next, a.spans_fwd + (size_t)(next_hi - (uint32_t)nbn) * kSpanRows);
             const uint32_t h2 = next_hi - (uint32_t)nbn;
             if (h2 > rs) idx_next = load_idx(h2 - 1u, (int)min((uint32_t)kBatch, h2 - rs), -1);
           }
-          spans(buf, nb, true, nullptr, 0u, 0);
-          __syncthreads();
           prefixes(nb);
           __syncthreads();
           int k1 = sub_end(0, nb);
@@ -947,21 +912,11 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
         dlr = dl.x; dlg = dl.y; dlb = dl.z;
       }
       if (in_tile) s.pdl[pl] = make_float4(dlr, dlg, dlb, 0.0f);
-      // a batch [lo, lo + nb) takes its spans from the forward's cache when
-      // the forward covered all of it
-      auto span_cached = [&](uint32_t lo, int nb) -> bool {
-        return scache && lo >= span_lo && lo + (uint32_t)nb - rs <= a.span_cache_tets;
-      };
-      auto span_src = [&](uint32_t lo, int nb) -> const uint8_t* {
-        return span_cached(lo, nb) ? scache + (size_t)(lo - rs) * kSpanRows : nullptr;
-      };
       if (re > rs) {
-        // the forward's span-cache writes, before the bulk copies that read them
-        if (scache) fence_proxy_async_global();
-        __syncthreads();
+        __syncthreads();  // the forward's last reads of the copy buffers
         {
           const int nb0 = (int)min((uint32_t)kBatch, re - rs);
-          issue(0, nb0, load_idx(rs, nb0, +1), span_src(rs, nb0));
+          issue(0, nb0, load_idx(rs, nb0, +1), a.spans_adj + (size_t)rs * kSpanRows);
         }
         uint32_t idx_next = 0u;
         if (re - rs > (uint32_t)kBatch) {
@@ -982,17 +937,13 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
             asm volatile("prefetch.global.L1 [%0];" ::"l"(rp));
             asm volatile("prefetch.global.L1 [%0];" ::"l"(reinterpret_cast<const char*>(rp) + 32));
           }
-          // adjoint: edge crossings only, from the forward's cache when it
-          // covered the whole batch
-          if (span_cached(lo, nb))
-            cached_spans(buf, nb);
-          else
-            spans(buf, nb, false, nullptr, 0u, 0);
+          // adjoint: edge crossings only (backward_tiled_compute.wgsl:241-299)
+          load_spans(buf, nb, false);
           __syncthreads();
           // the next batch's copies, after span_pf has been read
           if (next_lo < re) {
             const int nbn = (int)min((uint32_t)kBatch, re - next_lo);
-            issue(buf ^ 1, nbn, idx_next, span_src(next_lo, nbn));
+            issue(buf ^ 1, nbn, idx_next, a.spans_adj + (size_t)next_lo * kSpanRows);
             const uint32_t l2 = next_lo + (uint32_t)nbn;
             if (l2 < re) idx_next = load_idx(l2, (int)min((uint32_t)kBatch, re - l2), +1);
           }
@@ -1324,6 +1275,106 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
     }
     if (!a.persistent) break;
     __syncthreads();
+  }
+}
+
+// Pixel spans of every sorted (tile, tet) pair, kSpanRows one-byte rows per
+// pair and rule (row_spans), over the rows its tet reaches (the row table rule
+// of the tile kernel): the tile kernel bulk-copies a batch's rows with its tet
+// records instead of deriving them between block barriers.  Other rows, tets
+// with a vertex behind the camera and sentinel slots get empty spans (the tile
+// kernel reads none of them).  Each warp takes 32 consecutive pairs; lane l
+// sets up pair l, and the warp's (pair, row) tasks are spread over its lanes
+// through a prefix of the row counts, so lanes stay busy whatever the rows per
+// tet.  The rows go to shared memory and each pair's two 16-byte records are
+// stored whole.
+struct PairSpanArgs {
+  const ViewParams* views;
+  int n_views;
+  const uint32_t* keys;              // sorted global tile ids
+  const uint32_t* vals;              // the pairs' entry indices (per-view tet records)
+  const unsigned long long* n_ptr;   // pair count
+  unsigned long long cap;
+  const TetView* vis_view;
+  uint8_t* spans_fwd;
+  uint8_t* spans_adj;
+};
+
+__global__ void __launch_bounds__(256) pair_spans_kernel(PairSpanArgs a) {
+  static_assert(kSpanRows == 16, "one 16-byte row record per pair and rule");
+  __shared__ __align__(16) uint8_t s_fwd[256][kSpanRows];
+  __shared__ __align__(16) uint8_t s_adj[256][kSpanRows];
+  const int lane = threadIdx.x & 31, wbase = threadIdx.x & ~31;
+  const unsigned long long n = *a.n_ptr < a.cap ? *a.n_ptr : a.cap;
+  const uint4 empty = make_uint4(0xF0F0F0F0u, 0xF0F0F0F0u, 0xF0F0F0F0u, 0xF0F0F0F0u);
+  for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < n;
+       base += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long p = base + threadIdx.x;
+    *reinterpret_cast<uint4*>(s_fwd[threadIdx.x]) = empty;
+    *reinterpret_cast<uint4*>(s_adj[threadIdx.x]) = empty;
+    float vpx[4] = {0.f, 0.f, 0.f, 0.f}, vpy[4] = {0.f, 0.f, 0.f, 0.f};
+    int valid_cols = 0, r0 = 0, nrows = 0;
+    if (p < n) {
+      const uint32_t key = a.keys[p];
+      if (key != kSentinel) {
+        const ViewParams& V = a.views[view_of_tile(a.views, a.n_views, key)];
+        const int TS = V.TS;
+        const uint32_t local = key - V.tile_base;
+        const uint32_t ty = local / (uint32_t)V.tiles_x, tx = local - ty * (uint32_t)V.tiles_x;
+        valid_cols = min(TS, V.W - (int)(tx * (uint32_t)TS));
+        const int valid_rows = min(TS, V.H - (int)(ty * (uint32_t)TS));
+        const TetView* tv = a.vis_view + a.vals[p];
+        if (!((__float_as_uint(__ldg(&tv->gm.w)) >> 4) & 1u)) {
+          const float4 gx4 = __ldg(&tv->px), gy4 = __ldg(&tv->py);
+          const float tile_ox = (float)(tx * (uint32_t)TS), tile_oy = (float)(ty * (uint32_t)TS);
+          vpx[0] = gx4.x - tile_ox; vpx[1] = gx4.y - tile_ox; vpx[2] = gx4.z - tile_ox; vpx[3] = gx4.w - tile_ox;
+          vpy[0] = gy4.x - tile_oy; vpy[1] = gy4.y - tile_oy; vpy[2] = gy4.z - tile_oy; vpy[3] = gy4.w - tile_oy;
+          // rows r with floor(ylo) <= r <= floor(yhi), clipped to the image: the
+          // only rows the forward's reach rule can accept
+          const float ylo = fminf(fminf(vpy[0], vpy[1]), fminf(vpy[2], vpy[3]));
+          const float yhi = fmaxf(fmaxf(vpy[0], vpy[1]), fmaxf(vpy[2], vpy[3]));
+          const float flo = fmaxf(floorf(ylo), 0.0f);
+          const float fhi = fminf(floorf(yhi), (float)(valid_rows - 1));
+          if (flo <= fhi) {
+            r0 = (int)flo;
+            nrows = (int)fhi - r0 + 1;
+          }
+        }
+      }
+    }
+    int pre = nrows;  // inclusive prefix of the row counts over the warp's lanes
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, pre, o);
+      if (lane >= o) pre += y;
+    }
+    const int total = __shfl_sync(0xffffffffu, pre, 31);
+    const int first_row = r0 - (pre - nrows);  // row of task t of this lane's pair: first_row + t
+    __syncwarp();  // the records' empty rows are set before any task writes one
+    for (int t0 = 0; t0 < total; t0 += 32) {  // warp-uniform trip count
+      const int t = t0 + lane;
+      int k = 0;  // the lane whose pair owns task t: first inclusive prefix > t
+#pragma unroll
+      for (int st = 16; st > 0; st >>= 1) {
+        const int pv = __shfl_sync(0xffffffffu, pre, k + st - 1);
+        if (pv <= t) k += st;
+      }
+      const int row = __shfl_sync(0xffffffffu, first_row, k) + t;
+      const int vc = __shfl_sync(0xffffffffu, valid_cols, k);
+      float qx[4], qy[4];
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        qx[q] = __shfl_sync(0xffffffffu, vpx[q], k);
+        qy[q] = __shfl_sync(0xffffffffu, vpy[q], k);
+      }
+      if (t < total) row_spans(qx, qy, row, vc, s_fwd[wbase + k][row], s_adj[wbase + k][row]);
+    }
+    __syncwarp();
+    if (p < n) {
+      *reinterpret_cast<uint4*>(a.spans_fwd + p * kSpanRows) = *reinterpret_cast<const uint4*>(s_fwd[threadIdx.x]);
+      *reinterpret_cast<uint4*>(a.spans_adj + p * kSpanRows) = *reinterpret_cast<const uint4*>(s_adj[threadIdx.x]);
+    }
+    __syncwarp();  // the stores' reads before the next chunk's rows are reset
   }
 }
 
