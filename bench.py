@@ -50,13 +50,13 @@ LR_SH = 2.5e-3
 # DRAM bytes (read + write) per (tile, tet) pair of the fused compositing
 # kernel, from a one-kernel ncu capture of a 4-view case of this workload's
 # mesh and resolution mix (bench.py --views 4: 8.13 M pairs,
-# dram__bytes_read.sum + dram__bytes_write.sum = 2.437 GB); the roofline's
+# dram__bytes_read.sum + dram__bytes_write.sum = 2.594 GB); the roofline's
 # "traffic" scales it to the run's pair count.
-TILE_DRAM_BYTES_PER_PAIR = 300.0
+TILE_DRAM_BYTES_PER_PAIR = 319.0
 # Warp instructions per (tile, tet) pair of the same kernel, from the same
-# capture (smsp__inst_executed.sum = 10.16 G); the issue ceiling is 148 SMs x
+# capture (smsp__inst_executed.sum = 9.404 G); the issue ceiling is 148 SMs x
 # 4 schedulers x one instruction per clock.
-TILE_WARP_INST_PER_PAIR = 1249.0
+TILE_WARP_INST_PER_PAIR = 1157.0
 
 
 def issue_roofline(n_pairs: int, launch_ms: float, sm_mhz) -> dict:

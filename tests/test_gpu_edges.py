@@ -1,7 +1,7 @@
 """Edge cases of the CUDA path vs the oracle (needs a B200): a view that sees
 nothing, a camera inside the mesh (negative depth keys, vertices behind the
 camera), a multi-view step whose tiles exceed 2^16 in total, pair-buffer
-overflow, tile lists longer than the span cache, the reference's grid mesh,
+overflow, tile lists of thousands of tets, the reference's grid mesh,
 its cross-renderer cameras, and tets large enough that a batch's covered
 pixels exceed the kernel's sub-batch capacity."""
 from __future__ import annotations
@@ -109,11 +109,12 @@ def test_pair_buffer_overflow_grows_and_retries(oracle32):
     r.close()
 
 
-def test_long_tile_lists_past_the_span_cache(c2_scene):
+def test_long_tile_lists(c2_scene):
     """65k tets seen at 48x48 (16 tiles of 12x12): each tile's list holds
-    thousands of tets, more than the 2,048 entries of the per-CTA span cache,
-    so the batched adjoint reads cached spans for the head of each list and
-    recomputes the tail; losses and parameters equal the plain path's."""
+    thousands of tets (hundreds of 32-tet batches, each with its span records
+    bulk-copied beside its tet records, the forward stopping at the
+    transmittance cut-off long before the adjoint's end of the list); losses
+    and parameters of the persistent batched path equal the plain path's."""
     from rmesh_b200.camera import orbit_cameras
 
     cams = orbit_cameras(2, seed=21, radius=(2.8, 3.2), resolutions=((48, 48),))
@@ -125,7 +126,7 @@ def test_long_tile_lists_past_the_span_cache(c2_scene):
         losses = [r.train_step_views(cams, gts, 1e-4, 1e-2, 1e-3, 1, mode=mode, lr_sh=2.5e-3) for _ in range(2)]
         out[mode] = (np.array(losses), r.get_params(), r.info().n_pairs_last)
         r.close()
-    assert out["batched"][2] / (2 * 16) > 2048  # mean tile list longer than the cache
+    assert out["batched"][2] / (2 * 16) > 2048  # mean tile list of more than 2,048 tets
     np.testing.assert_allclose(out["batched"][0], out["plain"][0], rtol=1e-4)
     for k in out["plain"][1]:
         assert rel_l2(out["batched"][1][k], out["plain"][1][k]) <= 1e-3, k

@@ -141,8 +141,8 @@ def test_train_step_matches_oracle(c1_scene):
 
 @pytest.mark.parametrize("ts", [8, 12, 16])
 def test_views_modes_agree(c1_scene, ts):
-    """plain (one launch per view, no span cache) vs batched and graph
-    (persistent launches whose adjoint reads the forward's span cache)."""
+    """plain (one launch per view, one CTA per tile) vs batched and graph
+    (persistent launches over all views' tiles, longest lists first)."""
     from rmesh_b200.camera import orbit_cameras
 
     cams = orbit_cameras(4, seed=3, radius=(2.5, 3.5), resolutions=((96, 96), (128, 80), (64, 64)))
