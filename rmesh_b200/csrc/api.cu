@@ -424,8 +424,8 @@ int ensure_run_buffers(RmeshCtx* c, int n_views, uint64_t total_pixels, uint32_t
   CKR(ensure_buf(c, c->pair_val, c->cap_pairs * 4));
   CKR(ensure_buf(c, c->pair_key_alt, c->cap_pairs * 4));
   CKR(ensure_buf(c, c->pair_val_alt, c->cap_pairs * 4));
-  CKR(ensure_buf(c, c->spans_fwd, c->cap_pairs * kSpanRows));
-  CKR(ensure_buf(c, c->spans_adj, c->cap_pairs * kSpanRows));
+  CKR(ensure_buf(c, c->spans_fwd, c->cap_pairs * kSpanRec));
+  CKR(ensure_buf(c, c->spans_adj, c->cap_pairs * kSpanRec));
   const uint64_t sort_items = std::max<uint64_t>(std::max<uint64_t>(items, c->cap_pairs), 4ull * c->M);
   CKR(ensure_buf(c, c->sort_status, ((sort_items + kSortPart - 1) / kSortPart + 1) * 256 * 8));
   CKR(ensure_buf(c, c->scan_status, ((items + 255) / 256 + 2) * 8));

@@ -52,6 +52,9 @@ constexpr int kBatch = 32;
 // are one 16-byte line).  A row's span [lo, hi] (columns < 16) is one byte,
 // lo << 4 | hi; an empty row is 0xF0 (lo > hi).
 constexpr int kSpanRows = 16;
+// per-pair span record of one rule: kSpanRows span bytes, then kSpanRows
+// bytes holding the pair's covered pixels in the rows above each row
+constexpr int kSpanRec = 2 * kSpanRows;
 __device__ __forceinline__ uint8_t pack_span(short2 sp) {
   return sp.x > sp.y ? (uint8_t)0xF0u : (uint8_t)((sp.x << 4) | sp.y);
 }
@@ -100,9 +103,9 @@ struct TileArgs {
   Counters* counters;
   const AdamParams* hp;
   int persistent;
-  // per sorted pair position: the pair's pixel spans of the tile's rows under
-  // the forward's rule and under the adjoint's (kSpanRows one-byte rows each,
-  // see pack_span), from pair_spans_kernel
+  // per sorted pair position: the pair's span record under the forward's rule
+  // and under the adjoint's (kSpanRec bytes each: one-byte row spans, see
+  // pack_span, and the pixels of the rows above each row), from pair_spans_kernel
   const uint8_t* spans_fwd;
   const uint8_t* spans_adj;
   // persistent launches: ticket -> tile (longest lists first); nullptr = identity
@@ -120,10 +123,10 @@ template <int TS, bool AUX, bool WIDE = false>
 struct TileCfg {
   static constexpr int NT = (WIDE ? 2 : 1) * (((TS * TS + 31) / 32) * 32);
   static constexpr int NW = NT / 32;
-  // items per sub-batch; 792 for 12x12 tiles fills a quarter of the SM's
+  // items per sub-batch; 780 for 12x12 tiles fills a quarter of the SM's
   // 228 KB of shared memory (four resident CTAs, the register limit at 96
   // registers per thread): fewer sub-batches, fewer block barriers
-  static constexpr int CAP = WIDE ? (TS == 8 ? 512 : (TS == 12 ? 2048 : 1024)) : (TS == 12 ? 792 : 512);
+  static constexpr int CAP = WIDE ? (TS == 8 ? 512 : (TS == 12 ? 2048 : 1024)) : (TS == 12 ? 780 : 512);
   // resident CTAs per SM the register budget is sized for
   static constexpr int MINB = (WIDE ? 1 : 2) * (TS == 16 ? 1 : (TS == 12 ? 2 : 4));
 };
@@ -132,7 +135,7 @@ template <int TS, bool AUX, bool WIDE = false>
 struct __align__(16) TileSmem {
   using Cfg = TileCfg<TS, AUX, WIDE>;
   TetView view[2][kBatch];  // staged per-view tet records (double buffered)
-  uint8_t span_pf[kBatch][kSpanRows];  // adjoint: the next batch's cached spans (bulk copy, packed)
+  uint8_t span_pf[kBatch][kSpanRec];  // the next batch's span records (bulk copy)
   float mom[kBatch][kMom];  // adjoint moments per tet (phase 2)
   float4 pdir[TS * TS];     // pixel ray direction
   float4 pdl[TS * TS];      // pixel dL/dRGB (adjoint)
@@ -375,13 +378,13 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
       if (warp != 0 || lane >= nb) return 0u;
       return a.pair_val[dir < 0 ? first - (uint32_t)lane : first + (uint32_t)lane];
     };
-    // span_src: the batch's pixel spans (kSpanRows bytes per list position,
+    // span_src: the batch's span records (kSpanRec bytes per list position,
     // ascending), copied into span_pf on the same barrier
     auto issue = [&](int buf, int nb, uint32_t idx, const uint8_t* span_src) {
       if (warp == 0) {
         if (lane == 0) {
           fence_proxy_async_smem();
-          const uint32_t span_bytes = span_src ? (uint32_t)(nb * kSpanRows) : 0u;
+          const uint32_t span_bytes = span_src ? (uint32_t)(nb * kSpanRec) : 0u;
           mbar_arrive_expect_tx(&s.bar[buf], (uint32_t)nb * (uint32_t)sizeof(TetView) + span_bytes);
           if (span_src) bulk_copy_g2s(&s.span_pf[0][0], span_src, span_bytes, &s.bar[buf]);
         }
@@ -448,31 +451,32 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
     };
     // row of task t of tet k (all lanes call)
     auto task_row = [&](int t, int k) -> int { return __shfl_sync(0xffffffffu, rr_lo - (rr_pre - rr_n), k) + t; };
-    // the batch's spans, already copied into span_pf by the batch's bulk copy
-    // (pair_spans_kernel wrote them per list position): tet k is list position
-    // k of the copy, or nb - 1 - k when the batch runs front to back (rev)
+    // the batch's span records, already copied into span_pf by the batch's
+    // bulk copy (pair_spans_kernel wrote them per list position): tet k is list
+    // position k of the copy, or nb - 1 - k when the batch runs front to back
+    // (rev).  Each row's span goes to the span table and its item offset
+    // relative to the tet's first item (the pixels of the rows above, minus the
+    // row's first column) to rowoff.
     auto load_spans = [&](int buf, int nb, bool rev) {
       row_ranges(buf, nb);
       for (int i = tid; i < TS * TS; i += NT) s.pmask[i] = 0u;
       for (int task = tid; task < nb * TS; task += NT) {
         const int k = task / TS, row = task - (task / TS) * TS;
-        s.span[k][row] = s.span_pf[rev ? nb - 1 - k : k][row];
+        const uint8_t* rec = s.span_pf[rev ? nb - 1 - k : k];
+        const uint8_t sb = rec[row];
+        s.span[k][row] = sb;
+        s.rowoff[k][row] = (int16_t)((int)rec[kSpanRows + row] - (int)unpack_span(sb).x);
       }
     };
-    // per-tet row prefix sums over the tet's reachable rows and tet-major item
-    // offsets (after spans; warp 0, lane = tet)
+    // tet-major item offsets (after load_spans; warp 0, lane = tet): a tet's
+    // item count is its last reachable row's offset plus that row's last column
     auto prefixes = [&](int nb) {
       if (warp == 0) {
         uint32_t cnt = 0;
-        if (lane < nb) {
-          const int k = lane;
-          uint32_t acc = 0;
-          for (int r = rr_lo; r < rr_lo + rr_n; ++r) {
-            const short2 sp = unpack_span(s.span[k][r]);
-            s.rowoff[k][r] = (int16_t)((int)acc - (int)sp.x);
-            acc += (uint32_t)max(sp.y - sp.x + 1, 0);
-          }
-          cnt = acc;
+        if (lane < nb && rr_n > 0) {
+          const int last = rr_lo + rr_n - 1;
+          const short2 sp = unpack_span(s.span[lane][last]);
+          cnt = (uint32_t)((int)s.rowoff[lane][last] + (sp.x <= sp.y ? sp.y + 1 : 0));
         }
         uint32_t x = cnt;  // exclusive scan over the batch's tets (nb <= 32)
 #pragma unroll
@@ -603,7 +607,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
       if (re > rs) {
         {
           const int nb0 = (int)min((uint32_t)kBatch, re - rs);
-          issue(0, nb0, load_idx(re - 1u, nb0, -1), a.spans_fwd + (size_t)(re - (uint32_t)nb0) * kSpanRows);
+          issue(0, nb0, load_idx(re - 1u, nb0, -1), a.spans_fwd + (size_t)(re - (uint32_t)nb0) * kSpanRec);
         }
         uint32_t idx_next = 0u;  // record indices of the batch after the current one
         if (re - rs > (uint32_t)kBatch) {
@@ -622,7 +626,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
           // the next batch's copies, after span_pf has been read
           if (next_hi > rs) {
             const int nbn = (int)min((uint32_t)kBatch, next_hi - rs);
-            issue(buf ^ 1, nbn, idx_next, a.spans_fwd + (size_t)(next_hi - (uint32_t)nbn) * kSpanRows);
+            issue(buf ^ 1, nbn, idx_next, a.spans_fwd + (size_t)(next_hi - (uint32_t)nbn) * kSpanRec);
             const uint32_t h2 = next_hi - (uint32_t)nbn;
             if (h2 > rs) idx_next = load_idx(h2 - 1u, (int)min((uint32_t)kBatch, h2 - rs), -1);
           }
@@ -726,7 +730,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
       if (re > rs) {
         {
           const int nb0 = (int)min((uint32_t)kBatch, re - rs);
-          issue(0, nb0, load_idx(re - 1u, nb0, -1), a.spans_fwd + (size_t)(re - (uint32_t)nb0) * kSpanRows);
+          issue(0, nb0, load_idx(re - 1u, nb0, -1), a.spans_fwd + (size_t)(re - (uint32_t)nb0) * kSpanRec);
         }
         uint32_t idx_next = 0u;
         if (re - rs > (uint32_t)kBatch) {
@@ -744,7 +748,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
           __syncthreads();
           if (next_hi > rs) {
             const int nbn = (int)min((uint32_t)kBatch, next_hi - rs);
-            issue(buf ^ 1, nbn, idx_next, a.spans_fwd + (size_t)(next_hi - (uint32_t)nbn) * kSpanRows);
+            issue(buf ^ 1, nbn, idx_next, a.spans_fwd + (size_t)(next_hi - (uint32_t)nbn) * kSpanRec);
             const uint32_t h2 = next_hi - (uint32_t)nbn;
             if (h2 > rs) idx_next = load_idx(h2 - 1u, (int)min((uint32_t)kBatch, h2 - rs), -1);
           }
@@ -916,7 +920,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
         __syncthreads();  // the forward's last reads of the copy buffers
         {
           const int nb0 = (int)min((uint32_t)kBatch, re - rs);
-          issue(0, nb0, load_idx(rs, nb0, +1), a.spans_adj + (size_t)rs * kSpanRows);
+          issue(0, nb0, load_idx(rs, nb0, +1), a.spans_adj + (size_t)rs * kSpanRec);
         }
         uint32_t idx_next = 0u;
         if (re - rs > (uint32_t)kBatch) {
@@ -943,7 +947,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
           // the next batch's copies, after span_pf has been read
           if (next_lo < re) {
             const int nbn = (int)min((uint32_t)kBatch, re - next_lo);
-            issue(buf ^ 1, nbn, idx_next, a.spans_adj + (size_t)next_lo * kSpanRows);
+            issue(buf ^ 1, nbn, idx_next, a.spans_adj + (size_t)next_lo * kSpanRec);
             const uint32_t l2 = next_lo + (uint32_t)nbn;
             if (l2 < re) idx_next = load_idx(l2, (int)min((uint32_t)kBatch, re - l2), +1);
           }
@@ -1278,16 +1282,33 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
   }
 }
 
-// Pixel spans of every sorted (tile, tet) pair, kSpanRows one-byte rows per
-// pair and rule (row_spans), over the rows its tet reaches (the row table rule
+// Span records of every sorted (tile, tet) pair, one per rule: kSpanRows
+// one-byte row spans (row_spans) over the rows its tet reaches (the row table rule
 // of the tile kernel): the tile kernel bulk-copies a batch's rows with its tet
 // records instead of deriving them between block barriers.  Other rows, tets
 // with a vertex behind the camera and sentinel slots get empty spans (the tile
 // kernel reads none of them).  Each warp takes 32 consecutive pairs; lane l
 // sets up pair l, and the warp's (pair, row) tasks are spread over its lanes
 // through a prefix of the row counts, so lanes stay busy whatever the rows per
-// tet.  The rows go to shared memory and each pair's two 16-byte records are
-// stored whole.
+// tet.  The rows go to shared memory; the owner lane then adds, per row, the
+// pixels of the rows above it (at most 15 x 16 = 240, one byte) and stores
+// the pair's two 32-byte records whole.
+// Byte r of the result: the covered pixels of span rows 0..r-1 of v (16
+// packed spans, one per byte).
+__device__ __forceinline__ uint4 rows_above(uint4 v) {
+  const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+  uint32_t c[4] = {0u, 0u, 0u, 0u};
+  uint32_t acc = 0u;
+#pragma unroll
+  for (int r = 0; r < 16; ++r) {
+    const uint32_t b = (w[r >> 2] >> (8 * (r & 3))) & 0xFFu;
+    c[r >> 2] |= acc << (8 * (r & 3));
+    const uint32_t lo = b >> 4, hi = b & 15u;
+    acc += lo <= hi ? hi - lo + 1u : 0u;
+  }
+  return make_uint4(c[0], c[1], c[2], c[3]);
+}
+
 struct PairSpanArgs {
   const ViewParams* views;
   int n_views;
@@ -1301,7 +1322,7 @@ struct PairSpanArgs {
 };
 
 __global__ void __launch_bounds__(256) pair_spans_kernel(PairSpanArgs a) {
-  static_assert(kSpanRows == 16, "one 16-byte row record per pair and rule");
+  static_assert(kSpanRows == 16 && kSpanRec == 32, "16 span bytes + 16 row-offset bytes per pair and rule");
   __shared__ __align__(16) uint8_t s_fwd[256][kSpanRows];
   __shared__ __align__(16) uint8_t s_adj[256][kSpanRows];
   const int lane = threadIdx.x & 31, wbase = threadIdx.x & ~31;
@@ -1371,8 +1392,14 @@ __global__ void __launch_bounds__(256) pair_spans_kernel(PairSpanArgs a) {
     }
     __syncwarp();
     if (p < n) {
-      *reinterpret_cast<uint4*>(a.spans_fwd + p * kSpanRows) = *reinterpret_cast<const uint4*>(s_fwd[threadIdx.x]);
-      *reinterpret_cast<uint4*>(a.spans_adj + p * kSpanRows) = *reinterpret_cast<const uint4*>(s_adj[threadIdx.x]);
+      const uint4 vf = *reinterpret_cast<const uint4*>(s_fwd[threadIdx.x]);
+      const uint4 va = *reinterpret_cast<const uint4*>(s_adj[threadIdx.x]);
+      uint4* df = reinterpret_cast<uint4*>(a.spans_fwd + p * kSpanRec);
+      uint4* da = reinterpret_cast<uint4*>(a.spans_adj + p * kSpanRec);
+      df[0] = vf;
+      df[1] = rows_above(vf);
+      da[0] = va;
+      da[1] = rows_above(va);
     }
     __syncwarp();  // the stores' reads before the next chunk's rows are reset
   }
