@@ -468,15 +468,17 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
         s.rowoff[k][row] = (int16_t)((int)rec[kSpanRows + row] - (int)unpack_span(sb).x);
       }
     };
-    // tet-major item offsets (after load_spans; warp 0, lane = tet): a tet's
-    // item count is its last reachable row's offset plus that row's last column
-    auto prefixes = [&](int nb) {
+    // tet-major item offsets (warp 0, lane = tet, read from the span records in
+    // span_pf, so it runs beside load_spans before the same barrier): a tet's
+    // item count is its last reachable row's pixels above plus that row's width
+    auto prefixes = [&](int nb, bool rev) {
       if (warp == 0) {
         uint32_t cnt = 0;
         if (lane < nb && rr_n > 0) {
           const int last = rr_lo + rr_n - 1;
-          const short2 sp = unpack_span(s.span[lane][last]);
-          cnt = (uint32_t)((int)s.rowoff[lane][last] + (sp.x <= sp.y ? sp.y + 1 : 0));
+          const uint8_t* rec = s.span_pf[rev ? nb - 1 - lane : lane];
+          const short2 sp = unpack_span(rec[last]);
+          cnt = (uint32_t)rec[kSpanRows + last] + (uint32_t)max(sp.y - sp.x + 1, 0);
         }
         uint32_t x = cnt;  // exclusive scan over the batch's tets (nb <= 32)
 #pragma unroll
@@ -622,6 +624,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
           wait_buf(buf);
           if (failed) break;
           load_spans(buf, nb, true);
+          prefixes(nb, true);
           __syncthreads();
           // the next batch's copies, after span_pf has been read
           if (next_hi > rs) {
@@ -630,8 +633,6 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
             const uint32_t h2 = next_hi - (uint32_t)nbn;
             if (h2 > rs) idx_next = load_idx(h2 - 1u, (int)min((uint32_t)kBatch, h2 - rs), -1);
           }
-          prefixes(nb);
-          __syncthreads();
           int k1 = sub_end(0, nb);
           fill(0, k1);
           __syncthreads();
@@ -745,6 +746,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
           wait_buf(buf);
           if (failed) break;
           load_spans(buf, nb, true);
+          prefixes(nb, true);
           __syncthreads();
           if (next_hi > rs) {
             const int nbn = (int)min((uint32_t)kBatch, next_hi - rs);
@@ -752,8 +754,6 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
             const uint32_t h2 = next_hi - (uint32_t)nbn;
             if (h2 > rs) idx_next = load_idx(h2 - 1u, (int)min((uint32_t)kBatch, h2 - rs), -1);
           }
-          prefixes(nb);
-          __syncthreads();
           int k1 = sub_end(0, nb);
           fill(0, k1);
           __syncthreads();
@@ -943,6 +943,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
           }
           // adjoint: edge crossings only (backward_tiled_compute.wgsl:241-299)
           load_spans(buf, nb, false);
+          prefixes(nb, false);
           __syncthreads();
           // the next batch's copies, after span_pf has been read
           if (next_lo < re) {
@@ -951,8 +952,6 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
             const uint32_t l2 = next_lo + (uint32_t)nbn;
             if (l2 < re) idx_next = load_idx(l2, (int)min((uint32_t)kBatch, re - l2), +1);
           }
-          prefixes(nb);
-          __syncthreads();
           int k1 = sub_end(0, nb);
           fill(0, k1);
           __syncthreads();
