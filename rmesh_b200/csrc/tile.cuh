@@ -239,7 +239,7 @@ __device__ __forceinline__ void integrate(const float4& cb, float dcdt, float t_
 // fwd under the forward's rule (rasterize_compute.wgsl:170-275: a row is
 // reached when an edge crosses its centre line or a vertex lies in the row),
 // adj under the adjoint's (backward_tiled_compute.wgsl:241-299: edge crossings
-// only).  vpx, vpy: the vertex projections minus the tile origin; columns past
+// only).  The vertex projections are taken minus the tile origin; columns past
 // valid_cols (outside the image) are dropped, as the reference skips their
 // pixels (rasterize_compute.wgsl:332).  The projections use fast arithmetic,
 // and spans include pixels up to 0.001 px outside the silhouette, where the
@@ -255,36 +255,45 @@ __device__ __forceinline__ short2 span_of_cols(float xl, float xr, int valid_col
   }
   return sp;
 }
-__device__ __forceinline__ void row_spans(const float vpx[4], const float vpy[4], int row, int valid_cols, uint8_t& fwd,
+// sx, sy: the four vertices sorted by y.  An edge crosses the row's centre
+// line yc when its lower end is <= yc < its upper end, so with b vertices at
+// or below yc the crossing edges are exactly the pairs (i, j) of sorted ranks
+// i < b <= j: three edges for b = 1 or 3, four for b = 2, none otherwise.
+__device__ __forceinline__ void row_spans(const float sx[4], const float sy[4], int row, int valid_cols, uint8_t& fwd,
                                           uint8_t& adj) {
   fwd = 0xF0u;
   adj = 0xF0u;
   const float yc = fa((float)row, 0.5f);
-  const float ylo = fminf(fminf(vpy[0], vpy[1]), fminf(vpy[2], vpy[3]));
-  const float yhi = fmaxf(fmaxf(vpy[0], vpy[1]), fmaxf(vpy[2], vpy[3]));
+  const float blo = fs(yc, 0.5f), bhi = fa(yc, 0.5f);
   // the adjoint's reach (some edge crosses yc) implies the forward's
-  if (!(yhi >= fs(yc, 0.5f) && ylo < fa(yc, 0.5f))) return;
+  if (!(sy[3] >= blo && sy[0] < bhi)) return;
+  const int nb = (sy[0] <= yc ? 1 : 0) + (sy[1] <= yc ? 1 : 0) + (sy[2] <= yc ? 1 : 0) + (sy[3] <= yc ? 1 : 0);
   float xl = 1e10f, xr = -1e10f;
-  const int ei[6] = {0, 0, 0, 1, 1, 2};
-  const int ej[6] = {1, 2, 3, 2, 3, 3};
-#pragma unroll
-  for (int e = 0; e < 6; ++e) {
-    const float yi = vpy[ei[e]], yj = vpy[ej[e]];
-    if ((yi <= yc && yj > yc) || (yj <= yc && yi > yc)) {
-      const float t = __fdividef(yc - yi, yj - yi);
-      const float x = vpx[ei[e]] + t * (vpx[ej[e]] - vpx[ei[e]]);
-      xl = fminf(xl, x);
-      xr = fmaxf(xr, x);
-    }
+  auto cross = [&](float xi, float yi, float xj, float yj) {
+    const float t = __fdividef(yc - yi, yj - yi);
+    const float x = xi + t * (xj - xi);
+    xl = fminf(xl, x);
+    xr = fmaxf(xr, x);
+  };
+  if (nb >= 1 && nb <= 3) {
+    cross(sx[0], sy[0], sx[3], sy[3]);  // (0, 3) crosses in every band
+    // (0, 1) | (0, 2) | (1, 3) for b = 1 | 2 | 3
+    const float ax = nb == 3 ? sx[1] : sx[0], ay = nb == 3 ? sy[1] : sy[0];
+    const float bx = nb == 1 ? sx[1] : (nb == 2 ? sx[2] : sx[3]), by = nb == 1 ? sy[1] : (nb == 2 ? sy[2] : sy[3]);
+    cross(ax, ay, bx, by);
+    // (0, 2) | (1, 2) | (2, 3)
+    const float cx = nb == 1 ? sx[0] : (nb == 2 ? sx[1] : sx[2]), cy = nb == 1 ? sy[0] : (nb == 2 ? sy[1] : sy[2]);
+    const float dx = nb == 3 ? sx[3] : sx[2], dy = nb == 3 ? sy[3] : sy[2];
+    cross(cx, cy, dx, dy);
+    if (nb == 2) cross(sx[1], sy[1], sx[3], sy[3]);  // (1, 3)
   }
   adj = pack_span(span_of_cols(xl, xr, valid_cols));  // empty when no edge crosses yc
-  const float blo = fs(yc, 0.5f), bhi = fa(yc, 0.5f);
 #pragma unroll
   for (int q = 0; q < 4; ++q) {
-    const float vyq = vpy[q];
+    const float vyq = sy[q];
     if (vyq >= blo && vyq < bhi) {
-      xl = fminf(xl, vpx[q]);
-      xr = fmaxf(xr, vpx[q]);
+      xl = fminf(xl, sx[q]);
+      xr = fmaxf(xr, sx[q]);
     }
   }
   fwd = pack_span(span_of_cols(xl, xr, valid_cols));
@@ -1349,10 +1358,18 @@ __global__ void __launch_bounds__(256) pair_spans_kernel(PairSpanArgs a) {
           const float tile_ox = (float)(tx * (uint32_t)TS), tile_oy = (float)(ty * (uint32_t)TS);
           vpx[0] = gx4.x - tile_ox; vpx[1] = gx4.y - tile_ox; vpx[2] = gx4.z - tile_ox; vpx[3] = gx4.w - tile_ox;
           vpy[0] = gy4.x - tile_oy; vpy[1] = gy4.y - tile_oy; vpy[2] = gy4.z - tile_oy; vpy[3] = gy4.w - tile_oy;
+          // the vertices sorted by y (five compare-exchanges), as row_spans takes them
+          auto cx = [&](int i, int j) {
+            if (vpy[j] < vpy[i]) {
+              const float ty = vpy[i], tx = vpx[i];
+              vpy[i] = vpy[j]; vpx[i] = vpx[j];
+              vpy[j] = ty; vpx[j] = tx;
+            }
+          };
+          cx(0, 1); cx(2, 3); cx(0, 2); cx(1, 3); cx(1, 2);
           // rows r with floor(ylo) <= r <= floor(yhi), clipped to the image: the
           // only rows the forward's reach rule can accept
-          const float ylo = fminf(fminf(vpy[0], vpy[1]), fminf(vpy[2], vpy[3]));
-          const float yhi = fmaxf(fmaxf(vpy[0], vpy[1]), fmaxf(vpy[2], vpy[3]));
+          const float ylo = vpy[0], yhi = vpy[3];
           const float flo = fmaxf(floorf(ylo), 0.0f);
           const float fhi = fminf(floorf(yhi), (float)(valid_rows - 1));
           if (flo <= fhi) {
