@@ -95,8 +95,16 @@ struct EmitArgs {
   Counters* counters;
 };
 
-// One thread per sorted entry, 256 entries per block: the block's pair
-// offset comes from emit_scan_kernel, so blocks never wait on each other.
+// 256 sorted entries per block, one per thread: the block's pair offset comes
+// from emit_scan_kernel (blocks never wait on each other) plus a block-local
+// scan of the entries' tile counts.  Each warp then spreads its entries'
+// (entry, tile row) tasks over its lanes through a prefix of the row counts,
+// so a lane whose entry spans many tile rows does not hold up the others.  A
+// row's first pair slot is the entry's pairs of the rows before it: a scan of
+// the row widths within the round plus the entry's pairs of earlier rounds.
+// The pairs are exactly the per-entry loop's: rows in order, tiles in order,
+// the first cnt of them (cnt from the projection's count), and sentinels for
+// the slots an entry leaves unfilled.
 __global__ void __launch_bounds__(256) emit_kernel(EmitArgs a) {
   __shared__ unsigned long long s_wsum[8];
   const uint32_t blk = blockIdx.x;
@@ -125,35 +133,99 @@ __global__ void __launch_bounds__(256) emit_kernel(EmitArgs a) {
 #pragma unroll
   for (int w = 0; w < 8; ++w)
     if (w < warp) woff += s_wsum[w];
-  if (!in || cnt == 0) return;
   const unsigned long long off = a.group_off[blk] + woff + x - cnt;
 
+  // this lane's entry: projected vertices and tile box
   const uint32_t view = (uint32_t)(key >> 32) & 0xFFu;
-  const ViewParams& V = a.views[view];
-  const float4 q0 = a.vis_proj[2 * (size_t)j], q1 = a.vis_proj[2 * (size_t)j + 1];
-  const float px[4] = {q0.x, q0.z, q1.x, q1.z};
-  const float py[4] = {q0.y, q0.w, q1.y, q1.w};
-  uint32_t local = 0;
+  float px[4] = {0.f, 0.f, 0.f, 0.f}, py[4] = {0.f, 0.f, 0.f, 0.f};
+  TileBox tb = {0u, 0u, 0u, 0u};
+  uint32_t TS = 1u, tile_base = 0u, tiles_x = 0u;
+  int nrows = 0;
+  if (in && cnt > 0) {
+    const ViewParams& V = a.views[view];
+    TS = (uint32_t)V.TS;
+    tile_base = V.tile_base;
+    tiles_x = (uint32_t)V.tiles_x;
+    const float4 q0 = a.vis_proj[2 * (size_t)j], q1 = a.vis_proj[2 * (size_t)j + 1];
+    px[0] = q0.x; px[1] = q0.z; px[2] = q1.x; px[3] = q1.z;
+    py[0] = q0.y; py[1] = q0.w; py[2] = q1.y; py[3] = q1.w;
+    if (tile_range(px, py, V.Wf, V.Hf, TS, tb)) nrows = (int)(tb.max_y - tb.min_y) + 1;
+  }
+  int pre = nrows;  // inclusive prefix of the row counts over the warp's lanes
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, pre, o);
+    if (lane >= o) pre += y;
+  }
+  const int excl = pre - nrows;
+  const int total = __shfl_sync(0xffffffffu, pre, 31);
+  uint32_t emitted = 0u;  // pairs of this lane's entry in the rows handled so far
   bool overflow = false;
-  scanline_tiles(px, py, V.Wf, V.Hf, (uint32_t)V.TS, [&](uint32_t ty, uint32_t tx0, uint32_t tx1) {
-    for (uint32_t tx = tx0; tx <= tx1 && local < cnt; ++tx, ++local) {
-      const unsigned long long w = off + local;
+  for (int t0 = 0; t0 < total; t0 += 32) {  // warp-uniform trip count
+    const int t = t0 + lane;
+    int e = 0;  // the lane whose entry owns task t: first inclusive prefix > t
+#pragma unroll
+    for (int st = 16; st > 0; st >>= 1) {
+      const int pv = __shfl_sync(0xffffffffu, pre, e + st - 1);
+      if (pv <= t) e += st;
+    }
+    const int e_excl = __shfl_sync(0xffffffffu, excl, e);
+    float qx[4], qy[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      qx[q] = __shfl_sync(0xffffffffu, px[q], e);
+      qy[q] = __shfl_sync(0xffffffffu, py[q], e);
+    }
+    TileBox eb;
+    eb.min_x = __shfl_sync(0xffffffffu, tb.min_x, e);
+    eb.max_x = __shfl_sync(0xffffffffu, tb.max_x, e);
+    eb.min_y = __shfl_sync(0xffffffffu, tb.min_y, e);
+    eb.max_y = __shfl_sync(0xffffffffu, tb.max_y, e);
+    const uint32_t e_ts = __shfl_sync(0xffffffffu, TS, e);
+    const uint32_t ty = eb.min_y + (uint32_t)(t - e_excl);
+    uint32_t tx0 = 0u, tx1 = 0u, width = 0u;
+    if (t < total && tile_row_span(qx, qy, e_ts, eb, ty, tx0, tx1)) width = tx1 - tx0 + 1u;
+    uint32_t incl = width;  // inclusive scan of the row widths over the round
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    const uint32_t exw = incl - width;
+    // the entry's first slot of this row: its pairs of earlier rounds plus the
+    // widths of its earlier rows in this round
+    const int first_lane = max(e_excl - t0, 0);
+    const uint32_t pos = __shfl_sync(0xffffffffu, emitted, e) + exw - __shfl_sync(0xffffffffu, exw, first_lane);
+    const unsigned long long e_off = __shfl_sync(0xffffffffu, off, e);
+    const uint32_t e_cnt = __shfl_sync(0xffffffffu, cnt, e);
+    const uint32_t e_j = __shfl_sync(0xffffffffu, j, e);
+    const uint32_t e_base = __shfl_sync(0xffffffffu, tile_base, e);
+    const uint32_t e_tx = __shfl_sync(0xffffffffu, tiles_x, e);
+    for (uint32_t i = 0; i < width && pos + i < e_cnt; ++i) {
+      const unsigned long long w = e_off + pos + i;
       if (w < a.cap) {
-        a.pair_key[w] = V.tile_base + ty * (uint32_t)V.tiles_x + tx;
-        a.pair_val[w] = j;
+        a.pair_key[w] = e_base + ty * e_tx + tx0 + i;
+        a.pair_val[w] = e_j;
       } else {
         overflow = true;
       }
     }
-  });
-  if (local < cnt) atomicOr(&a.counters->shortfall[view], 1u);
-  for (; local < cnt; ++local) {
-    const unsigned long long w = off + local;
-    if (w < a.cap) {
-      a.pair_key[w] = kSentinel;
-      a.pair_val[w] = 0u;
-    } else {
-      overflow = true;
+    // this lane's entry: add the widths of its rows in this round
+    const int my_first = max(excl - t0, 0), my_last = min(pre - t0, 32) - 1;
+    const uint32_t hi_sum = __shfl_sync(0xffffffffu, incl, max(my_last, 0));
+    const uint32_t lo_sum = __shfl_sync(0xffffffffu, exw, min(my_first, 31));
+    if (nrows > 0 && my_first <= my_last) emitted += hi_sum - lo_sum;
+  }
+  if (in && cnt > 0) {
+    if (emitted < cnt) atomicOr(&a.counters->shortfall[view], 1u);
+    for (uint32_t l = emitted; l < cnt; ++l) {
+      const unsigned long long w = off + l;
+      if (w < a.cap) {
+        a.pair_key[w] = kSentinel;
+        a.pair_val[w] = 0u;
+      } else {
+        overflow = true;
+      }
     }
   }
   if (overflow) atomicOr(&a.counters->err, kErrPairOverflow);

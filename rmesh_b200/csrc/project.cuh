@@ -40,55 +40,71 @@ __global__ void __launch_bounds__(256) build_records_kernel(int M, const float* 
 }
 
 // Conservative scanline over tile rows (project_compute.wgsl:202-259 ==
-// tile_gen_scan_compute.wgsl:119-201), exact arithmetic.  Calls
+// tile_gen_scan_compute.wgsl:119-201), exact arithmetic.  tile_range gives a
+// tet's clamped pixel box in tiles (false when it is empty), tile_row_span one
+// tile row's [tx0, tx1] (false when the row is empty); scanline_tiles calls
 // f(ty, tx0, tx1) for every tile row with a non-empty clamped span.
-template <class F>
-__device__ __forceinline__ void scanline_tiles(const float px[4], const float py[4], float W, float H, uint32_t TS,
-                                               F&& f) {
+struct TileBox {
+  uint32_t min_x, max_x, min_y, max_y;
+};
+__device__ __forceinline__ bool tile_range(const float px[4], const float py[4], float W, float H, uint32_t TS,
+                                           TileBox& tb) {
   const float pix_min_x = fmaxf(fminf(fminf(px[0], px[1]), fminf(px[2], px[3])), 0.0f);
   const float pix_max_x = fminf(fmaxf(fmaxf(px[0], px[1]), fmaxf(px[2], px[3])), fs(W, 1.0f));
   const float pix_min_y = fmaxf(fminf(fminf(py[0], py[1]), fminf(py[2], py[3])), 0.0f);
   const float pix_max_y = fminf(fmaxf(fmaxf(py[0], py[1]), fmaxf(py[2], py[3])), fs(H, 1.0f));
-  if (pix_min_x > pix_max_x || pix_min_y > pix_max_y) return;
+  if (pix_min_x > pix_max_x || pix_min_y > pix_max_y) return false;
   const float T = (float)TS;
   const uint32_t tiles_x_total = __float2uint_rz(ceilf(fdv(W, T)));
-  const uint32_t tile_min_x = __float2uint_rz(fdv(pix_min_x, T));
-  const uint32_t tile_max_x = min(__float2uint_rz(fdv(pix_max_x, T)), tiles_x_total - 1u);
-  const uint32_t tile_min_y = __float2uint_rz(fdv(pix_min_y, T));
-  const uint32_t tile_max_y = min(__float2uint_rz(fdv(pix_max_y, T)), __float2uint_rz(ceilf(fdv(H, T))) - 1u);
+  tb.min_x = __float2uint_rz(fdv(pix_min_x, T));
+  tb.max_x = min(__float2uint_rz(fdv(pix_max_x, T)), tiles_x_total - 1u);
+  tb.min_y = __float2uint_rz(fdv(pix_min_y, T));
+  tb.max_y = min(__float2uint_rz(fdv(pix_max_y, T)), __float2uint_rz(ceilf(fdv(H, T))) - 1u);
+  return true;
+}
+__device__ __forceinline__ bool tile_row_span(const float px[4], const float py[4], uint32_t TS, const TileBox& tb,
+                                              uint32_t ty, uint32_t& tx0, uint32_t& tx1) {
+  const float T = (float)TS;
   const int ei[6] = {0, 0, 0, 1, 1, 2};
   const int ej[6] = {1, 2, 3, 2, 3, 3};
-  for (uint32_t ty = tile_min_y; ty <= tile_max_y; ++ty) {
-    float xl = 1e10f, xr = -1e10f;
+  float xl = 1e10f, xr = -1e10f;
 #pragma unroll
-    for (int e = 0; e < 6; ++e) {
-      const float yi = py[ei[e]], yj = py[ej[e]], xi = px[ei[e]], xj = px[ej[e]];
+  for (int e = 0; e < 6; ++e) {
+    const float yi = py[ei[e]], yj = py[ej[e]], xi = px[ei[e]], xj = px[ej[e]];
 #pragma unroll
-      for (uint32_t b = 0; b < 2; ++b) {
-        const float ytest = fm((float)(ty + b), T);
-        if ((yi <= ytest && yj > ytest) || (yj <= ytest && yi > ytest)) {
-          const float t = fdv(fs(ytest, yi), fs(yj, yi));
-          const float x = fa(xi, fm(t, fs(xj, xi)));
-          xl = fminf(xl, x);
-          xr = fmaxf(xr, x);
-        }
+    for (uint32_t b = 0; b < 2; ++b) {
+      const float ytest = fm((float)(ty + b), T);
+      if ((yi <= ytest && yj > ytest) || (yj <= ytest && yi > ytest)) {
+        const float t = fdv(fs(ytest, yi), fs(yj, yi));
+        const float x = fa(xi, fm(t, fs(xj, xi)));
+        xl = fminf(xl, x);
+        xr = fmaxf(xr, x);
       }
     }
-    const float band_lo = fm((float)ty, T), band_hi = fm((float)(ty + 1u), T);
+  }
+  const float band_lo = fm((float)ty, T), band_hi = fm((float)(ty + 1u), T);
 #pragma unroll
-    for (int v = 0; v < 4; ++v) {
-      if (py[v] >= band_lo && py[v] <= band_hi) {
-        xl = fminf(xl, px[v]);
-        xr = fmaxf(xr, px[v]);
-      }
+  for (int v = 0; v < 4; ++v) {
+    if (py[v] >= band_lo && py[v] <= band_hi) {
+      xl = fminf(xl, px[v]);
+      xr = fmaxf(xr, px[v]);
     }
-    if (xl <= xr) {
-      uint32_t tx0 = __float2uint_rz(fmaxf(floorf(fdv(xl, T)), 0.0f));
-      uint32_t tx1 = __float2uint_rz(fmaxf(floorf(fdv(xr, T)), 0.0f));
-      tx0 = min(max(tx0, tile_min_x), tile_max_x);
-      tx1 = min(max(tx1, tile_min_x), tile_max_x);
-      f(ty, tx0, tx1);
-    }
+  }
+  if (!(xl <= xr)) return false;
+  tx0 = __float2uint_rz(fmaxf(floorf(fdv(xl, T)), 0.0f));
+  tx1 = __float2uint_rz(fmaxf(floorf(fdv(xr, T)), 0.0f));
+  tx0 = min(max(tx0, tb.min_x), tb.max_x);
+  tx1 = min(max(tx1, tb.min_x), tb.max_x);
+  return true;
+}
+template <class F>
+__device__ __forceinline__ void scanline_tiles(const float px[4], const float py[4], float W, float H, uint32_t TS,
+                                               F&& f) {
+  TileBox tb;
+  if (!tile_range(px, py, W, H, TS, tb)) return;
+  for (uint32_t ty = tb.min_y; ty <= tb.max_y; ++ty) {
+    uint32_t tx0, tx1;
+    if (tile_row_span(px, py, TS, tb, ty, tx0, tx1)) f(ty, tx0, tx1);
   }
 }
 

@@ -13,23 +13,24 @@
 //            planes, colour base, projected vertices; written once per
 //            (view, tet) by the project kernel) into shared memory with TMA
 //            bulk copies (double buffered: batch b+1 is in flight while batch
-//            b is composited);
-//   spans    (tet, row) tasks derive each row's pixel span exactly as the
-//            reference scanline does; every covered (pixel, tet) pair is an
-//            "item", numbered tet-major through per-tet / per-row prefix sums,
-//            and each pixel gets a 32-bit mask of the tets covering it;
+//            b is composited), and with them each pair's span record of the
+//            pass (pair_spans_kernel, below: every tile row's pixel span under
+//            the reference scanline's rule and the pixels of the rows above);
+//   spans    every covered (pixel, tet) pair is an "item", numbered tet-major
+//            through the records' row offsets and one scan over the batch's
+//            tets, and each pixel gets a 32-bit mask of the tets covering it;
 //   phase 0  item-parallel (every thread busy): ray-tet intersection and the
 //            segment integral of each item -> premultiplied colour, depth;
 //   phase 1  pixel-sequential (the only order-dependent part, a few
 //            instructions per item): the pixel's owner walks its mask and
 //            composites front to back (forward) or undoes back to front and
 //            records the restored transmittance and d(logT) (adjoint);
-//   phase 2  adjoint only, item-parallel: the gradient of each item, then a
-//            warp-segmented reduction by tet (items are tet-major, so each
-//            warp's 32 items form contiguous per-tet segments) into 24 shared
-//            moments per tet, from which the tet's 19 gradients are rebuilt and
-//            flushed to global memory with five 16-byte vector atomics per tet
-//            and batch.
+//   phase 2  adjoint only, item-parallel: the gradient of each item, summed
+//            per thread over a run of one tet's items, then a warp-segmented
+//            reduction by tet (a tet's runs sit in adjacent lanes) into 24
+//            shared moments per tet, from which the tet's 19 gradients are
+//            rebuilt and flushed to global memory with five 16-byte vector
+//            atomics per tet and batch.
 // A tet covers ~5-20 of a tile's 144-256 pixels, so working on items keeps
 // all lanes busy where a thread-per-pixel sweep would idle most of them.
 // Batches whose item count exceeds the item buffer run in several sub-batches.
@@ -1302,17 +1303,23 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
 // pixels of the rows above it (at most 15 x 16 = 240, one byte) and stores
 // the pair's two 32-byte records whole.
 // Byte r of the result: the covered pixels of span rows 0..r-1 of v (16
-// packed spans, one per byte).
+// packed spans, one per byte), four rows per 32-bit word at a time: per byte,
+// (hi | 0x80) - lo keeps bit 7 exactly when lo <= hi and holds hi - lo below
+// it; the word's prefix sum of the widths is one multiply by 0x01010101 (no
+// byte carries: at most 15 x 16 = 240 pixels lie above any row).
 __device__ __forceinline__ uint4 rows_above(uint4 v) {
   const uint32_t w[4] = {v.x, v.y, v.z, v.w};
-  uint32_t c[4] = {0u, 0u, 0u, 0u};
+  uint32_t c[4];
   uint32_t acc = 0u;
 #pragma unroll
-  for (int r = 0; r < 16; ++r) {
-    const uint32_t b = (w[r >> 2] >> (8 * (r & 3))) & 0xFFu;
-    c[r >> 2] |= acc << (8 * (r & 3));
-    const uint32_t lo = b >> 4, hi = b & 15u;
-    acc += lo <= hi ? hi - lo + 1u : 0u;
+  for (int q = 0; q < 4; ++q) {
+    const uint32_t lo = (w[q] >> 4) & 0x0F0F0F0Fu, hi = w[q] & 0x0F0F0F0Fu;
+    const uint32_t d = (hi | 0x80808080u) - lo;
+    const uint32_t mask = ((d & 0x80808080u) >> 7) * 0xFFu;
+    const uint32_t width = ((d & 0x7F7F7F7Fu) + 0x01010101u) & mask;
+    const uint32_t incl = width * 0x01010101u;
+    c[q] = incl - width + acc * 0x01010101u;
+    acc += incl >> 24;
   }
   return make_uint4(c[0], c[1], c[2], c[3]);
 }
