@@ -50,11 +50,11 @@ LR_SH = 2.5e-3
 # DRAM bytes (read + write) per (tile, tet) pair of the fused compositing
 # kernel, from a one-kernel ncu capture of a 4-view case of this workload's
 # mesh and resolution mix (bench.py --views 4: 8.13 M pairs,
-# dram__bytes_read.sum + dram__bytes_write.sum = 2.594 GB); the roofline's
+# dram__bytes_read.sum + dram__bytes_write.sum = 2.907 GB); the roofline's
 # "traffic" scales it to the run's pair count.
-TILE_DRAM_BYTES_PER_PAIR = 319.0
+TILE_DRAM_BYTES_PER_PAIR = 358.0
 # Warp instructions per (tile, tet) pair of the same kernel, from the same
-# capture (smsp__inst_executed.sum = 9.404 G); the issue ceiling is 148 SMs x
+# capture (smsp__inst_executed.sum = 9.408 G); the issue ceiling is 148 SMs x
 # 4 schedulers x one instruction per clock.
 TILE_WARP_INST_PER_PAIR = 1157.0
 
