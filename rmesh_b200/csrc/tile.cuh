@@ -124,10 +124,10 @@ template <int TS, bool AUX, bool WIDE = false>
 struct TileCfg {
   static constexpr int NT = (WIDE ? 2 : 1) * (((TS * TS + 31) / 32) * 32);
   static constexpr int NW = NT / 32;
-  // items per sub-batch; 780 for 12x12 tiles fills a quarter of the SM's
+  // items per sub-batch; 812 for 12x12 tiles fills a quarter of the SM's
   // 228 KB of shared memory (four resident CTAs, the register limit at 96
   // registers per thread): fewer sub-batches, fewer block barriers
-  static constexpr int CAP = WIDE ? (TS == 8 ? 512 : (TS == 12 ? 2048 : 1024)) : (TS == 12 ? 780 : 512);
+  static constexpr int CAP = WIDE ? (TS == 8 ? 512 : (TS == 12 ? 2048 : 1024)) : (TS == 12 ? 812 : 512);
   // resident CTAs per SM the register budget is sized for
   static constexpr int MINB = (WIDE ? 1 : 2) * (TS == 16 ? 1 : (TS == 12 ? 2 : 4));
 };
@@ -138,8 +138,8 @@ struct __align__(16) TileSmem {
   TetView view[2][kBatch];  // staged per-view tet records (double buffered)
   uint8_t span_pf[kBatch][kSpanRec];  // the next batch's span records (bulk copy)
   float mom[kBatch][kMom];  // adjoint moments per tet (phase 2)
-  float4 pdir[TS * TS];     // pixel ray direction
-  float4 pdl[TS * TS];      // pixel dL/dRGB (adjoint)
+  float4 pdir[TS * TS];     // pixel ray direction; w: the pixel's dL/dR (adjoint)
+  float2 pdl[TS * TS];      // the pixel's dL/dG, dL/dB (adjoint); pixel and SSIM error (error mode)
   float4 item[Cfg::CAP];    // (cp.rgb, od) -> adjoint: (t_prev, d_od_state, has, aux_s)
   float4 itemx[Cfg::CAP];   // (t_min, t_max, packed faces | tet | pixel, alpha_t)
   float red[Cfg::NW][32][kRedCols];  // per-warp face sums and transpose (odd row stride)
@@ -736,8 +736,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
     // tet_count.
     if (MODE == kModeError) {
       bool alive = valid;
-      if (in_tile) s.pdl[pl] = valid ? make_float4(a.pixel_err[pix], a.ssim_err[pix], 0.f, 0.f)
-                                     : make_float4(0.f, 0.f, 0.f, 0.f);
+      if (in_tile) s.pdl[pl] = valid ? make_float2(a.pixel_err[pix], a.ssim_err[pix]) : make_float2(0.f, 0.f);
       if (re > rs) {
         {
           const int nb0 = (int)min((uint32_t)kBatch, re - rs);
@@ -808,7 +807,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
                   const int p = (int)(pk >> 10);
                   const float w = st.x;
                   const float4 d = s.pdir[p];
-                  const float4 e = s.pdl[p];
+                  const float2 e = s.pdl[p];
                   const float ox = camx + d.x * V.min_t, oy = camy + d.y * V.min_t, oz = camz + d.z * V.min_t;
                   m[0] = w;
                   m[1] = w * e.x;
@@ -925,7 +924,10 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
         dlogT = -dl.w * (1.0f - img.w);
         dlr = dl.x; dlg = dl.y; dlb = dl.z;
       }
-      if (in_tile) s.pdl[pl] = make_float4(dlr, dlg, dlb, 0.0f);
+      if (in_tile) {
+        s.pdir[pl].w = dlr;
+        s.pdl[pl] = make_float2(dlg, dlb);
+      }
       if (re > rs) {
         __syncthreads();  // the forward's last reads of the copy buffers
         {
@@ -1079,16 +1081,16 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
                 const float t_min = ix.x, t_max = ix.y;
                 const float t_prev = st.x, d_od_state = st.y;
                 const float4 d = s.pdir[p];
-                const float4 dlv = s.pdl[p];
+                const float2 dgb = s.pdl[p];
                 const TetView& tv = s.view[buf][k];
                 const float4 cb = tv.cb;
                 const float4 gg = tv.gm;
                 const float dcdt = dot3x(gg.x, gg.y, gg.z, d.x, d.y, d.z);
                 Integral I;
                 integrate(cb, dcdt, t_min, t_max, I, ix.w);
-                const float dcpr = clipf(dlv.x * t_prev, kMinVal, kMaxVal);
-                const float dcpg = clipf(dlv.y * t_prev, kMinVal, kMaxVal);
-                const float dcpb = clipf(dlv.z * t_prev, kMinVal, kMaxVal);
+                const float dcpr = clipf(d.w * t_prev, kMinVal, kMaxVal);
+                const float dcpg = clipf(dgb.x * t_prev, kMinVal, kMaxVal);
+                const float dcpb = clipf(dgb.y * t_prev, kMinVal, kMaxVal);
                 float dph;
                 if (fabsf(I.od) < 0.02f)
                   dph = -0.5f + I.od * (1.0f / 3.0f + I.od * (-1.0f / 8.0f + I.od * (1.0f / 30.0f)));
