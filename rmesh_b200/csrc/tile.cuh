@@ -124,10 +124,10 @@ template <int TS, bool AUX, bool WIDE = false>
 struct TileCfg {
   static constexpr int NT = (WIDE ? 2 : 1) * (((TS * TS + 31) / 32) * 32);
   static constexpr int NW = NT / 32;
-  // items per sub-batch; 812 for 12x12 tiles fills a quarter of the SM's
+  // items per sub-batch; 920 for 12x12 tiles fills a quarter of the SM's
   // 228 KB of shared memory (four resident CTAs, the register limit at 96
   // registers per thread): fewer sub-batches, fewer block barriers
-  static constexpr int CAP = WIDE ? (TS == 8 ? 512 : (TS == 12 ? 2048 : 1024)) : (TS == 12 ? 812 : 512);
+  static constexpr int CAP = WIDE ? (TS == 8 ? 512 : (TS == 12 ? 2048 : 1024)) : (TS == 12 ? 920 : 512);
   // resident CTAs per SM the register budget is sized for
   static constexpr int MINB = (WIDE ? 1 : 2) * (TS == 16 ? 1 : (TS == 12 ? 2 : 4));
 };
@@ -141,7 +141,10 @@ struct __align__(16) TileSmem {
   float4 pdir[TS * TS];     // pixel ray direction; w: the pixel's dL/dR (adjoint)
   float2 pdl[TS * TS];      // the pixel's dL/dG, dL/dB (adjoint); pixel and SSIM error (error mode)
   float4 item[Cfg::CAP];    // (cp.rgb, od) -> adjoint: (t_prev, d_od_state, has, aux_s)
-  float4 itemx[Cfg::CAP];   // (t_min, t_max, packed faces | tet | pixel, alpha_t)
+  // per item: (t_min, t_max) and the packed faces | tet | pixel (pack_item);
+  // its alpha_t = exp(-od) is recomputed from the od the item keeps
+  float2 itemt[Cfg::CAP];
+  uint32_t itemp[Cfg::CAP];
   float red[Cfg::NW][32][kRedCols];  // per-warp face sums and transpose (odd row stride)
   uint32_t toff[kBatch + 1];   // tet-major item offsets
   uint32_t pmask[TS * TS];
@@ -300,7 +303,7 @@ __device__ __forceinline__ void row_spans(const float sx[4], const float sy[4], 
   fwd = pack_span(span_of_cols(xl, xr, valid_cols));
 }
 
-// itemx.z packs the adjoint's exit/entry faces, the tet's batch slot and the pixel
+// itemp packs the adjoint's exit/entry faces, the tet's batch slot and the pixel
 __device__ __forceinline__ uint32_t pack_item(int fmin, int fmax, int k, int p) {
   return (uint32_t)fmin | ((uint32_t)fmax << 3) | ((uint32_t)k << 5) | ((uint32_t)p << 10);
 }
@@ -582,7 +585,8 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
         float t_min, t_max;
         int fmin, fmax;
         float4 out = make_float4(0.f, 0.f, 0.f, -1.0f);  // od < 0: the ray misses
-        float4 out2 = make_float4(0.f, 0.f, 0.f, 0.f);
+        float2 out_t = make_float2(0.f, 0.f);
+        uint32_t out_p = 0u;
         const bool hit = intersect4(tv.nrm, nump, d.x, d.y, d.z, t_min, t_max, fmin, fmax);
         if (hit) {
           float4 cb = tv.cb;
@@ -595,11 +599,15 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
           out = make_float4(clipf(I.cer * I.w0 + I.csr * I.w1, lo, kMaxVal),
                             clipf(I.ceg * I.w0 + I.csg * I.w1, lo, kMaxVal),
                             clipf(I.ceb * I.w0 + I.csb * I.w1, lo, kMaxVal), I.od);
-          out2 = make_float4(t_min, t_max, __uint_as_float(pack_item(fmin, fmax, k, p)), I.alpha_t);
+          out_t = make_float2(t_min, t_max);
+          out_p = pack_item(fmin, fmax, k, p);
         }
         if (MODE == kModeError && hit) out.x = out.y = out.z = 0.0f;  // (weight, counted) filled by phase 1
         s.item[i] = out;
-        if (AUX || !fwd || MODE == kModeError) s.itemx[i] = out2;
+        if (AUX || !fwd || MODE == kModeError) {
+          s.itemt[i] = out_t;
+          s.itemp[i] = out_p;
+        }
       }
     };
 
@@ -665,10 +673,11 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
                   Cr += c.x * Tj; Cg += c.y * Tj; Cb += c.z * Tj;
                   logT -= c.w;
                   if (AUX) {
-                    const float4 c2 = s.itemx[it];
-                    const float t_min = c2.x, t_max = c2.y, alpha_t = c2.w;
-                    const int entry = (int)(__float_as_uint(c2.z) & 7u);
+                    const float2 c2 = s.itemt[it];
+                    const float t_min = c2.x, t_max = c2.y;
+                    const int entry = (int)(s.itemp[it] & 7u);
                     const float od = c.w;
+                    const float alpha_t = __expf(-od);  // as the intersection phase computed it
                     const float ph = fabsf(od) < 0.02f
                                          ? 1.0f + od * (-0.5f + od * (1.0f / 6.0f + od * (-1.0f / 24.0f)))
                                          : clipf(__fdividef(1.0f - alpha_t, od), kMinVal, kMaxVal);
@@ -800,8 +809,8 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
               int k = -1;
               if (i < n_items) {
                 const float4 st = s.item[i];
-                const float4 ix = s.itemx[i];
-                const uint32_t pk = __float_as_uint(ix.z);
+                const float2 ix = s.itemt[i];
+                const uint32_t pk = s.itemp[i];
                 k = (int)((pk >> 5) & 31u);
                 if (st.y > 0.5f) {
                   const int p = (int)(pk >> 10);
@@ -995,7 +1004,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
                     const float* dla = a.dl_aux + pix * (size_t)a.aux_dim;
                     const float* ad = a.aux_data + (size_t)s.view[buf][k].meta.x * a.aux_dim;
                     for (int ai = 0; ai < a.aux_dim; ++ai) aux_s += dla[ai] * ad[ai];
-                    aux_w = (1.0f - s.itemx[it].w) * aux_s;  // alpha * aux_s
+                    aux_w = (1.0f - __expf(-c.w)) * aux_s;  // alpha * aux_s
                   }
                   dlogT = clipf(dlogT + (dlr * c.x + dlg * c.y + dlb * c.z + aux_w) * t_prev, kMinVal, kMaxVal);
                   s.item[it] = make_float4(t_prev, d_od_state, 1.0f, aux_s);
@@ -1072,8 +1081,8 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
                 // (t_prev, d_od_state, 1, aux_s) for an item with a gradient; ray misses
                 // and items below the transmittance cut have z = 0
                 if (!(st.z > 0.5f)) continue;
-                const float4 ix = s.itemx[i];
-                const uint32_t pk = __float_as_uint(ix.z);
+                const float2 ix = s.itemt[i];
+                const uint32_t pk = s.itemp[i];
                 const int p = (int)(pk >> 10);
                 int fmin = (int)(pk & 7u);
                 const int fmax = (int)((pk >> 3) & 3u);
@@ -1087,7 +1096,7 @@ __global__ void __launch_bounds__(TileCfg<TS, AUX, WIDE>::NT, TileCfg<TS, AUX, W
                 const float4 gg = tv.gm;
                 const float dcdt = dot3x(gg.x, gg.y, gg.z, d.x, d.y, d.z);
                 Integral I;
-                integrate(cb, dcdt, t_min, t_max, I, ix.w);
+                integrate(cb, dcdt, t_min, t_max, I);
                 const float dcpr = clipf(d.w * t_prev, kMinVal, kMaxVal);
                 const float dcpg = clipf(dgb.x * t_prev, kMinVal, kMaxVal);
                 const float dcpb = clipf(dgb.y * t_prev, kMinVal, kMaxVal);
