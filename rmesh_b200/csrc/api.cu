@@ -566,10 +566,13 @@ int run_bin(RmeshCtx* c, const ViewParams* views_dev, int n_views, uint32_t tota
   uint32_t* tv = nullptr;
   {
     StageScope sc(c, kStTetSort, capturing);
-    const int view_bits = n_views <= 1 ? 0 : bitlen((uint64_t)(n_views - 1));
+    // depth bits only: pairs of different views never share a tile, so the
+    // emission needs each view's entries in depth order (ties in item order,
+    // i.e. by tet id), which a stable sort of all views' keys on depth alone
+    // gives; the view and tile count ride in the key's high bits
     CKR(radix_sort<unsigned long long>(c, c->vis_key.as<unsigned long long>(), c->vis_val.as<uint32_t>(),
                                        c->vis_key_alt.as<unsigned long long>(), c->vis_val_alt.as<uint32_t>(),
-                                       &cnt->n_vis, 0, items, 32 + view_bits, &tk, &tv, capturing));
+                                       &cnt->n_vis, 0, items, 32, &tk, &tv, capturing));
   }
   {
     StageScope sc(c, kStEmit, capturing);
