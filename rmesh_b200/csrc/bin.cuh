@@ -1,8 +1,10 @@
 // Tile binning: emit (tile, tet) pairs in depth order, then per-tile ranges.
 //
-// Order of work (B200 design): tets are first sorted by (view, ~depth) at tet
-// granularity (onesweep, 32 + view bits; the tile count rides in the key's
-// high bits), then each tet emits its tiles at offsets given by a scan of
+// Order of work (B200 design): tets are first sorted by ~depth at tet
+// granularity (onesweep over the 32 depth bits of all views' entries at once:
+// pairs of different views never share a tile, so each view's entries in
+// depth order suffice; the view and tile count ride in the key's high bits),
+// then each tet emits its tiles at offsets given by a scan of
 // tiles_touched in that order (emit_scan_kernel), and a short
 // stable sort on the global tile id (ceil(log2 tiles) bits) finishes the job.
 // Per tile this yields exactly the reference's order -- ascending 64-bit key

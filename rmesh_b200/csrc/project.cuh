@@ -381,11 +381,11 @@ __device__ __forceinline__ uint32_t depth_key(const float4 C, const float* cam) 
 }
 
 // Sort keys of the tile-touching items, compacted in item order (within one
-// view: ascending tet id, the tie order of the stable (view, depth) sort):
+// view: ascending tet id, the tie order of the stable depth sort):
 //   key = count << 40 | view << 32 | ~bits(depth),  value = item index.
-// The sort orders bits 0..39 only (view < 64); the tile count rides in bits
-// 40..63 for the emission stage (saturated at kKeyCountMax, which then reads
-// vis_cnt).  A chained scan over blocks of kCompactItems items, each thread
+// The sort orders bits 0..31 only; the view (< 64) in bits 32..39 and the tile
+// count in bits 40..63 ride along for the emission stage (the count saturated
+// at kKeyCountMax, which then reads vis_cnt).  A chained scan over blocks of kCompactItems items, each thread
 // taking kCompactPerThread consecutive items.
 constexpr int kCompactPerThread = 8;
 constexpr int kCompactItems = 256 * kCompactPerThread;
